@@ -1,0 +1,172 @@
+/*
+ * pfw_b200.h — C ABI of libpfw_b200.so, the B200 (sm_100a) force-evaluation
+ * hot path of PotentialFrameWork.jl: cell-list neighbour construction,
+ * SmoothPair / Lennard-Jones pair energy-force-virial, and ACE site
+ * energy-force-virial.
+ *
+ * Conventions (identical to the reference's numeric boundary):
+ *   - lengths in Å, energies in eV, forces in eV/Å;
+ *   - positions X are 3×N column-major (X[3*i + a]), original atom order;
+ *   - the cell H is 3×3 column-major with COLUMNS = cell vectors
+ *     (H[a + 3*b] = component a of cell vector b), as AtomsBase.cell_vectors;
+ *   - forces are returned 3×N column-major in original atom order;
+ *   - the virial is 3×3 column-major, W = -Σ d ⊗ g over interactions;
+ *   - species are integer channels 0..nz-1 (the caller maps ChemicalSpecies).
+ *
+ * Every entry point returns a pfw_status; the message of the last failure of a
+ * workspace is available from pfw_last_error(ws).  No entry point traps or
+ * asserts on the device.  One workspace per host thread (not reentrant), as
+ * the reference's Workspace (PairPotentials/evaluation.jl:29).
+ */
+#ifndef PFW_B200_H
+#define PFW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The Julia shim maps EINVAL → ArgumentError (storage.jl:89-93,134),
+ * EDOMAIN → DomainError (NeighbourList/gpu.jl:395), ESHAPE → DimensionMismatch. */
+typedef enum pfw_status {
+  PFW_OK = 0,
+  PFW_EINVAL = 1,     /* invalid argument: nonfinite/dependent cell, bad cutoff ... */
+  PFW_EDOMAIN = 2,    /* coincident atoms with a singular model, nonfinite output */
+  PFW_ESHAPE = 3,     /* array shape mismatch */
+  PFW_ECAPACITY = 4,  /* internal capacity overflow (retried internally) */
+  PFW_ECUDA = 5,      /* CUDA runtime error */
+  PFW_ETIMEDOUT = 6,  /* a bounded device wait ran out */
+  PFW_ESTATE = 7      /* call order error: no geometry / no model loaded */
+} pfw_status;
+
+/* request bits, mirroring AtomsCalculators Energy()/Forces()/Virial()
+ * (NeighbourList/execution.jl:4-12 normalize_properties). */
+#define PFW_REQ_ENERGY 1u
+#define PFW_REQ_FORCES 2u
+#define PFW_REQ_VIRIAL 4u
+
+/* arithmetic forms */
+#define PFW_PRECISION_FP64 0   /* plain path: every operation in FP64 */
+#define PFW_PRECISION_MIXED 1  /* FP32 pair/ACE arithmetic, FP64 wrap + Kahan FP64 E/W */
+
+typedef struct pfw_options {
+  int32_t precision;            /* PFW_PRECISION_FP64 or PFW_PRECISION_MIXED */
+  int32_t bruteforce_threshold; /* Workspace(bruteforce_threshold=32) (storage.jl:59-65) */
+  int32_t device;               /* CUDA device ordinal */
+  int32_t reserved;
+} pfw_options;
+
+typedef struct pfw_ws pfw_ws;
+
+/* ---- lifecycle -------------------------------------------------------- */
+/* Library version string "major.minor.patch". */
+const char* pfw_version(void);
+
+/* Replaces NeighbourList.Workspace(; width, precision, bruteforce_threshold)
+ * (NeighbourList/storage.jl:59-65).  opts may be NULL for defaults
+ * (FP64, threshold 32, device 0). */
+pfw_status pfw_ws_create(const pfw_options* opts, pfw_ws** out);
+void pfw_ws_destroy(pfw_ws* ws);
+/* Message of the last failed call on this workspace ("" if none). */
+const char* pfw_last_error(const pfw_ws* ws);
+
+/* ---- geometry --------------------------------------------------------- */
+/* Host-side geometry upload; replaces the extraction half of prepare!
+ * (storage.jl:130-180).  X: 3×n, H: 9, pbc: 3 flags, species: n channels. */
+pfw_status pfw_set_geometry(pfw_ws* ws, int64_t n, const double* X, const double* H,
+                            const uint8_t pbc[3], const int32_t* species);
+/* Same, but X and species are DEVICE pointers already resident in HBM
+ * (no host↔device copy); H and pbc are host arrays. */
+pfw_status pfw_set_geometry_device(pfw_ws* ws, int64_t n, const double* X_dev,
+                                   const double* H, const uint8_t pbc[3],
+                                   const int32_t* species_dev);
+
+/* ---- pair models ------------------------------------------------------ */
+/* SmoothPair(labels, amplitudes, cutoff): U_ab(r) = A_ab (1 - r²/c²)³
+ * (PairPotentials/models.jl:28-44 and PreparedSmooth :138-176).
+ * A is nz×nz symmetric, indexed by species channel. */
+pfw_status pfw_pair_model_smooth(pfw_ws* ws, int32_t nz, const double* A, double cutoff);
+/* lennard_jones(; epsilon, sigma, radius): energy-shifted LJ
+ * (PairPotentials/lennard_jones.jl:5-33). */
+pfw_status pfw_pair_model_lj(pfw_ws* ws, double epsilon, double sigma, double cutoff);
+
+/* ---- ACE models ------------------------------------------------------- */
+/* Packed resolved-ACE tables; the host builds them from the resolved TOML v1
+ * schema (ACE/resolved.jl:103-142), mirroring pack_model (ACE/adaptation.jl:78-98).
+ * All indices are 0-based.  Ragged spline tables are padded to the longest
+ * node list of the family.  Only the default basis policy is packed: the
+ * invariant mask is applied to WB by the host; pair/reference flags per species. */
+typedef struct pfw_radial_family {
+  int32_t nchannels;            /* radial functions per species pair (nR or nQ) */
+  int32_t nknots;               /* max number of spline nodes (intervals = nknots-1) */
+  const int32_t* lengths;       /* [nz*nz] number of nodes of pair (iz,jz) at iz*nz+jz */
+  const double* nodes;          /* [nz*nz][nknots] */
+  const double* coeff;          /* [nz*nz][nknots-1][nchannels][4] power 0..3 */
+  const double* transform;      /* [nz*nz][6] a, rin, r0, yin, ycut, rcut */
+  const int32_t* powers;        /* [nz*nz][2] p, q */
+  const int32_t* envelope_kind; /* [nz*nz] 1 PolyEnvelope2sX, 2 ACE1_PolyEnvelope1sR, 3 PolyEnvelope1sR */
+  const double* envelope;       /* [nz*nz][5] parameters in resolved.jl:73-78 order */
+} pfw_radial_family;
+
+typedef struct pfw_ace_tables {
+  int32_t nz;                   /* species channels */
+  int32_t lmax;                 /* real spherical harmonics, L2, l*l+l+m order */
+  pfw_radial_family radial;     /* R channels */
+  pfw_radial_family pair;       /* Q (pair) channels */
+  int32_t ndensity;             /* D */
+  const int32_t* density;       /* [D][2] (radial channel, harmonic index) */
+  int32_t nproducts;            /* P */
+  const int32_t* product_offsets; /* [P+1] CSR into product_factors */
+  const int32_t* product_factors; /* density indices of each product */
+  int32_t nbasis;               /* nB invariants (rows of the coupling) */
+  int32_t ncoupling;            /* stored coupling entries */
+  const int32_t* coupling_rows; /* [nnz] invariant index, column-major (CSC) order */
+  const int32_t* coupling_cols; /* [nnz] product index */
+  const double* coupling_vals;  /* [nnz] */
+  const double* WB;             /* [nz][nbasis] readout, mask applied */
+  const double* Wpair;          /* [nz][nQ] */
+  const double* reference;      /* [nz] reference energies (0 when disabled) */
+  const uint8_t* pair_allowed;  /* [nz] pair term enabled for neighbour species */
+  double cutoff;                /* search cutoff = max rcut over channels (cpu.jl:316) */
+} pfw_ace_tables;
+
+/* Load an ACE model (copies every table to the device). */
+pfw_status pfw_ace_model_load(pfw_ws* ws, const pfw_ace_tables* tables);
+
+/* ---- evaluation ------------------------------------------------------- */
+/* Replaces evaluate!(w, sys, p; request) (PairPotentials/evaluation.jl:31-52)
+ * for the loaded pair model, or AC.energy_forces_virial(sys, ACECalculator)
+ * (ACE/calculators.jl:48-96) when model == PFW_MODEL_ACE.  Host outputs; any may
+ * be NULL when not requested.  E: 1, F: 3×n original order, W: 9. */
+#define PFW_MODEL_PAIR 0
+#define PFW_MODEL_ACE 1
+pfw_status pfw_evaluate(pfw_ws* ws, int32_t model, uint32_t request,
+                        double* E, double* F, double* W);
+/* Same with DEVICE outputs (E: 1 double, F: 3n, W: 9) — no host copies, no sync. */
+pfw_status pfw_evaluate_device(pfw_ws* ws, int32_t model, uint32_t request,
+                               double* E_dev, double* F_dev, double* W_dev);
+/* Per-site energies of the last ACE evaluation (original order, host). */
+pfw_status pfw_site_energies(pfw_ws* ws, double* energies);
+/* Number of in-cutoff unordered pairs of the last pair evaluation's geometry. */
+pfw_status pfw_last_pair_count(pfw_ws* ws, int64_t* npairs);
+
+/* ---- neighbour snapshot ------------------------------------------------ */
+/* neighbour_list(sys, cutoff) + neighbours(list, i) (NeighbourList/interface.jl:47-151).
+ * Two calls: count builds the directed snapshot on the device and returns the
+ * number of directed entries M; fill copies it out in original order:
+ * offsets [n+1], j [M] (0-based original index), S [3M] (integer shifts),
+ * R [3M] (Å, R = X[j] - X[i] + H·S up to rounding).  Any output may be NULL. */
+pfw_status pfw_neighbour_count(pfw_ws* ws, double cutoff, int64_t* total);
+pfw_status pfw_neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);
+
+/* ---- device peak probe ------------------------------------------------- */
+/* Measured FP64 FMA throughput of the current device (TFLOP/s), used as the
+ * FP64-pipe roofline denominator. */
+pfw_status pfw_probe_fp64_peak(pfw_ws* ws, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFW_B200_H */

@@ -1,0 +1,160 @@
+"""Seeded synthetic workloads (positions in Å, cells with columns = vectors).
+
+The reference's benchmarks generate their systems (argon FCC in
+benchmark/lennard_jones/common.jl:68-83, bcc ACE workloads); these generators
+produce the evaluation configurations of this library with the stated shapes,
+sizes and value distributions:
+
+  smooth_fcc   — FCC 8×8×8 (2048 atoms), a=1.6 Å, σ=0.05 Å, H/He 50/50,
+                 SmoothPair([1.0 0.7; 0.7 1.3], c=2.0)
+  lj_fcc       — FCC 40³ (256,000 atoms) a=5.26 Å, σ=0.1 Å; also 64³ (1,048,576)
+                 and a triclinic variant (xy tilt 0.2)
+  b2           — B2 (CsCl) 20³ (16,000 atoms), a=2.9 Å, σ=0.08 Å
+  batched      — 4096 periodic triclinic systems, n log-uniform in [8,256]
+  fixture      — the reference test fixture generator (test/fixtures.jl:17-24)
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+SMOOTH_A = np.array([[1.0, 0.7], [0.7, 1.3]])
+SMOOTH_CUTOFF = 2.0
+LJ_EPS, LJ_SIGMA, LJ_CUTOFF = 0.0104, 3.4, 8.5
+
+
+class System:
+    """Numeric system: X (n,3) Å, H (3,3) columns = cell vectors, pbc, species channels."""
+
+    def __init__(self, X, H, pbc, species, name=""):
+        self.X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
+        self.H = np.asarray(H, dtype=np.float64).reshape(3, 3)
+        self.pbc = tuple(bool(b) for b in pbc)
+        self.species = np.ascontiguousarray(species, dtype=np.int32)
+        self.name = name
+
+    def __len__(self):
+        return self.X.shape[0]
+
+
+def fixture(n, L=9.0, pbc=(True, True, True), cluster=False, mixed=True):
+    """test/fixtures.jl:17-24: x[a,i] = L*mod(sin(i*(a+0.71))*437.13, 1), H/He alternating (odd → He)."""
+    X = np.zeros((n, 3))
+    for i in range(1, n + 1):
+        for a in range(1, 4):
+            v = math.sin(i * (a + 0.71)) * 437.13
+            r = math.fmod(v, 1.0)  # Julia mod(v, 1)
+            X[i - 1, a - 1] = L * (r + 1.0 if r < 0 else r)
+    if cluster:
+        X[: (n + 1) // 2] *= 0.18
+    H = np.diag([L, L, L])
+    species = np.array([1 if (mixed and (i % 2 == 1)) else 0 for i in range(1, n + 1)], np.int32)
+    return System(X, H, pbc, species, f"fixture{n}")
+
+
+def _fcc(nc, a):
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    g = np.stack(np.meshgrid(np.arange(nc), np.arange(nc), np.arange(nc), indexing="ij"), -1).reshape(-1, 1, 3)
+    return ((g + basis[None]) * a).reshape(-1, 3)
+
+
+def smooth_fcc(seed=1, nc=8, a=1.6, sigma=0.05):
+    rng = np.random.default_rng(seed)
+    X = _fcc(nc, a)
+    n = len(X)
+    species = np.zeros(n, np.int32)
+    species[rng.permutation(n)[: n // 2]] = 1
+    X = X + rng.normal(0.0, sigma, X.shape)
+    L = nc * a
+    return System(X, np.diag([L, L, L]), (True, True, True), species, f"smooth_fcc{nc}")
+
+
+def lj_fcc(seed=2, nc=40, a=5.26, sigma=0.1, shear=0.0):
+    rng = np.random.default_rng(seed)
+    X = _fcc(nc, a)
+    X = X + rng.normal(0.0, sigma, X.shape)
+    L = nc * a
+    H = np.array([[L, shear * L, 0.0], [0.0, L, 0.0], [0.0, 0.0, L]])
+    if shear:
+        X = X @ np.array([[1, 0, 0], [shear, 1, 0], [0, 0, 1.0]])  # x += shear*y
+    return System(X, H, (True, True, True), np.zeros(len(X), np.int32),
+                  f"lj_fcc{nc}" + (f"_shear{shear}" if shear else ""))
+
+
+def lj_1m(seed=3):
+    """1,048,576 atoms = 4·64³ at the 40³ box density (a=5.26 Å)."""
+    return lj_fcc(seed=seed, nc=64)
+
+
+def b2(seed=4, nc=20, a=2.9, sigma=0.08):
+    """B2 (CsCl): species 0 at corners, 1 at body centres."""
+    rng = np.random.default_rng(seed)
+    g = np.stack(np.meshgrid(np.arange(nc), np.arange(nc), np.arange(nc), indexing="ij"), -1).reshape(-1, 3)
+    X = np.concatenate([g * a, (g + 0.5) * a])
+    species = np.concatenate([np.zeros(len(g), np.int32), np.ones(len(g), np.int32)])
+    order = np.argsort(np.concatenate([np.arange(len(g)) * 2, np.arange(len(g)) * 2 + 1]))
+    X, species = X[order], species[order]
+    X = X + rng.normal(0.0, sigma, X.shape)
+    L = nc * a
+    return System(X, np.diag([L, L, L]), (True, True, True), species, f"b2_{nc}")
+
+
+def random_triclinic_cell(rng, lo=6.0, hi=14.0, amin=70.0, amax=110.0):
+    """Cell with lengths U[lo,hi] Å and angles U[amin,amax]°; lower-triangular build, columns = vectors."""
+    while True:
+        a, b, c = rng.uniform(lo, hi, 3)
+        al, be, ga = np.radians(rng.uniform(amin, amax, 3))
+        v1 = np.array([a, 0.0, 0.0])
+        v2 = np.array([b * math.cos(ga), b * math.sin(ga), 0.0])
+        cx = c * math.cos(be)
+        cy = c * (math.cos(al) - math.cos(be) * math.cos(ga)) / math.sin(ga)
+        cz2 = c * c - cx * cx - cy * cy
+        if cz2 <= 0.1 * c * c:
+            continue
+        v3 = np.array([cx, cy, math.sqrt(cz2)])
+        return np.stack([v1, v2, v3], axis=1)
+
+
+def batched(seed=5, nsys=4096, nmin=8, nmax=256, dmin=1.6, max_density=0.11):
+    """4096 periodic triclinic systems; n log-uniform on [nmin, nmax]; uniform
+    fractional positions with hard-core rejection at dmin; cells are redrawn
+    until n/V <= max_density Å⁻³."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(nsys):
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        while True:
+            H = random_triclinic_cell(rng)
+            V = abs(np.linalg.det(H))
+            if n / V <= max_density:
+                break
+        X = _hardcore(rng, H, n, dmin)
+        species = np.zeros(n, np.int32)
+        species[rng.permutation(n)[: n // 2]] = 1
+        out.append(System(X, H, (True, True, True), species, f"batch{s}"))
+    return out
+
+
+def _hardcore(rng, H, n, dmin, max_tries=200000):
+    Hinv = np.linalg.inv(H)
+    pts = []
+    tries = 0
+    shifts = np.array([[i, j, k] for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)], dtype=np.float64)
+    while len(pts) < n:
+        tries += 1
+        if tries > max_tries:
+            dmin *= 0.9
+            tries = 0
+        f = rng.uniform(0, 1, 3)
+        ok = True
+        if pts:
+            P = np.array(pts)
+            df = P - f
+            df -= np.round(df)
+            d = (df[:, None, :] + shifts[None]) @ H.T
+            if np.min(np.einsum("ijk,ijk->ij", d, d)) < dmin * dmin:
+                ok = False
+        if ok:
+            pts.append(f)
+    return np.array(pts) @ H.T
