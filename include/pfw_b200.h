@@ -166,6 +166,22 @@ pfw_status pfw_neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t*
  * FP64-pipe roofline denominator. */
 pfw_status pfw_probe_fp64_peak(pfw_ws* ws, double* tflops);
 
+/* Number of kernels this workspace has launched (monotone counter). */
+uint64_t pfw_launch_count(const pfw_ws* ws);
+
+/* Run the workspace's work on the caller's CUDA stream (a cudaStream_t; NULL
+ * restores the workspace's own stream).  The caller keeps ownership. */
+pfw_status pfw_set_stream(pfw_ws* ws, void* stream);
+
+/* Stage diagnostics (the reference's gpu_stage_stamp!, ACE/gpu.jl:565-570):
+ * when on, CUDA events bracket each stage of pfw_evaluate*; pfw_stage_times
+ * waits for the last evaluation and returns its stage durations in ms:
+ * [0] geometry (wrap, bins, sort), [1] main kernel (pair or ACE sites),
+ * [2] reductions and force assembly, [3] neighbour-list build (ACE).
+ * Returns the number of stages written (<= cap). */
+pfw_status pfw_set_diagnostics(pfw_ws* ws, int32_t on);
+int32_t pfw_stage_times(pfw_ws* ws, double* ms, int32_t cap);
+
 #ifdef __cplusplus
 }
 #endif

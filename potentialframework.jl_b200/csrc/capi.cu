@@ -1,0 +1,273 @@
+// capi.cu — the extern "C" boundary of libpfw_b200.so (include/pfw_b200.h).
+//
+// Every entry point catches internal errors and returns a pfw_status with
+// the message kept in the workspace (pfw_last_error).  Nothing here falls
+// back to a CPU computation: a missing device is an error.
+#include <cmath>
+#include <cstdio>
+#include <new>
+
+#include "pfw_internal.h"
+
+using pfw::Error;
+
+namespace {
+
+pfw_status fail(pfw_ws* ws, pfw_status code, const std::string& msg) {
+  if (ws) ws->err = msg;
+  return code;
+}
+
+template <class F>
+pfw_status guarded(pfw_ws* ws, F&& f) {
+  if (!ws) return PFW_EINVAL;
+  try {
+    PFW_CUDA(cudaSetDevice(ws->opt.device));
+    ws->err.clear();
+    f();
+    return PFW_OK;
+  } catch (const Error& e) {
+    return fail(ws, e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(ws, PFW_ECUDA, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(ws, PFW_EINVAL, e.what());
+  }
+}
+
+void upload_geometry(pfw_ws* ws, int64_t n, const double* X, const double* H, const uint8_t pbc[3],
+                     const int32_t* species, bool device_ptrs) {
+  if (n < 0 || n > (int64_t)INT32_MAX / 4) throw Error(PFW_EINVAL, "atom count out of range");
+  if (n > 0 && (!X || !species)) throw Error(PFW_EINVAL, "positions and species are required");
+  if (!H || !pbc) throw Error(PFW_EINVAL, "cell and pbc are required");
+  pfw::HostSystem hs;
+  for (int k = 0; k < 9; ++k) hs.H[k] = H[k];
+  for (int a = 0; a < 3; ++a) hs.pbc[a] = pbc[a] ? 1 : 0;
+  hs.atom_begin = 0;
+  hs.natoms = (int32_t)n;
+  ws->systems.assign(1, hs);
+  ws->n = (int32_t)n;
+  cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  ws->X.ensure(sizeof(double) * 3 * std::max<int64_t>(n, 1));
+  ws->species.ensure(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  if (n > 0) {
+    PFW_CUDA(cudaMemcpyAsync(ws->X.ptr, X, sizeof(double) * 3 * n, kind, ws->stream));
+    PFW_CUDA(cudaMemcpyAsync(ws->species.ptr, species, sizeof(int32_t) * n, kind, ws->stream));
+  }
+  ws->max_species = 0;
+  if (!device_ptrs && n > 0) {
+    for (int64_t i = 0; i < n; ++i) {
+      if (species[i] < 0) throw Error(PFW_EINVAL, "species channels must be nonnegative");
+      ws->max_species = std::max(ws->max_species, species[i]);
+    }
+  }
+  ws->prep.valid = false;
+  ws->nb_total = -1;
+  ws->last_pairs = -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pfw_version(void) { return "0.1.0"; }
+
+pfw_status pfw_ws_create(const pfw_options* opts, pfw_ws** out) {
+  if (!out) return PFW_EINVAL;
+  *out = nullptr;
+  pfw_ws* ws = new (std::nothrow) pfw_ws();
+  if (!ws) return PFW_ECUDA;
+  if (opts) ws->opt = *opts;
+  else {
+    ws->opt.precision = PFW_PRECISION_FP64;
+    ws->opt.bruteforce_threshold = 32;
+    ws->opt.device = 0;
+  }
+  if (ws->opt.bruteforce_threshold < 0 ||
+      (ws->opt.precision != PFW_PRECISION_FP64 && ws->opt.precision != PFW_PRECISION_MIXED)) {
+    delete ws;
+    return PFW_EINVAL;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev <= ws->opt.device) {
+    delete ws;
+    return PFW_ECUDA;
+  }
+  if (cudaSetDevice(ws->opt.device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ws;
+    return PFW_ECUDA;
+  }
+  *out = ws;
+  return PFW_OK;
+}
+
+void pfw_ws_destroy(pfw_ws* ws) {
+  if (!ws) return;
+  cudaSetDevice(ws->opt.device);
+  if (ws->stream) cudaStreamSynchronize(ws->stream);
+  pfw::ace_free(ws);
+  pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
+                         &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
+                         &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
+                         &ws->minmax, &ws->cellpart, &ws->out_E, &ws->out_F, &ws->out_W, &ws->counters,
+                         &ws->nb_count, &ws->nb_offsets, &ws->nb_j, &ws->nb_S, &ws->nb_R};
+  for (auto* b : bufs) b->release();
+  if (ws->stream) cudaStreamDestroy(ws->stream);
+  delete ws;
+}
+
+const char* pfw_last_error(const pfw_ws* ws) { return ws ? ws->err.c_str() : "null workspace"; }
+
+pfw_status pfw_set_geometry(pfw_ws* ws, int64_t n, const double* X, const double* H, const uint8_t pbc[3],
+                            const int32_t* species) {
+  return guarded(ws, [&] { upload_geometry(ws, n, X, H, pbc, species, false); });
+}
+
+pfw_status pfw_set_geometry_device(pfw_ws* ws, int64_t n, const double* X_dev, const double* H,
+                                   const uint8_t pbc[3], const int32_t* species_dev) {
+  return guarded(ws, [&] { upload_geometry(ws, n, X_dev, H, pbc, species_dev, true); });
+}
+
+pfw_status pfw_pair_model_smooth(pfw_ws* ws, int32_t nz, const double* A, double cutoff) {
+  return guarded(ws, [&] {
+    if (nz < 1 || nz > 4) throw Error(PFW_EINVAL, "SmoothPair supports 1 to 4 species channels");
+    if (!A) throw Error(PFW_EINVAL, "amplitude table required");
+    if (!(std::isfinite(cutoff) && cutoff > 0)) throw Error(PFW_EINVAL, "cutoff must be finite and positive");
+    for (int a = 0; a < nz; ++a)
+      for (int b = 0; b < nz; ++b)
+        if (!std::isfinite(A[a * nz + b]) || A[a * nz + b] != A[b * nz + a])
+          throw Error(PFW_EINVAL, "amplitude table must be finite and symmetric");
+    ws->pair.kind = 0;
+    ws->pair.nz = nz;
+    ws->pair.A.assign(A, A + nz * nz);
+    ws->pair.cutoff = cutoff;
+  });
+}
+
+pfw_status pfw_pair_model_lj(pfw_ws* ws, double epsilon, double sigma, double cutoff) {
+  return guarded(ws, [&] {
+    if (!(std::isfinite(epsilon) && std::isfinite(sigma) && std::isfinite(cutoff) && epsilon > 0 && sigma > 0 &&
+          cutoff > 0))
+      throw Error(PFW_EINVAL, "LJ parameters must be positive and finite");
+    ws->pair.kind = 1;
+    ws->pair.nz = 1;
+    ws->pair.eps = epsilon;
+    ws->pair.sigma = sigma;
+    ws->pair.cutoff = cutoff;
+  });
+}
+
+pfw_status pfw_ace_model_load(pfw_ws* ws, const pfw_ace_tables* tables) {
+  return guarded(ws, [&] {
+    if (!tables) throw Error(PFW_EINVAL, "tables required");
+    pfw::ace_load(ws, tables);
+  });
+}
+
+pfw_status pfw_evaluate_device(pfw_ws* ws, int32_t model, uint32_t request, double* E_dev, double* F_dev,
+                               double* W_dev) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    if (model == PFW_MODEL_PAIR) pfw::pair_evaluate(ws, request, E_dev, F_dev, W_dev);
+    else if (model == PFW_MODEL_ACE) pfw::ace_evaluate(ws, request, E_dev, F_dev, W_dev);
+    else throw Error(PFW_EINVAL, "unknown model selector");
+  });
+}
+
+pfw_status pfw_evaluate(pfw_ws* ws, int32_t model, uint32_t request, double* E, double* F, double* W) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    const int n = ws->n;
+    double* dE = static_cast<double*>(ws->out_E.ensure(sizeof(double)));
+    double* dW = static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
+    double* dF = (request & PFW_REQ_FORCES) ? static_cast<double*>(ws->out_F.ensure(sizeof(double) * 3 * std::max(n, 1)))
+                                            : nullptr;
+    if (model == PFW_MODEL_PAIR) pfw::pair_evaluate(ws, request, dE, dF, dW);
+    else if (model == PFW_MODEL_ACE) pfw::ace_evaluate(ws, request, dE, dF, dW);
+    else throw Error(PFW_EINVAL, "unknown model selector");
+    double hE = 0, hW[9];
+    unsigned long long np = 0;
+    PFW_CUDA(cudaMemcpyAsync(&hE, dE, sizeof(double), cudaMemcpyDeviceToHost, ws->stream));
+    PFW_CUDA(cudaMemcpyAsync(hW, dW, sizeof(double) * 9, cudaMemcpyDeviceToHost, ws->stream));
+    if (model == PFW_MODEL_PAIR)
+      PFW_CUDA(cudaMemcpyAsync(&np, static_cast<unsigned long long*>(ws->counters.ptr) + 4, sizeof(np),
+                               cudaMemcpyDeviceToHost, ws->stream));
+    if (F && dF && n > 0)
+      PFW_CUDA(cudaMemcpyAsync(F, dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ws->stream));
+    PFW_CUDA(cudaStreamSynchronize(ws->stream));
+    if (model == PFW_MODEL_PAIR) ws->last_pairs = (int64_t)np / 2;
+    // the reference GPU reports nonfinite results as a DomainError (NeighbourList/gpu.jl:391-395)
+    bool finite = std::isfinite(hE);
+    for (double v : hW) finite = finite && std::isfinite(v);
+    if (!finite) throw Error(PFW_EDOMAIN, "nonfinite energy/virial (coincident atoms with a singular model?)");
+    if (E) *E = hE;
+    if (W)
+      for (int k = 0; k < 9; ++k) W[k] = hW[k];
+  });
+}
+
+pfw_status pfw_site_energies(pfw_ws* ws, double* energies) {
+  return guarded(ws, [&] { pfw::ace_site_energies(ws, energies); });
+}
+
+pfw_status pfw_last_pair_count(pfw_ws* ws, int64_t* npairs) {
+  return guarded(ws, [&] {
+    if (!npairs) throw Error(PFW_EINVAL, "null output");
+    *npairs = ws->last_pairs;
+  });
+}
+
+pfw_status pfw_neighbour_count(pfw_ws* ws, double cutoff, int64_t* total) {
+  return guarded(ws, [&] {
+    int64_t t = pfw::neighbour_build(ws, cutoff);
+    if (total) *total = t;
+  });
+}
+
+pfw_status pfw_neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R) {
+  return guarded(ws, [&] { pfw::neighbour_fill(ws, offsets, j, S, R); });
+}
+
+pfw_status pfw_probe_fp64_peak(pfw_ws* ws, double* tflops) {
+  return guarded(ws, [&] {
+    double v = pfw::probe_fp64(ws);
+    if (tflops) *tflops = v;
+  });
+}
+
+uint64_t pfw_launch_count(const pfw_ws* ws) { return ws ? ws->launches : 0; }
+
+pfw_status pfw_set_stream(pfw_ws* ws, void* stream) {
+  return guarded(ws, [&] {
+    PFW_CUDA(cudaStreamSynchronize(ws->stream));
+    ws->stream = stream ? static_cast<cudaStream_t>(stream) : ws->own_stream;
+  });
+}
+
+pfw_status pfw_set_diagnostics(pfw_ws* ws, int32_t on) {
+  return guarded(ws, [&] {
+    if (on && !ws->ev[0])
+      for (auto& e : ws->ev) PFW_CUDA(cudaEventCreate(&e));
+    ws->diag = on != 0;
+    for (auto& u : ws->ev_used) u = false;
+  });
+}
+
+int32_t pfw_stage_times(pfw_ws* ws, double* ms, int32_t cap) {
+  if (!ws || !ws->diag || !ms) return 0;
+  if (cudaSetDevice(ws->opt.device) != cudaSuccess) return 0;
+  int32_t k = 0;
+  for (int s = 0; s < 4 && k < cap; ++s, ++k) {
+    float t = 0;
+    if (ws->ev_used[s] && cudaEventSynchronize(ws->ev[2 * s + 1]) == cudaSuccess &&
+        cudaEventElapsedTime(&t, ws->ev[2 * s], ws->ev[2 * s + 1]) == cudaSuccess)
+      ms[k] = t;
+    else
+      ms[k] = 0;
+  }
+  return k;
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+// pfw_internal.h — workspace state and internal interfaces of libpfw_b200.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pfw_b200.h"
+#include "pfw_common.cuh"
+
+namespace pfw {
+
+struct Error : std::runtime_error {
+  pfw_status code;
+  Error(pfw_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define PFW_CUDA(call)                                                                             \
+  do {                                                                                             \
+    cudaError_t _e = (call);                                                                       \
+    if (_e != cudaSuccess)                                                                         \
+      throw ::pfw::Error(PFW_ECUDA, std::string(#call) + ": " + cudaGetErrorString(_e));           \
+  } while (0)
+
+// Growable device buffer (never shrinks; contents not preserved on growth).
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  void* ensure(size_t bytes) {
+    if (bytes > cap) {
+      if (ptr) cudaFree(ptr);
+      ptr = nullptr;
+      size_t want = bytes < 256 ? 256 : bytes + bytes / 4;
+      PFW_CUDA(cudaMalloc(&ptr, want));
+      cap = want;
+    }
+    return ptr;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+};
+
+// Host description of one system before device preparation.
+struct HostSystem {
+  double H[9];
+  uint8_t pbc[3];
+  int32_t atom_begin, natoms;
+};
+
+// Device geometry after prepare (sorted atoms in cells).
+struct Prepared {
+  double cutoff = -1;
+  int32_t n = 0;
+  int32_t ncells = 0;
+  int32_t nsys = 0;
+  int32_t max_cell = 0;  // largest cell population
+  bool any_image = false;
+  std::vector<SysGeom> sys;  // host copy
+  bool valid = false;
+};
+
+struct PairModel {
+  int kind = -1;  // 0 smooth, 1 LJ
+  int nz = 0;
+  std::vector<double> A;
+  double eps = 0, sigma = 0, cutoff = 0;
+};
+
+struct AceDevice;  // ace.cu
+
+}  // namespace pfw
+
+struct pfw_ws {
+  pfw_options opt{};
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // geometry input (original order)
+  int32_t n = 0;
+  int32_t max_species = 0;  // largest species channel of host-uploaded geometry
+  std::vector<pfw::HostSystem> systems;
+  pfw::DevBuf X, species, atom_sys;  // X: 3n doubles
+  // prepared geometry
+  pfw::Prepared prep;
+  pfw::DevBuf sysgeom, wrapped, bincoord, wind, cellid, slot, cell_count, cell_start, cell_sys, tmp_idx,
+      perm, inverse, pos, pos32, scan_tmp, minmax;
+  // pair evaluation
+  pfw::PairModel pair;
+  pfw::DevBuf cellpart, out_E, out_F, out_W, counters;
+  int64_t last_pairs = -1;
+  // neighbour snapshot
+  pfw::DevBuf nb_count, nb_offsets, nb_j, nb_S, nb_R;
+  int64_t nb_total = -1;
+  // ACE
+  pfw::AceDevice* ace = nullptr;
+  // bookkeeping
+  uint64_t launches = 0;
+  cudaStream_t own_stream = nullptr;  // the workspace's stream (stream may be the caller's)
+  // stage diagnostics: event pairs per stage
+  bool diag = false;
+  cudaEvent_t ev[8] = {};
+  bool ev_used[4] = {};
+  void stage_begin(int s) {
+    if (diag) {
+      cudaEventRecord(ev[2 * s], stream);
+      ev_used[s] = true;
+    }
+  }
+  void stage_end(int s) {
+    if (diag) cudaEventRecord(ev[2 * s + 1], stream);
+  }
+};
+
+namespace pfw {
+// geometry.cu
+void prepare(pfw_ws* ws, double cutoff);
+void exclusive_scan_i32(pfw_ws* ws, const int32_t* in, int32_t* out, int64_t n);  // out has n+1 entries
+void exclusive_scan_i64(pfw_ws* ws, const int32_t* in, int64_t* out, int64_t n);
+// pair.cu
+void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev);
+// snapshot.cu
+int64_t neighbour_build(pfw_ws* ws, double cutoff);
+void neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);
+// ace.cu
+void ace_load(pfw_ws* ws, const pfw_ace_tables* t);
+void ace_free(pfw_ws* ws);
+void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev);
+void ace_site_energies(pfw_ws* ws, double* host);
+double probe_fp64(pfw_ws* ws);
+
+inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
+}  // namespace pfw

@@ -1,0 +1,194 @@
+"""ctypes binding of libpfw_b200.so (the C ABI declared in include/pfw_b200.h).
+
+The library is built in-tree (potentialframework.jl_b200/lib/).  Loading
+fails loudly when it is missing or when no CUDA device is present: there is
+no CPU fallback anywhere in the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .ace_model import pfw_ace_tables
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBPATH = os.path.join(PKG, "lib", "libpfw_b200.so")
+
+OK, EINVAL, EDOMAIN, ESHAPE, ECAPACITY, ECUDA, ETIMEDOUT, ESTATE = range(8)
+REQ_E, REQ_F, REQ_V = 1, 2, 4
+FP64, MIXED = 0, 1
+MODEL_PAIR, MODEL_ACE = 0, 1
+
+
+class pfw_options(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("bruteforce_threshold", C.c_int32), ("device", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class PFWError(RuntimeError):
+    """Error status from the library; subclasses mirror the reference's exceptions."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class ArgumentError(PFWError, ValueError):
+    pass
+
+
+class DomainError(PFWError, ArithmeticError):
+    pass
+
+
+class DimensionMismatch(PFWError, ValueError):
+    pass
+
+
+_ERRORS = {EINVAL: ArgumentError, EDOMAIN: DomainError, ESHAPE: DimensionMismatch}
+_lib = None
+
+dp = C.POINTER(C.c_double)
+i32p = C.POINTER(C.c_int32)
+i64p = C.POINTER(C.c_int64)
+u8p = C.POINTER(C.c_uint8)
+vp = C.c_void_p
+
+
+def load():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise RuntimeError(f"libpfw_b200.so not built: run `python -m pfw_b200.build` in {PKG}")
+    L = C.CDLL(LIBPATH)
+    L.pfw_version.restype = C.c_char_p
+    L.pfw_ws_create.argtypes = [C.POINTER(pfw_options), C.POINTER(vp)]
+    L.pfw_ws_destroy.argtypes = [vp]
+    L.pfw_ws_destroy.restype = None
+    L.pfw_last_error.argtypes = [vp]
+    L.pfw_last_error.restype = C.c_char_p
+    L.pfw_set_geometry.argtypes = [vp, C.c_int64, dp, dp, u8p, i32p]
+    L.pfw_set_geometry_device.argtypes = [vp, C.c_int64, vp, dp, u8p, vp]
+    L.pfw_pair_model_smooth.argtypes = [vp, C.c_int32, dp, C.c_double]
+    L.pfw_pair_model_lj.argtypes = [vp, C.c_double, C.c_double, C.c_double]
+    L.pfw_ace_model_load.argtypes = [vp, C.POINTER(pfw_ace_tables)]
+    L.pfw_evaluate.argtypes = [vp, C.c_int32, C.c_uint32, dp, dp, dp]
+    L.pfw_evaluate_device.argtypes = [vp, C.c_int32, C.c_uint32, vp, vp, vp]
+    L.pfw_site_energies.argtypes = [vp, dp]
+    L.pfw_last_pair_count.argtypes = [vp, i64p]
+    L.pfw_neighbour_count.argtypes = [vp, C.c_double, i64p]
+    L.pfw_neighbour_fill.argtypes = [vp, i64p, i32p, i32p, dp]
+    L.pfw_probe_fp64_peak.argtypes = [vp, dp]
+    L.pfw_launch_count.argtypes = [vp]
+    L.pfw_launch_count.restype = C.c_uint64
+    _lib = L
+    return L
+
+
+def ptr(a, t):
+    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+class Handle:
+    """Owns one pfw_ws (one per host thread; not reentrant)."""
+
+    def __init__(self, precision=FP64, bruteforce_threshold=32, device=0):
+        L = load()
+        opt = pfw_options(int(precision), int(bruteforce_threshold), int(device), 0)
+        h = vp()
+        rc = L.pfw_ws_create(C.byref(opt), C.byref(h))
+        if rc != OK:
+            raise PFWError(rc, "pfw_ws_create failed (no CUDA device, or invalid options)")
+        self.ws = h
+        self.L = L
+
+    def check(self, rc):
+        if rc != OK:
+            msg = self.L.pfw_last_error(self.ws).decode()
+            raise _ERRORS.get(rc, PFWError)(rc, msg)
+
+    def close(self):
+        if getattr(self, "ws", None):
+            self.L.pfw_ws_destroy(self.ws)
+            self.ws = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self):
+        return int(self.L.pfw_launch_count(self.ws))
+
+    # --- thin wrappers ---------------------------------------------------
+    def set_geometry(self, X, H, pbc, species):
+        X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
+        Hf = np.asarray(H, dtype=np.float64).reshape(3, 3).ravel(order="F").copy()
+        pb = np.array([1 if b else 0 for b in pbc], dtype=np.uint8)
+        sp = np.ascontiguousarray(species, dtype=np.int32)
+        self.check(self.L.pfw_set_geometry(self.ws, X.shape[0], ptr(X, C.c_double), ptr(Hf, C.c_double),
+                                           ptr(pb, C.c_uint8), ptr(sp, C.c_int32)))
+        self.n = X.shape[0]
+
+    def set_geometry_device(self, n, X_dev_ptr, H, pbc, species_dev_ptr):
+        Hf = np.asarray(H, dtype=np.float64).reshape(3, 3).ravel(order="F").copy()
+        pb = np.array([1 if b else 0 for b in pbc], dtype=np.uint8)
+        self.check(self.L.pfw_set_geometry_device(self.ws, int(n), X_dev_ptr, ptr(Hf, C.c_double),
+                                                  ptr(pb, C.c_uint8), species_dev_ptr))
+        self.n = int(n)
+
+    def smooth(self, A, cutoff):
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        self.check(self.L.pfw_pair_model_smooth(self.ws, A.shape[0], ptr(A, C.c_double), float(cutoff)))
+
+    def lj(self, eps, sigma, cutoff):
+        self.check(self.L.pfw_pair_model_lj(self.ws, float(eps), float(sigma), float(cutoff)))
+
+    def ace(self, packed):
+        self._ace_tables = packed.tables()
+        self._ace_packed = packed
+        self.check(self.L.pfw_ace_model_load(self.ws, C.byref(self._ace_tables)))
+
+    def evaluate(self, model=MODEL_PAIR, request=7):
+        E = np.zeros(1)
+        W = np.zeros(9)
+        F = np.zeros((self.n, 3)) if request & REQ_F else None
+        self.check(self.L.pfw_evaluate(self.ws, model, request, ptr(E, C.c_double), ptr(F, C.c_double),
+                                       ptr(W, C.c_double)))
+        return float(E[0]), F, W.reshape(3, 3, order="F")
+
+    def evaluate_device(self, model, request, E_ptr, F_ptr, W_ptr):
+        self.check(self.L.pfw_evaluate_device(self.ws, model, request, E_ptr, F_ptr, W_ptr))
+
+    def site_energies(self):
+        e = np.zeros(self.n)
+        self.check(self.L.pfw_site_energies(self.ws, ptr(e, C.c_double)))
+        return e
+
+    def pair_count(self):
+        v = np.zeros(1, np.int64)
+        self.check(self.L.pfw_last_pair_count(self.ws, ptr(v, C.c_int64)))
+        return int(v[0])
+
+    def neighbour_list(self, cutoff):
+        tot = np.zeros(1, np.int64)
+        self.check(self.L.pfw_neighbour_count(self.ws, float(cutoff), ptr(tot, C.c_int64)))
+        M = int(tot[0])
+        offs = np.zeros(self.n + 1, np.int64)
+        j = np.zeros(M, np.int32)
+        S = np.zeros((M, 3), np.int32)
+        R = np.zeros((M, 3))
+        self.check(self.L.pfw_neighbour_fill(self.ws, ptr(offs, C.c_int64), ptr(j, C.c_int32), ptr(S, C.c_int32),
+                                             ptr(R, C.c_double)))
+        return offs, j, S, R
+
+    def probe_fp64(self):
+        v = np.zeros(1)
+        self.check(self.L.pfw_probe_fp64_peak(self.ws, ptr(v, C.c_double)))
+        return float(v[0])
