@@ -15,11 +15,11 @@
 #include <cmath>
 
 #include "pfw_internal.h"
+#include "traverse.cuh"
 
 namespace pfw {
 
 constexpr int PAIR_WARPS = 4;  // warps (home cells) per CTA
-constexpr int STAGE = 32;      // neighbour atoms staged per pass
 
 struct PairParams {
   int kind, nz;
@@ -35,248 +35,215 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// MODE 0: displacement = (x_j - x_i) + shift (explicit images, or minimum
-// image with the per-cell wrap); MODE 1: per-system runtime choice.
-template <int KIND, int MODE>
-__global__ void __launch_bounds__(PAIR_WARPS * 32)
-    k_pair64(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
-             const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
-             double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
-  __shared__ double4 stage[PAIR_WARPS][STAGE];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cell = blockIdx.x * PAIR_WARPS + warp;
-  if (cell >= ncells) return;
-  const SysGeom& g = sysv[cell_sys[cell]];
-  const int b = cell_start[cell], e = cell_start[cell + 1];
-  const int local = cell - g.cell_begin;
-  const int key[3] = {local / (g.dims[1] * g.dims[2]), (local / g.dims[2]) % g.dims[1], local % g.dims[2]};
-  const int cnt0 = stencil_count(g, 0), cnt1 = stencil_count(g, 1), cnt2 = stencil_count(g, 2);
-  const double c2 = g.c2;
-  double acc_e = 0, w0 = 0, w1 = 0, w2 = 0, w3 = 0, w4 = 0, w5 = 0;
-  unsigned long long np = 0;
-  for (int i0 = b; i0 < e; i0 += 32) {
-    const int i = i0 + lane;
-    const bool have = i < e;
-    double4 pi = have ? pos[i] : make_double4(0, 0, 0, 0);
-    double arow[4] = {0, 0, 0, 0};
-    if (KIND == 0) {
-      const int zi = min(max((int)pi.w, 0), prm.nz - 1);
+__device__ __forceinline__ void write_cell_parts(double* cellpart, int cell, int lane, double e, const double w[6],
+                                                 unsigned long long np, unsigned long long* npairs) {
+  e = warp_sum(e);
+  double ws[6];
 #pragma unroll
-      for (int z = 0; z < 4; ++z) arow[z] = z < prm.nz ? prm.A[zi * prm.nz + z] : 0.0;
-    }
-    double fx = 0, fy = 0, fz = 0;
-    for (int t0 = 0; t0 < cnt0; ++t0)
-      for (int t1 = 0; t1 < cnt1; ++t1)
-        for (int t2 = 0; t2 < cnt2; ++t2) {
-          const int off[3] = {stencil_offset(g, 0, t0), stencil_offset(g, 1, t1), stencil_offset(g, 2, t2)};
-          StencilEntry se;
-          stencil_entry(g, key, off, se);
-          if (se.cell < 0) continue;
-          const int jb = cell_start[se.cell], je = cell_start[se.cell + 1];
-          for (int j0 = jb; j0 < je; j0 += STAGE) {
-            const int nj = min(STAGE, je - j0);
-            __syncwarp();
-            if (lane < nj) stage[warp][lane] = pos[j0 + lane];
-            __syncwarp();
-            if (!have) continue;
-            for (int t = 0; t < nj; ++t) {
-              const double4 pj = stage[warp][t];
-              if (se.zero && j0 + t == i) continue;
-              double d[3];
-              if (MODE == 0) {
-                d[0] = xadd(xsub(pj.x, pi.x), se.sh[0]);
-                d[1] = xadd(xsub(pj.y, pi.y), se.sh[1]);
-                d[2] = xadd(xsub(pj.z, pi.z), se.sh[2]);
-              } else {
-                displacement(g, se, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, d);
-              }
-              const double r2 = xr2(d[0], d[1], d[2]);
-              if (!(r2 < c2)) continue;
-              ++np;
-              double en, coef;
-              if (KIND == 0) {
-                const int zj = (int)pj.w;
-                const double a = zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3];
-                const double q = 1.0 - r2 * prm.invc2;
-                const double aq2 = a * q * q;
-                en = aq2 * q;
-                coef = -6.0 * aq2 * prm.invc2;
-              } else {
-                const double ir2 = 1.0 / r2;
-                const double s2 = prm.sigma2 * ir2;
-                const double s6 = s2 * s2 * s2;
-                en = prm.eps4 * (s6 * s6 - s6) - prm.shift;
-                coef = prm.eps24 * (s6 - 2.0 * s6 * s6) * ir2;
-              }
-              const double gx = coef * d[0], gy = coef * d[1], gz = coef * d[2];
-              fx += gx;
-              fy += gy;
-              fz += gz;
-              acc_e += en;
-              w0 += d[0] * gx;
-              w1 += d[1] * gy;
-              w2 += d[2] * gz;
-              w3 += d[0] * gy;
-              w4 += d[0] * gz;
-              w5 += d[1] * gz;
-            }
-          }
-        }
-    if (have && prm.want_f) {
-      const int o = perm[i];
-      F[3 * o] = fx;
-      F[3 * o + 1] = fy;
-      F[3 * o + 2] = fz;
-    }
-  }
-  // every directed pair is seen from both ends: E and W take one half each
-  acc_e = warp_sum(acc_e);
-  w0 = warp_sum(w0); w1 = warp_sum(w1); w2 = warp_sum(w2);
-  w3 = warp_sum(w3); w4 = warp_sum(w4); w5 = warp_sum(w5);
+  for (int k = 0; k < 6; ++k) ws[k] = warp_sum(w[k]);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(0xffffffffu, np, o);
   if (lane == 0) {
+    // every directed pair is seen from both ends: E and W take one half each
     double* cp = cellpart + 8 * (size_t)cell;
-    cp[0] = 0.5 * acc_e;
-    cp[1] = -0.5 * w0; cp[2] = -0.5 * w1; cp[3] = -0.5 * w2;
-    cp[4] = -0.5 * w3; cp[5] = -0.5 * w4; cp[6] = -0.5 * w5;
+    cp[0] = 0.5 * e;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) cp[1 + k] = -0.5 * ws[k];
     cp[7] = 0;
     if (np) atomicAdd(npairs, np);
   }
 }
 
-// Mixed form: candidate test and pair arithmetic in FP32 on positions taken
-// relative to the home cell's first atom (the FP64 wrap/shift is applied
-// before the conversion); energy and virial accumulated per lane in
-// Kahan-compensated FP64.
+// Plain FP64 path.  MODE 0: displacement = (x_j - x_i) + cell shift;
+// MODE 1: per-pair minimum image (small boxes).
+template <int KIND, int MODE>
+__global__ void __launch_bounds__(PAIR_WARPS * 32)
+    k_pair64(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
+             const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
+             double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
+  __shared__ WarpStage stage[PAIR_WARPS];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cell = blockIdx.x * PAIR_WARPS + warp;
+  if (cell >= ncells) return;
+  const SysGeom& g = sysv[cell_sys[cell]];
+  double acc_e = 0, w[6] = {0, 0, 0, 0, 0, 0};
+  unsigned long long np = 0;
+  int cur = -1;
+  double fx = 0, fy = 0, fz = 0;
+  double arow[4] = {0, 0, 0, 0};
+  const bool want_f = prm.want_f;
+  warp_traverse_cell<MODE>(
+      g, cell, cell_start, pos, stage[warp], lane,
+      [&](int i, int, const double4& pi, const double4& pj, const StencilEntry&, const double* d, double r2) {
+        if (i != cur) {
+          if (cur >= 0 && want_f) {
+            const int o = perm[cur];
+            F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
+          }
+          cur = i;
+          fx = fy = fz = 0;
+          if (KIND == 0) {
+            const int zi = min(max((int)pi.w, 0), prm.nz - 1);
+#pragma unroll
+            for (int z = 0; z < 4; ++z) arow[z] = z < prm.nz ? prm.A[zi * prm.nz + z] : 0.0;
+          }
+        }
+        ++np;
+        double en, coef;
+        if (KIND == 0) {
+          const int zj = (int)pj.w;
+          const double a = zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3];
+          const double q = 1.0 - r2 * prm.invc2;
+          const double aq2 = a * q * q;
+          en = aq2 * q;
+          coef = -6.0 * aq2 * prm.invc2;
+        } else {
+          const double ir2 = __drcp_rn(r2);
+          const double s2 = prm.sigma2 * ir2;
+          const double s6 = s2 * s2 * s2;
+          en = prm.eps4 * (s6 * s6 - s6) - prm.shift;
+          coef = prm.eps24 * (s6 - 2.0 * s6 * s6) * ir2;
+        }
+        const double gx = coef * d[0], gy = coef * d[1], gz = coef * d[2];
+        fx += gx; fy += gy; fz += gz;
+        acc_e += en;
+        w[0] += d[0] * gx; w[1] += d[1] * gy; w[2] += d[2] * gz;
+        w[3] += d[0] * gy; w[4] += d[0] * gz; w[5] += d[1] * gz;
+      });
+  if (cur >= 0 && want_f) {
+    const int o = perm[cur];
+    F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
+  }
+  write_cell_parts(cellpart, cell, lane, acc_e, w, np, npairs);
+}
+
+// Mixed form: candidate test and pair arithmetic in FP32 on coordinates
+// relative to the home cell's first atom, the FP64 wrap/image shift applied
+// before the conversion; energy and virial per neighbour chunk folded into
+// Kahan-compensated FP64 accumulators.
 template <int KIND>
 __global__ void __launch_bounds__(PAIR_WARPS * 32)
     k_pair32(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
              const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
              double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
-  __shared__ float4 stage[PAIR_WARPS][STAGE];
+  __shared__ float4 stage[PAIR_WARPS][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * PAIR_WARPS + warp;
   if (cell >= ncells) return;
   const SysGeom& g = sysv[cell_sys[cell]];
   const int b = cell_start[cell], e = cell_start[cell + 1];
-  if (b == e) {
-    if (lane < 8) cellpart[8 * (size_t)cell + lane] = 0.0;
-    return;
-  }
-  const int local = cell - g.cell_begin;
-  const int key[3] = {local / (g.dims[1] * g.dims[2]), (local / g.dims[2]) % g.dims[1], local % g.dims[2]};
-  const int cnt0 = stencil_count(g, 0), cnt1 = stencil_count(g, 1), cnt2 = stencil_count(g, 2);
-  const double4 ref = pos[b];
-  const float c2 = (float)g.c2;
-  const float invc2 = (float)prm.invc2, eps4 = (float)prm.eps4, eps24 = (float)prm.eps24,
-              sigma2 = (float)prm.sigma2, shift = (float)prm.shift;
   Kahan ke, kw[6];
   unsigned long long np = 0;
-  for (int i0 = b; i0 < e; i0 += 32) {
-    const int i = i0 + lane;
-    const bool have = i < e;
-    const double4 pd = have ? pos[i] : ref;
-    const float xi = (float)(pd.x - ref.x), yi = (float)(pd.y - ref.y), zi_ = (float)(pd.z - ref.z);
-    float arow[4] = {0, 0, 0, 0};
-    if (KIND == 0) {
-      const int zi = min(max((int)pd.w, 0), prm.nz - 1);
+  if (b < e) {
+    const int local = cell - g.cell_begin;
+    const int key[3] = {local / (g.dims[1] * g.dims[2]), (local / g.dims[2]) % g.dims[1], local % g.dims[2]};
+    const int cnt0 = stencil_count(g, 0), cnt1 = stencil_count(g, 1), cnt2 = stencil_count(g, 2);
+    const bool rint_path = g.minimum_image && !g.fast_shift;
+    const double4 ref = pos[b];
+    const float c2 = (float)g.c2;
+    const float invc2 = (float)prm.invc2, eps4 = (float)prm.eps4, eps24 = (float)prm.eps24,
+                sigma2 = (float)prm.sigma2, shift = (float)prm.shift;
+    const float L0 = (float)g.L[0], L1 = (float)g.L[1], L2 = (float)g.L[2];
+    for (int i0 = b; i0 < e; i0 += 32) {
+      const int i = i0 + lane;
+      const bool have = i < e;
+      const double4 pd = have ? pos[i] : ref;
+      const float xi = (float)(pd.x - ref.x), yi = (float)(pd.y - ref.y), zi_ = (float)(pd.z - ref.z);
+      float arow[4] = {0, 0, 0, 0};
+      if (KIND == 0) {
+        const int zi = min(max((int)pd.w, 0), prm.nz - 1);
 #pragma unroll
-      for (int z = 0; z < 4; ++z) arow[z] = z < prm.nz ? (float)prm.A[zi * prm.nz + z] : 0.f;
-    }
-    float fx = 0, fy = 0, fz = 0;
-    for (int t0 = 0; t0 < cnt0; ++t0)
-      for (int t1 = 0; t1 < cnt1; ++t1)
-        for (int t2 = 0; t2 < cnt2; ++t2) {
-          const int off[3] = {stencil_offset(g, 0, t0), stencil_offset(g, 1, t1), stencil_offset(g, 2, t2)};
-          StencilEntry se;
-          stencil_entry(g, key, off, se);
-          if (se.cell < 0) continue;
-          const int jb = cell_start[se.cell], je = cell_start[se.cell + 1];
-          const bool rint_path = g.minimum_image && !g.fast_shift;
-          for (int j0 = jb; j0 < je; j0 += STAGE) {
-            const int nj = min(STAGE, je - j0);
-            __syncwarp();
-            if (lane < nj) {
-              const double4 q = pos[j0 + lane];
-              double dx = q.x - ref.x, dy = q.y - ref.y, dz = q.z - ref.z;
-              if (rint_path) {
-                // minimum image relative to the home cell's reference atom
-                if (g.pbc[0]) dx -= rint(dx / g.L[0]) * g.L[0];
-                if (g.pbc[1]) dy -= rint(dy / g.L[1]) * g.L[1];
-                if (g.pbc[2]) dz -= rint(dz / g.L[2]) * g.L[2];
+        for (int z = 0; z < 4; ++z) arow[z] = z < prm.nz ? (float)prm.A[zi * prm.nz + z] : 0.f;
+      }
+      float fx = 0, fy = 0, fz = 0;
+      for (int t0 = 0; t0 < cnt0; ++t0)
+        for (int t1 = 0; t1 < cnt1; ++t1)
+          for (int t2 = 0; t2 < cnt2; ++t2) {
+            const int off[3] = {stencil_offset(g, 0, t0), stencil_offset(g, 1, t1), stencil_offset(g, 2, t2)};
+            StencilEntry se;
+            stencil_entry(g, key, off, se);
+            if (se.cell < 0) continue;
+            const int jb = cell_start[se.cell], je = cell_start[se.cell + 1];
+            for (int j0 = jb; j0 < je; j0 += 32) {
+              const int nj = min(32, je - j0);
+              __syncwarp();
+              if (lane < nj) {
+                const double4 q = pos[j0 + lane];
+                double dx = q.x - ref.x, dy = q.y - ref.y, dz = q.z - ref.z;
+                if (!rint_path) {
+                  dx += se.sh[0];
+                  dy += se.sh[1];
+                  dz += se.sh[2];
+                }
+                stage[warp][lane] = make_float4((float)dx, (float)dy, (float)dz, (float)q.w);
               } else {
-                dx += se.sh[0];
-                dy += se.sh[1];
-                dz += se.sh[2];
+                stage[warp][lane] = make_float4(1e30f, 1e30f, 1e30f, 0.f);
               }
-              stage[warp][lane] = make_float4((float)dx, (float)dy, (float)dz, (float)q.w);
+              __syncwarp();
+              if (!have) continue;
+              unsigned mask = 0u;
+#pragma unroll
+              for (int t = 0; t < 32; ++t) {
+                const float4 q = stage[warp][t];
+                float d0 = q.x - xi, d1 = q.y - yi, d2 = q.z - zi_;
+                if (rint_path) {
+                  d0 -= rintf(d0 / L0) * L0;
+                  d1 -= rintf(d1 / L1) * L1;
+                  d2 -= rintf(d2 / L2) * L2;
+                }
+                const float r2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2));
+                mask |= (r2 < c2 ? 1u : 0u) << t;
+              }
+              if (se.zero && i >= j0 && i < j0 + 32) mask &= ~(1u << (i - j0));
+              float ex = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
+              while (mask) {
+                const int t = __ffs(mask) - 1;
+                mask &= mask - 1u;
+                const float4 q = stage[warp][t];
+                float d0 = q.x - xi, d1 = q.y - yi, d2 = q.z - zi_;
+                if (rint_path) {
+                  d0 -= rintf(d0 / L0) * L0;
+                  d1 -= rintf(d1 / L1) * L1;
+                  d2 -= rintf(d2 / L2) * L2;
+                }
+                const float r2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2));
+                ++np;
+                float en, coef;
+                if (KIND == 0) {
+                  const int zj = (int)q.w;
+                  const float a = zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3];
+                  const float qq = 1.f - r2 * invc2;
+                  const float aq2 = a * qq * qq;
+                  en = aq2 * qq;
+                  coef = -6.f * aq2 * invc2;
+                } else {
+                  const float ir2 = __frcp_rn(r2);
+                  const float s2 = sigma2 * ir2;
+                  const float s6 = s2 * s2 * s2;
+                  en = eps4 * (s6 * s6 - s6) - shift;
+                  coef = eps24 * (s6 - 2.f * s6 * s6) * ir2;
+                }
+                const float gx = coef * d0, gy = coef * d1, gz = coef * d2;
+                fx += gx; fy += gy; fz += gz;
+                ex += en;
+                v0 += d0 * gx; v1 += d1 * gy; v2 += d2 * gz;
+                v3 += d0 * gy; v4 += d0 * gz; v5 += d1 * gz;
+              }
+              ke.add(ex);
+              kw[0].add(v0); kw[1].add(v1); kw[2].add(v2);
+              kw[3].add(v3); kw[4].add(v4); kw[5].add(v5);
             }
-            __syncwarp();
-            if (!have) continue;
-            float ex = 0, vx0 = 0, vx1 = 0, vx2 = 0, vx3 = 0, vx4 = 0, vx5 = 0;
-            for (int t = 0; t < nj; ++t) {
-              const float4 pj = stage[warp][t];
-              if (se.zero && j0 + t == i) continue;
-              float d0 = pj.x - xi, d1 = pj.y - yi, d2 = pj.z - zi_;
-              if (rint_path) {
-                // the pair itself may still need the wrap (small boxes)
-                if (g.pbc[0]) d0 -= rintf(d0 / (float)g.L[0]) * (float)g.L[0];
-                if (g.pbc[1]) d1 -= rintf(d1 / (float)g.L[1]) * (float)g.L[1];
-                if (g.pbc[2]) d2 -= rintf(d2 / (float)g.L[2]) * (float)g.L[2];
-              }
-              const float r2 = d0 * d0 + d1 * d1 + d2 * d2;
-              if (!(r2 < c2)) continue;
-              ++np;
-              float en, coef;
-              if (KIND == 0) {
-                const int zj = (int)pj.w;
-                const float a = zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3];
-                const float q = 1.f - r2 * invc2;
-                const float aq2 = a * q * q;
-                en = aq2 * q;
-                coef = -6.f * aq2 * invc2;
-              } else {
-                const float ir2 = 1.f / r2;
-                const float s2 = sigma2 * ir2;
-                const float s6 = s2 * s2 * s2;
-                en = eps4 * (s6 * s6 - s6) - shift;
-                coef = eps24 * (s6 - 2.f * s6 * s6) * ir2;
-              }
-              const float gx = coef * d0, gy = coef * d1, gz = coef * d2;
-              fx += gx;
-              fy += gy;
-              fz += gz;
-              ex += en;
-              vx0 += d0 * gx; vx1 += d1 * gy; vx2 += d2 * gz;
-              vx3 += d0 * gy; vx4 += d0 * gz; vx5 += d1 * gz;
-            }
-            ke.add(ex);
-            kw[0].add(vx0); kw[1].add(vx1); kw[2].add(vx2);
-            kw[3].add(vx3); kw[4].add(vx4); kw[5].add(vx5);
           }
-        }
-    if (have && prm.want_f) {
-      const int o = perm[i];
-      F[3 * o] = fx;
-      F[3 * o + 1] = fy;
-      F[3 * o + 2] = fz;
+      if (have && prm.want_f) {
+        const int o = perm[i];
+        F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
+      }
     }
   }
-  double acc_e = warp_sum(ke.s - ke.c);
   double w[6];
 #pragma unroll
-  for (int k = 0; k < 6; ++k) w[k] = warp_sum(kw[k].s - kw[k].c);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(0xffffffffu, np, o);
-  if (lane == 0) {
-    double* cp = cellpart + 8 * (size_t)cell;
-    cp[0] = 0.5 * acc_e;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) cp[1 + k] = -0.5 * w[k];
-    cp[7] = 0;
-    if (np) atomicAdd(npairs, np);
-  }
+  for (int k = 0; k < 6; ++k) w[k] = kw[k].s - kw[k].c;
+  write_cell_parts(cellpart, cell, lane, ke.s - ke.c, w, np, npairs);
 }
 
 // Deterministic reduction of per-cell partials → E and the 3×3 virial

@@ -18,7 +18,7 @@ template <int MODE>
 __global__ void __launch_bounds__(NB_WARPS * 32)
     k_nb_count(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
                const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, int* __restrict__ count) {
-  __shared__ double4 stage[NB_WARPS][TRAVERSE_STAGE];
+  __shared__ WarpStage stage[NB_WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * NB_WARPS + warp;
   if (cell >= ncells) return;
@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(NB_WARPS * 32)
   // each atom is visited by one lane within one contiguous chunk pass
   int cur_i = -1, cnt = 0;
   warp_traverse_cell<MODE>(g, cell, cell_start, pos, stage[warp], lane,
-                           [&](int i, int, const double4&, const double4&, const StencilEntry&, const double*) {
+                           [&](int i, int, const double4&, const double4&, const StencilEntry&, const double*, double) {
                              if (i != cur_i) {
                                if (cur_i >= 0) count[perm[cur_i]] = cnt;
                                cur_i = i;
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(NB_WARPS * 32)
               const double4* __restrict__ pos, const int* __restrict__ perm, const int* __restrict__ wind, int ncells,
               const int64_t* __restrict__ offsets, int* __restrict__ jout, int* __restrict__ Sout,
               double* __restrict__ Rout) {
-  __shared__ double4 stage[NB_WARPS][TRAVERSE_STAGE];
+  __shared__ WarpStage stage[NB_WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * NB_WARPS + warp;
   if (cell >= ncells) return;
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(NB_WARPS * 32)
   int wi[3] = {0, 0, 0};
   warp_traverse_cell<MODE>(g, cell, cell_start, pos, stage[warp], lane,
                            [&](int i, int j, const double4& pi, const double4& pj, const StencilEntry& se,
-                               const double* d) {
+                               const double* d, double) {
                              const int a = perm[i], bb = perm[j];
                              if (i != cur_i) {
                                cur_i = i;

@@ -34,25 +34,43 @@ def needs_build():
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(verbose=False, force=False, extra=()):
-    if not force and not needs_build():
-        return OUT
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    cmd = [nvcc(), "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-ffp-contract=off",
-           "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "--expt-relaxed-constexpr",
-           "--extended-lambda", "-Xptxas", "-warn-spills", "-o", OUT + ".tmp"]
-    cmd += list(extra)
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        print(" ".join(cmd))
-    r = subprocess.run(cmd, capture_output=True, text=True)
+FLAGS = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off", "-gencode",
+         "arch=compute_100a,code=sm_100a", "-lineinfo", "--expt-relaxed-constexpr", "--extended-lambda",
+         "-Xptxas", "-warn-spills"]
+
+
+def build(verbose=False, force=False, extra=(), out=None):
+    """Compile every source to an object in parallel, then link the shared library."""
+    out = out or OUT
+    if not force and out == OUT and not needs_build():
+        return out
+    objdir = os.path.join(PKG, "lib", "obj")
+    os.makedirs(objdir, exist_ok=True)
+    procs = []
+    for s in SOURCES:
+        obj = os.path.join(objdir, s.replace(".cu", ".o"))
+        cmd = [nvcc(), *FLAGS, *extra, "-c", os.path.join(CSRC, s), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((s, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    objs, failed = [], False
+    for s, obj, p in procs:
+        text = p.communicate()[0]
+        if p.returncode != 0:
+            sys.stderr.write(text)
+            failed = True
+        elif verbose and text.strip():
+            print(text)
+        objs.append(obj)
+    if failed:
+        raise RuntimeError("nvcc failed")
+    link = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", out + ".tmp", *objs]
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed")
-    if verbose and (r.stdout or r.stderr):
-        print(r.stdout + r.stderr)
-    os.replace(OUT + ".tmp", OUT)
-    return OUT
+        raise RuntimeError("nvcc link failed")
+    os.replace(out + ".tmp", out)
+    return out
 
 
 if __name__ == "__main__":
