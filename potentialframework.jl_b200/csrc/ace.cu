@@ -10,12 +10,7 @@
 //                 CSR over sorted centres; edge displacement X_j - X_i + H·S
 //                 from the ORIGINAL coordinates (environments.jl:97-102)
 //   k_edge_rev    index of the reverse edge (j→i, -S) of every edge
-//   k_ace_site    one CTA per site, edges in chunks of 32:
-//                   radial splines and harmonics → A-basis A[a] = Σ_j R[j,n_a]Y[j,m_a]
-//                   products P_k and adjoints dA (division-free, per-density
-//                   term lists), site energy
-//                   T1[j,n] = Σ dA·Y, T2[j,m] = Σ dA·R, then per-edge gradient
-//                   g_j = r̂(Σ_n dR·T1 + Σ Wpair·dQ) + Σ_m ∇Y·T2
+//   k_ace_sites   persistent site kernel (ace_site.cuh)
 //   k_ace_gather  F_k = Σ_{e∈out(k)} g_e - g_{rev(e)}  (reduce_site!,
 //                 NeighbourList/execution.jl:256-273, without a racing scatter)
 //   k_ace_reduce  E and the 3×3 virial from per-site partials
@@ -24,21 +19,19 @@
 #include <vector>
 
 #include "ace_math.cuh"
+#include "ace_site.cuh"
 #include "pfw_internal.h"
 #include "traverse.cuh"
 
 namespace pfw {
 
-constexpr int ACE_THREADS = 128;
-constexpr int ACE_CHUNK = 32;
-
 struct AceDevice {
-  int nz = 0, lmax = 0, nY = 0, nR = 0, nQ = 0, D = 0, P = 0, nB = 0, max_order = 0;
+  int nz = 0, lmax = 0, nY = 0, nR = 0, nQ = 0, D = 0, P = 0, T = 0, nB = 0, max_order = 0;
   double cutoff = 0;
   RadialDev R{}, Q{};
   DevBuf r_len, r_nodes, r_coeff, r_tr, r_pow, r_envk, r_env;
   DevBuf q_len, q_nodes, q_coeff, q_tr, q_pow, q_envk, q_env;
-  DevBuf density, dn_off, dn, dm_off, dm, prod_off, prod_fac, term_off, term, weights, wpair, ref, pair_ok, Fnorm;
+  DevBuf density, dn_off, dn, dm_off, dm, prods, term_off, terms, weights, wpair, ref, pair_ok, Fnorm;
   DevBuf c_rows, c_cols, c_vals;
   int ncoupling = 0;
   // per evaluation
@@ -46,25 +39,6 @@ struct AceDevice {
   int64_t nedges = 0;
   int n = 0;
   bool evaluated = false;
-};
-
-struct AceParams {
-  RadialDev R, Q;
-  int nz, lmax, nY, nR, nQ, D, P;
-  const int2* density;   // [D] (n, m)
-  const int* dn_off;     // [nR+1] densities by radial channel
-  const int2* dn;        //   (a, m)
-  const int* dm_off;     // [nY+1] densities by harmonic
-  const int2* dm;        //   (a, n)
-  const int* prod_off;   // [P+1]
-  const int* prod_fac;   // factors
-  const int* term_off;   // [D+1] occurrences of each density in products
-  const int2* term;      //   (k, position)
-  const double* weights; // [nz][P]
-  const double* wpair;   // [nz][nQ]
-  const double* ref;     // [nz]
-  const int* pair_ok;    // [nz]
-  const double* Fnorm;   // [(L+1)^2]
 };
 
 // ---------------------------------------------------------------------------
@@ -155,244 +129,7 @@ __global__ void k_edge_rev(int n, const int* __restrict__ off, const int* __rest
   }
 }
 
-// ---------------------------------------------------------------------------
-// site kernel
-// ---------------------------------------------------------------------------
-struct SiteSmem {
-  double *A, *dA, *Y, *dY, *R, *dR, *T1, *T2, *eu, *ee, *ede, *edu, *dq, *er, *ed, *red;
-  int *ek0, *epidx;
-  static size_t bytes(int D, int nY, int nR) {
-    size_t d = 2 * (size_t)D + (size_t)ACE_CHUNK * (nY + 3 * nY + 3 * nR + nY) + ACE_CHUNK * (7 + 3) + ACE_THREADS * 10;
-    return d * sizeof(double) + 2 * ACE_CHUNK * sizeof(int);
-  }
-  __device__ void carve(double* base, int D, int nY, int nR) {
-    double* p = base;
-    A = p; p += D;
-    dA = p; p += D;
-    Y = p; p += ACE_CHUNK * nY;
-    dY = p; p += ACE_CHUNK * nY * 3;
-    R = p; p += ACE_CHUNK * nR;
-    dR = p; p += ACE_CHUNK * nR;
-    T1 = p; p += ACE_CHUNK * nR;
-    T2 = p; p += ACE_CHUNK * nY;
-    eu = p; p += ACE_CHUNK;
-    ee = p; p += ACE_CHUNK;
-    ede = p; p += ACE_CHUNK;
-    edu = p; p += ACE_CHUNK;
-    dq = p; p += ACE_CHUNK;
-    er = p; p += ACE_CHUNK;
-    ed = p; p += 3 * ACE_CHUNK + ACE_CHUNK;  // + spare
-    red = p; p += ACE_THREADS * 10;
-    ek0 = reinterpret_cast<int*>(p);
-    epidx = ek0 + ACE_CHUNK;
-  }
-};
 
-template <int L>
-__device__ __forceinline__ int lmax_of(int runtime) {
-  return L >= 0 ? L : runtime;
-}
-
-// Per-edge set-up of one chunk (thread t < nc): geometry, radial interval and
-// envelope, pair term, harmonics (values, and gradients when Grad).
-template <int L, bool Grad>
-__device__ __forceinline__ void chunk_edges(const AceParams& p, SiteSmem& S, const double4* __restrict__ edge_d, int e0,
-                                            int nc, int iz, double& e_acc, int* status) {
-  const int t = threadIdx.x;
-  if (t >= nc) return;
-  const double4 d = edge_d[e0 + t];
-  const int zj = min(max((int)d.w, 0), p.nz - 1);
-  const int pidx = iz * p.nz + zj;
-  const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
-  if (!(r > 0.0)) atomicOr(status, 2);
-  const double rr = r > 0.0 ? r : 1.0;
-  S.er[t] = rr;
-  S.ed[3 * t] = d.x;
-  S.ed[3 * t + 1] = d.y;
-  S.ed[3 * t + 2] = d.z;
-  const EdgeRadial<double> er = edge_radial<double>(p.R, pidx, rr);
-  S.ek0[t] = er.k0;
-  S.epidx[t] = pidx;
-  S.eu[t] = er.u;
-  S.ee[t] = er.e;
-  S.ede[t] = er.de;
-  S.edu[t] = er.du;
-  // pair radials: energy Σ_n Wpair[n]·Q_n, or gradient factor Σ_n Wpair[n]·dQ_n/dr
-  double qe = 0.0, qd = 0.0;
-  if (p.pair_ok[zj] && p.nQ > 0) {
-    const EdgeRadial<double> eq = edge_radial<double>(p.Q, pidx, rr);
-    if (!eq.ok) atomicOr(status, 2);
-    const double* wp = p.wpair + (size_t)iz * p.nQ;
-    for (int n = 0; n < p.nQ; ++n) {
-      double v, dv;
-      channel_ed(channel_coeff(p.Q, pidx, eq.k0, n), eq, v, dv);
-      qe += v * wp[n];
-      qd += wp[n] * dv;
-    }
-  }
-  if (!Grad) e_acc += qe;
-  S.dq[t] = qd;
-  const int nY = p.nY;
-  double* Yt = S.Y + t * nY;
-  double* dYt = S.dY + t * nY * 3;
-  harmonics<double, Grad, L>(p.Fnorm, rr, d.x, d.y, d.z, [&](int idx, const Jet<double, Grad>& j) {
-    Yt[idx] = j.v;
-    if constexpr (Grad) {
-      dYt[3 * idx] = j.gx;
-      dYt[3 * idx + 1] = j.gy;
-      dYt[3 * idx + 2] = j.gz;
-    }
-  });
-}
-
-template <int L>
-__global__ void __launch_bounds__(ACE_THREADS)
-    k_ace_site(AceParams p, int nsites, const int* __restrict__ edge_off, const double4* __restrict__ edge_d,
-               const double4* __restrict__ pos, double* __restrict__ edge_g, double* __restrict__ site_out,
-               int want_grad, int* __restrict__ status) {
-  extern __shared__ double smem_raw[];
-  SiteSmem S;
-  S.carve(smem_raw, p.D, p.nY, p.nR);
-  const int s = blockIdx.x;
-  if (s >= nsites) return;
-  const int tid = threadIdx.x;
-  const int iz = min(max((int)pos[s].w, 0), p.nz - 1);
-  const int eb = edge_off[s], E = edge_off[s + 1] - eb;
-  const int D = p.D, nY = p.nY, nR = p.nR, P = p.P;
-  double e_acc = 0.0;
-  for (int a = tid; a < D; a += ACE_THREADS) S.A[a] = 0.0;
-  // ---- A-basis -------------------------------------------------------
-  for (int c0 = 0; c0 < E; c0 += ACE_CHUNK) {
-    const int nc = min(ACE_CHUNK, E - c0);
-    __syncthreads();
-    chunk_edges<L, false>(p, S, edge_d, eb + c0, nc, iz, e_acc, status);
-    __syncthreads();
-    for (int idx = tid; idx < nc * nR; idx += ACE_THREADS) {
-      const int t = idx / nR, n = idx - t * nR;
-      const double* c = channel_coeff(p.R, S.epidx[t], S.ek0[t], n);
-      const double u = S.eu[t];
-      S.R[t * nR + n] = S.ee[t] * (((c[3] * u + c[2]) * u + c[1]) * u + c[0]);
-    }
-    __syncthreads();
-    for (int a = tid; a < D; a += ACE_THREADS) {
-      const int2 nm = p.density[a];
-      double acc = S.A[a];
-      for (int t = 0; t < nc; ++t) acc += S.R[t * nR + nm.x] * S.Y[t * nY + nm.y];
-      S.A[a] = acc;
-    }
-  }
-  __syncthreads();
-  // ---- products, site energy and adjoints ------------------------------
-  const double* w = p.weights + (size_t)iz * P;
-  for (int k = tid; k < P; k += ACE_THREADS) {
-    double pk = 1.0;
-    for (int f = p.prod_off[k]; f < p.prod_off[k + 1]; ++f) pk *= S.A[p.prod_fac[f]];
-    e_acc += w[k] * pk;
-  }
-  for (int a = tid; a < D; a += ACE_THREADS) {
-    double acc = 0.0;
-    for (int q = p.term_off[a]; q < p.term_off[a + 1]; ++q) {
-      const int2 kt = p.term[q];
-      double v = w[kt.x];
-      const int f0 = p.prod_off[kt.x], f1 = p.prod_off[kt.x + 1];
-      for (int f = f0; f < f1; ++f)
-        if (f - f0 != kt.y) v *= S.A[p.prod_fac[f]];
-      acc += v;
-    }
-    S.dA[a] = acc;
-  }
-  double wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  // ---- pullback ---------------------------------------------------------
-  if (want_grad) {
-    for (int c0 = 0; c0 < E; c0 += ACE_CHUNK) {
-      const int nc = min(ACE_CHUNK, E - c0);
-      __syncthreads();
-      double dummy = 0.0;
-      chunk_edges<L, true>(p, S, edge_d, eb + c0, nc, iz, dummy, status);
-      __syncthreads();
-      for (int idx = tid; idx < nc * nR; idx += ACE_THREADS) {
-        const int t = idx / nR, n = idx - t * nR;
-        EdgeRadial<double> er;
-        er.u = S.eu[t];
-        er.e = S.ee[t];
-        er.de = S.ede[t];
-        er.du = S.edu[t];
-        double v, dv;
-        channel_ed(channel_coeff(p.R, S.epidx[t], S.ek0[t], n), er, v, dv);
-        S.R[t * nR + n] = v;
-        S.dR[t * nR + n] = dv;
-      }
-      __syncthreads();
-      for (int idx = tid; idx < nc * nR; idx += ACE_THREADS) {
-        const int t = idx / nR, n = idx - t * nR;
-        double acc = 0.0;
-        for (int q = p.dn_off[n]; q < p.dn_off[n + 1]; ++q) {
-          const int2 am = p.dn[q];
-          acc += S.dA[am.x] * S.Y[t * nY + am.y];
-        }
-        S.T1[t * nR + n] = acc;
-      }
-      for (int idx = tid; idx < nc * nY; idx += ACE_THREADS) {
-        const int t = idx / nY, m = idx - t * nY;
-        double acc = 0.0;
-        for (int q = p.dm_off[m]; q < p.dm_off[m + 1]; ++q) {
-          const int2 an = p.dm[q];
-          acc += S.dA[an.x] * S.R[t * nR + an.y];
-        }
-        S.T2[t * nY + m] = acc;
-      }
-      __syncthreads();
-      {
-        const int t = tid >> 2, q = tid & 3;  // 4 threads per edge
-        double s1 = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-        if (t < nc) {
-          for (int n = q; n < nR; n += 4) s1 += S.dR[t * nR + n] * S.T1[t * nR + n];
-          for (int m = q; m < nY; m += 4) {
-            const double t2 = S.T2[t * nY + m];
-            gx += S.dY[(t * nY + m) * 3] * t2;
-            gy += S.dY[(t * nY + m) * 3 + 1] * t2;
-            gz += S.dY[(t * nY + m) * 3 + 2] * t2;
-          }
-        }
-#pragma unroll
-        for (int o = 1; o < 4; o <<= 1) {
-          s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-          gx += __shfl_xor_sync(0xffffffffu, gx, o);
-          gy += __shfl_xor_sync(0xffffffffu, gy, o);
-          gz += __shfl_xor_sync(0xffffffffu, gz, o);
-        }
-        if (t < nc && q == 0) {
-          const double r = S.er[t];
-          const double dx = S.ed[3 * t], dy = S.ed[3 * t + 1], dz = S.ed[3 * t + 2];
-          const double radial = (s1 + S.dq[t]) / r;
-          const double g0 = radial * dx + gx, g1 = radial * dy + gy, g2 = radial * dz + gz;
-          double* ge = edge_g + 3 * (size_t)(eb + c0 + t);
-          ge[0] = g0;
-          ge[1] = g1;
-          ge[2] = g2;
-          const double dd[3] = {dx, dy, dz}, gg[3] = {g0, g1, g2};
-#pragma unroll
-          for (int b = 0; b < 3; ++b)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) wv[a + 3 * b] -= dd[a] * gg[b];
-        }
-      }
-    }
-  }
-  // ---- site energy and virial partials -----------------------------------
-  __syncthreads();
-  double* red = S.red;
-  red[tid] = e_acc;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) red[(k + 1) * ACE_THREADS + tid] = wv[k];
-  __syncthreads();
-  for (int st = ACE_THREADS / 2; st > 0; st >>= 1) {
-    if (tid < st)
-      for (int k = 0; k < 10; ++k) red[k * ACE_THREADS + tid] += red[k * ACE_THREADS + tid + st];
-    __syncthreads();
-  }
-  if (tid < 10) site_out[10 * (size_t)s + tid] = red[tid * ACE_THREADS] + (tid == 0 ? p.ref[iz] : 0.0);
-}
 
 // F_k = Σ_{e ∈ out(k)} g_e - g_rev(e), written in original order.
 __global__ void k_ace_gather(int n, const int* __restrict__ off, const int* __restrict__ rev,
@@ -438,6 +175,7 @@ __global__ void k_ace_reduce(int n, const double* __restrict__ site_out, const i
   }
 }
 
+
 // ---------------------------------------------------------------------------
 // host
 // ---------------------------------------------------------------------------
@@ -477,10 +215,10 @@ void ace_free(pfw_ws* ws) {
   AceDevice* a = ws->ace;
   DevBuf* bufs[] = {&a->r_len, &a->r_nodes, &a->r_coeff, &a->r_tr, &a->r_pow, &a->r_envk, &a->r_env,
                     &a->q_len, &a->q_nodes, &a->q_coeff, &a->q_tr, &a->q_pow, &a->q_envk, &a->q_env,
-                    &a->density, &a->dn_off, &a->dn, &a->dm_off, &a->dm, &a->prod_off, &a->prod_fac,
-                    &a->term_off, &a->term, &a->weights, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm,
-                    &a->c_rows, &a->c_cols, &a->c_vals, &a->edge_count, &a->edge_off, &a->edge_j, &a->edge_d,
-                    &a->edge_S, &a->edge_rev, &a->edge_g, &a->site_out, &a->site_E_orig, &a->status};
+                    &a->density, &a->dn_off, &a->dn, &a->dm_off, &a->dm, &a->prods, &a->term_off, &a->terms,
+                    &a->weights, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm, &a->c_rows, &a->c_cols, &a->c_vals,
+                    &a->edge_count, &a->edge_off, &a->edge_j, &a->edge_d, &a->edge_S, &a->edge_rev, &a->edge_g,
+                    &a->site_out, &a->site_E_orig, &a->status};
   for (auto* b : bufs) b->release();
   delete a;
   ws->ace = nullptr;
@@ -491,6 +229,8 @@ void ace_load(pfw_ws* ws, const pfw_ace_tables* t) {
   if (t->lmax < 0 || t->lmax > ACE_LMAX) throw Error(PFW_EINVAL, "ACE lmax must be in 0..6");
   if (t->radial.nchannels < 1) throw Error(PFW_EINVAL, "empty radial basis");
   if (!(std::isfinite(t->cutoff) && t->cutoff > 0)) throw Error(PFW_EINVAL, "invalid ACE cutoff");
+  if (t->ndensity < 1 || t->ndensity > 65534 || t->nproducts < 1 || t->nproducts > 65535)
+    throw Error(PFW_EINVAL, "ACE basis size out of range (density <= 65534, products <= 65535)");
   ace_free(ws);
   AceDevice* a = new AceDevice();
   ws->ace = a;
@@ -510,7 +250,7 @@ void ace_load(pfw_ws* ws, const pfw_ace_tables* t) {
     a->Q = upload_family(t->pair, nz, a->q_len, a->q_nodes, a->q_coeff, a->q_tr, a->q_pow, a->q_envk, a->q_env, st);
   else
     a->Q = a->R;
-  // density tables
+  // density tables, grouped by radial channel and by harmonic
   std::vector<int2> dens(a->D);
   for (int k = 0; k < a->D; ++k) {
     const int n = t->density[2 * k], m = t->density[2 * k + 1];
@@ -537,30 +277,43 @@ void ace_load(pfw_ws* ws, const pfw_ace_tables* t) {
   upload(a->dn, dn.data(), dn.size(), st);
   upload(a->dm_off, dm_off.data(), dm_off.size(), st);
   upload(a->dm, dm.data(), dm.size(), st);
-  // products and per-density occurrence lists
-  std::vector<int> poff(t->product_offsets, t->product_offsets + a->P + 1);
+  // products (≤ 4 factors, sentinel D) and the adjoint terms of each density:
+  // one term per occurrence of a in product k, holding the other factors
+  const int* poff = t->product_offsets;
   if (poff[0] != 0) throw Error(PFW_EINVAL, "product offsets must start at 0");
-  std::vector<int> pfac(t->product_factors, t->product_factors + poff[a->P]);
-  std::vector<int> toff(a->D + 1, 0);
+  const unsigned short SENT = (unsigned short)a->D;
+  std::vector<ushort4> prods(a->P);
+  std::vector<std::vector<ushort4>> per(a->D);
   for (int k = 0; k < a->P; ++k) {
-    if (poff[k + 1] <= poff[k]) throw Error(PFW_EINVAL, "empty ACE product");
-    a->max_order = std::max(a->max_order, poff[k + 1] - poff[k]);
-    for (int f = poff[k]; f < poff[k + 1]; ++f) {
-      if (pfac[f] < 0 || pfac[f] >= a->D) throw Error(PFW_EINVAL, "invalid product indices");
-      toff[pfac[f] + 1]++;
+    const int nu = poff[k + 1] - poff[k];
+    if (nu < 1) throw Error(PFW_EINVAL, "empty ACE product");
+    if (nu > 4) throw Error(PFW_EINVAL, "ACE correlation order above 4 is not supported");
+    a->max_order = std::max(a->max_order, nu);
+    unsigned short f[4] = {SENT, SENT, SENT, SENT};
+    for (int q = 0; q < nu; ++q) {
+      const int v = t->product_factors[poff[k] + q];
+      if (v < 0 || v >= a->D) throw Error(PFW_EINVAL, "invalid product indices");
+      f[q] = (unsigned short)v;
+    }
+    prods[k] = make_ushort4(f[0], f[1], f[2], f[3]);
+    for (int q = 0; q < nu; ++q) {
+      unsigned short o[3] = {SENT, SENT, SENT};
+      int c = 0;
+      for (int u = 0; u < nu; ++u)
+        if (u != q) o[c++] = f[u];
+      per[f[q]].push_back(make_ushort4((unsigned short)k, o[0], o[1], o[2]));
     }
   }
-  for (int k = 0; k < a->D; ++k) toff[k + 1] += toff[k];
-  std::vector<int2> term(toff[a->D]);
-  {
-    std::vector<int> fill(toff.begin(), toff.end() - 1);
-    for (int k = 0; k < a->P; ++k)
-      for (int f = poff[k]; f < poff[k + 1]; ++f) term[fill[pfac[f]]++] = make_int2(k, f - poff[k]);
+  std::vector<int> toff(a->D + 1, 0);
+  std::vector<ushort4> terms;
+  for (int d = 0; d < a->D; ++d) {
+    toff[d + 1] = toff[d] + (int)per[d].size();
+    terms.insert(terms.end(), per[d].begin(), per[d].end());
   }
-  upload(a->prod_off, poff.data(), poff.size(), st);
-  upload(a->prod_fac, pfac.data(), pfac.size(), st);
+  a->T = (int)terms.size();
+  upload(a->prods, prods.data(), prods.size(), st);
   upload(a->term_off, toff.data(), toff.size(), st);
-  upload(a->term, term.data(), term.size(), st);
+  upload(a->terms, terms.data(), terms.size(), st);
   // precontracted weights w[z][k] = Σ_b C[b,k]·WB[z][b] (ACE/cpu.jl:265-268)
   std::vector<double> wts((size_t)nz * a->P, 0.0);
   for (int z = 0; z < nz; ++z)
@@ -591,26 +344,25 @@ void ace_load(pfw_ws* ws, const pfw_ace_tables* t) {
   PFW_CUDA(cudaStreamSynchronize(st));
 }
 
-static AceParams params_of(AceDevice* a) {
-  AceParams p;
+static AceTables tables_of(AceDevice* a) {
+  AceTables p;
   p.R = a->R;
   p.Q = a->Q;
   p.nz = a->nz;
-  p.lmax = a->lmax;
   p.nY = a->nY;
   p.nR = a->nR;
   p.nQ = a->nQ;
   p.D = a->D;
   p.P = a->P;
+  p.T = a->T;
+  p.prods = a->prods.as<ushort4>();
+  p.term_off = a->term_off.as<int>();
+  p.terms = a->terms.as<ushort4>();
   p.density = a->density.as<int2>();
   p.dn_off = a->dn_off.as<int>();
   p.dn = a->dn.as<int2>();
   p.dm_off = a->dm_off.as<int>();
   p.dm = a->dm.as<int2>();
-  p.prod_off = a->prod_off.as<int>();
-  p.prod_fac = a->prod_fac.as<int>();
-  p.term_off = a->term_off.as<int>();
-  p.term = a->term.as<int2>();
   p.weights = a->weights.as<double>();
   p.wpair = a->wpair.as<double>();
   p.ref = a->ref.as<double>();
@@ -619,11 +371,32 @@ static AceParams params_of(AceDevice* a) {
   return p;
 }
 
-template <int L>
-static void launch_site(const AceParams& p, int n, size_t smem, cudaStream_t st, const int* off, const double4* ed,
-                        const double4* pos, double* g, double* out, int want_grad, int* status) {
-  PFW_CUDA(cudaFuncSetAttribute(k_ace_site<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_ace_site<L><<<n, ACE_THREADS, smem, st>>>(p, n, off, ed, pos, g, out, want_grad, status);
+// Largest working set that fits: two 128-thread groups with 32-edge chunks
+// when possible, else smaller chunks / one group.
+static AceLayout choose_layout(const AceTables& p, int device) {
+  int optin = 0;
+  PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  const size_t limit = (size_t)optin;
+  const int cand[][2] = {{32, 2}, {16, 2}, {32, 1}, {16, 1}, {8, 1}};
+  for (auto& c : cand) {
+    AceLayout lay;
+    lay.make(p, c[0], c[1]);
+    if (lay.total <= limit) return lay;
+  }
+  throw Error(PFW_EINVAL, "ACE model too large for the site kernel's shared memory");
+}
+
+template <int L, class T>
+static void launch_sites(const AceTables& p, const AceLayout& lay, int n, cudaStream_t st, int device, const int* off,
+                         const double4* ed, const double4* pos, double* g, double* out, int want_grad, int* status) {
+  auto kern = k_ace_sites<L, T>;
+  PFW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total));
+  int sms = 0, per_sm = 0;
+  PFW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  PFW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ACE_GROUP * lay.G, lay.total));
+  per_sm = std::max(per_sm, 1);
+  const int blocks = std::max(1, std::min(sms * per_sm, (n + lay.G - 1) / lay.G));
+  kern<<<blocks, ACE_GROUP * lay.G, lay.total, st>>>(p, lay, n, off, ed, pos, g, out, want_grad, status);
 }
 
 // Build the directed environments of the current geometry (sorted centres).
@@ -669,6 +442,21 @@ static void build_edges(pfw_ws* ws, AceDevice* a) {
   }
 }
 
+template <class T>
+static void dispatch_sites(int lmax, const AceTables& p, const AceLayout& lay, int n, cudaStream_t st, int device,
+                           const int* off, const double4* ed, const double4* pos, double* g, double* out,
+                           int want_grad, int* status) {
+  switch (lmax) {
+    case 0: launch_sites<0, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
+    case 1: launch_sites<1, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
+    case 2: launch_sites<2, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
+    case 3: launch_sites<3, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
+    case 4: launch_sites<4, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
+    case 5: launch_sites<5, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
+    default: launch_sites<6, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
+  }
+}
+
 void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev) {
   AceDevice* a = ws->ace;
   if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
@@ -689,23 +477,17 @@ void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   double* g = static_cast<double*>(a->edge_g.ensure(sizeof(double) * 3 * std::max<int64_t>(a->nedges, 1)));
   double* out = static_cast<double*>(a->site_out.ensure(sizeof(double) * 10 * std::max(n, 1)));
   double* Esite = static_cast<double*>(a->site_E_orig.ensure(sizeof(double) * std::max(n, 1)));
-  const AceParams p = params_of(a);
-  const size_t smem = SiteSmem::bytes(a->D, a->nY, a->nR);
-  if (smem > 200 * 1024) throw Error(PFW_EINVAL, "ACE model too large for the site kernel's shared memory");
+  const AceTables p = tables_of(a);
+  const AceLayout lay = choose_layout(p, ws->opt.device);
   ws->stage_begin(1);
   if (n > 0) {
     const int* off = a->edge_off.as<int>();
     const double4* ed = a->edge_d.as<double4>();
     const double4* pos = ws->pos.as<double4>();
-    switch (a->lmax) {
-      case 0: launch_site<0>(p, n, smem, st, off, ed, pos, g, out, want_grad, status); break;
-      case 1: launch_site<1>(p, n, smem, st, off, ed, pos, g, out, want_grad, status); break;
-      case 2: launch_site<2>(p, n, smem, st, off, ed, pos, g, out, want_grad, status); break;
-      case 3: launch_site<3>(p, n, smem, st, off, ed, pos, g, out, want_grad, status); break;
-      case 4: launch_site<4>(p, n, smem, st, off, ed, pos, g, out, want_grad, status); break;
-      case 5: launch_site<5>(p, n, smem, st, off, ed, pos, g, out, want_grad, status); break;
-      default: launch_site<6>(p, n, smem, st, off, ed, pos, g, out, want_grad, status); break;
-    }
+    if (ws->opt.precision == PFW_PRECISION_MIXED)
+      dispatch_sites<float>(a->lmax, p, lay, n, st, ws->opt.device, off, ed, pos, g, out, want_grad, status);
+    else
+      dispatch_sites<double>(a->lmax, p, lay, n, st, ws->opt.device, off, ed, pos, g, out, want_grad, status);
     ws->launches += 1;
   }
   ws->stage_end(1);

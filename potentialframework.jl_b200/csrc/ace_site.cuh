@@ -1,0 +1,335 @@
+// ace_site.cuh — the persistent ACE site kernel.
+//
+// One CTA per SM slot holds the model's product, adjoint-term and density
+// tables and the precontracted weights in shared memory (loaded once), and
+// runs G groups of 128 threads; each group evaluates one site at a time
+// (sites strided over the grid), with its own A/dA vectors and an edge-chunk
+// working set of CH edges:
+//
+//   pass 1 (per chunk)  radial spline values R[t,n], harmonics Y[t,m], pair
+//                       energy; A[a] += Σ_t R[t,n_a]·Y[t,m_a]
+//   products            P_k = Π A (≤ 4 factors, missing factors point at the
+//                       sentinel A[D] = 1), E_i = ref + Σ w_k P_k + pair;
+//                       dA[a] = Σ_{terms of a} w_k Π(other factors)
+//   pass 2 (per chunk)  R, dR/dr, Y, ∇Y; T1[t,n] = Σ dA·Y, T2[t,m] = Σ dA·R;
+//                       g_t = r̂ (Σ_n dR·T1 + Σ Wpair·dQ) + Σ_m ∇Y·T2
+//
+// Arithmetic type T is double for the plain path and float for the mixed
+// form (energies and the virial are accumulated in double either way).
+#pragma once
+#include "ace_math.cuh"
+
+namespace pfw {
+
+constexpr int ACE_GROUP = 128;
+
+struct AceTables {
+  RadialDev R, Q;
+  int nz, nY, nR, nQ, D, P, T;    // T: number of adjoint terms
+  const ushort4* prods;           // [P] factor indices, D = sentinel
+  const int* term_off;            // [D+1]
+  const ushort4* terms;           // [T] (k, other factors)
+  const int2* density;            // [D] (n, m)
+  const int* dn_off;              // [nR+1]
+  const int2* dn;                 // [D] (a, m)
+  const int* dm_off;              // [nY+1]
+  const int2* dm;                 // [D] (a, n)
+  const double* weights;          // [nz][P]
+  const double* wpair;            // [nz][nQ]
+  const double* ref;              // [nz]
+  const int* pair_ok;             // [nz]
+  const double* Fnorm;            // [(L+1)^2]
+};
+
+// shared-memory layout (byte offsets), computed identically on host and device
+struct AceLayout {
+  int CH, G;
+  size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, weights, tables_end;
+  size_t group_bytes, total;
+  // group-relative double offsets
+  int A, dA, Y, dY, R, dR, T1, T2, esc, ints;
+  __host__ __device__ static size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
+  __host__ __device__ void make(const AceTables& t, int ch, int g) {
+    CH = ch;
+    G = g;
+    size_t o = 0;
+    prods = o; o = align16(o + sizeof(ushort4) * t.P);
+    terms = o; o = align16(o + sizeof(ushort4) * t.T);
+    term_off = o; o = align16(o + sizeof(int) * (t.D + 1));
+    density = o; o = align16(o + sizeof(int2) * t.D);
+    dn_off = o; o = align16(o + sizeof(int) * (t.nR + 1));
+    dn = o; o = align16(o + sizeof(int2) * t.D);
+    dm_off = o; o = align16(o + sizeof(int) * (t.nY + 1));
+    dm = o; o = align16(o + sizeof(int2) * t.D);
+    weights = o; o = align16(o + sizeof(double) * t.nz * t.P);
+    tables_end = o;
+    int d = 0;
+    A = d; d += t.D + 1;
+    dA = d; d += t.D + 1;
+    Y = d; d += CH * t.nY;
+    dY = d; d += CH * t.nY * 3;
+    R = d; d += CH * t.nR;
+    dR = d; d += CH * t.nR;
+    T1 = d; d += CH * t.nR;
+    T2 = d; d += CH * t.nY;
+    esc = d; d += CH * 10 + 4 * 10;  // per-edge scalars, then warp partials
+    ints = d; d += CH;               // 2 ints per edge
+    group_bytes = align16(sizeof(double) * d);
+    total = tables_end + group_bytes * G;
+  }
+};
+
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(ACE_GROUP) : "memory");
+}
+
+template <class T>
+struct EdgeScalars {
+  // per-edge values of the current chunk (index t): u, e, de, du, dq, r, dx, dy, dz
+  double *u, *e, *de, *du, *dq, *r, *dx, *dy, *dz, *wred;
+  int *k0, *pidx;
+};
+
+template <int L, class T, bool Grad>
+__device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbase, const AceLayout& lay,
+                                                const EdgeScalars<T>& es, const double4* __restrict__ edge_d, int e0,
+                                                int nc, int iz, int lt, double& e_acc, int* status) {
+  if (lt >= nc) return;
+  const double4 d = edge_d[e0 + lt];
+  const int zj = min(max((int)d.w, 0), p.nz - 1);
+  const int pidx = iz * p.nz + zj;
+  const T dx = (T)d.x, dy = (T)d.y, dz = (T)d.z;
+  const T r0 = sqrt(dx * dx + dy * dy + dz * dz);
+  if (!(r0 > T(0))) atomicOr(status, 2);
+  const T r = r0 > T(0) ? r0 : T(1);
+  es.r[lt] = r;
+  es.dx[lt] = dx;
+  es.dy[lt] = dy;
+  es.dz[lt] = dz;
+  const EdgeRadial<T> er = edge_radial<T>(p.R, pidx, r);
+  es.k0[lt] = er.k0;
+  es.pidx[lt] = pidx;
+  es.u[lt] = er.u;
+  es.e[lt] = er.e;
+  es.de[lt] = er.de;
+  es.du[lt] = er.du;
+  double qe = 0.0;
+  T qd = T(0);
+  if (p.nQ > 0 && p.pair_ok[zj]) {
+    const EdgeRadial<T> eq = edge_radial<T>(p.Q, pidx, r);
+    if (!eq.ok) atomicOr(status, 2);
+    const double* wp = p.wpair + (size_t)iz * p.nQ;
+    for (int n = 0; n < p.nQ; ++n) {
+      T v, dv;
+      channel_ed<T>(channel_coeff(p.Q, pidx, eq.k0, n), eq, v, dv);
+      qe += (double)v * wp[n];
+      qd += (T)wp[n] * dv;
+    }
+  }
+  if (!Grad) e_acc += qe;
+  es.dq[lt] = qd;
+  double* Yt = gbase + lay.Y + lt * p.nY;
+  double* dYt = gbase + lay.dY + lt * p.nY * 3;
+  harmonics<T, Grad, L>(p.Fnorm, r, dx, dy, dz, [&](int idx, const Jet<T, Grad>& j) {
+    Yt[idx] = j.v;
+    if constexpr (Grad) {
+      dYt[3 * idx] = j.gx;
+      dYt[3 * idx + 1] = j.gy;
+      dYt[3 * idx + 2] = j.gz;
+    }
+  });
+}
+
+template <int L, class T>
+__global__ void __launch_bounds__(2 * ACE_GROUP)
+    k_ace_sites(AceTables p, AceLayout lay, int nsites, const int* __restrict__ edge_off,
+                const double4* __restrict__ edge_d, const double4* __restrict__ pos, double* __restrict__ edge_g,
+                double* __restrict__ site_out, int want_grad, int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  // ---- stage the model tables once per CTA ----
+  ushort4* s_prods = reinterpret_cast<ushort4*>(smem + lay.prods);
+  ushort4* s_terms = reinterpret_cast<ushort4*>(smem + lay.terms);
+  int* s_toff = reinterpret_cast<int*>(smem + lay.term_off);
+  int2* s_dens = reinterpret_cast<int2*>(smem + lay.density);
+  int* s_dnoff = reinterpret_cast<int*>(smem + lay.dn_off);
+  int2* s_dn = reinterpret_cast<int2*>(smem + lay.dn);
+  int* s_dmoff = reinterpret_cast<int*>(smem + lay.dm_off);
+  int2* s_dm = reinterpret_cast<int2*>(smem + lay.dm);
+  double* s_w = reinterpret_cast<double*>(smem + lay.weights);
+  for (int k = threadIdx.x; k < p.P; k += blockDim.x) s_prods[k] = p.prods[k];
+  for (int k = threadIdx.x; k < p.T; k += blockDim.x) s_terms[k] = p.terms[k];
+  for (int k = threadIdx.x; k <= p.D; k += blockDim.x) s_toff[k] = p.term_off[k];
+  for (int k = threadIdx.x; k < p.D; k += blockDim.x) {
+    s_dens[k] = p.density[k];
+    s_dn[k] = p.dn[k];
+    s_dm[k] = p.dm[k];
+  }
+  for (int k = threadIdx.x; k <= p.nR; k += blockDim.x) s_dnoff[k] = p.dn_off[k];
+  for (int k = threadIdx.x; k <= p.nY; k += blockDim.x) s_dmoff[k] = p.dm_off[k];
+  for (int k = threadIdx.x; k < p.nz * p.P; k += blockDim.x) s_w[k] = p.weights[k];
+  __syncthreads();
+
+  const int g = threadIdx.x / ACE_GROUP, lt = threadIdx.x % ACE_GROUP;
+  if (g >= lay.G) return;
+  double* gb = reinterpret_cast<double*>(smem + lay.tables_end + lay.group_bytes * g);
+  double* A = gb + lay.A;
+  double* dA = gb + lay.dA;
+  double* Yc = gb + lay.Y;
+  double* dYc = gb + lay.dY;
+  double* Rc = gb + lay.R;
+  double* dRc = gb + lay.dR;
+  double* T1 = gb + lay.T1;
+  double* T2 = gb + lay.T2;
+  EdgeScalars<T> es;
+  const int CH = lay.CH;
+  double* e0p = gb + lay.esc;
+  es.u = e0p; es.e = e0p + CH; es.de = e0p + 2 * CH; es.du = e0p + 3 * CH; es.dq = e0p + 4 * CH;
+  es.r = e0p + 5 * CH; es.dx = e0p + 6 * CH; es.dy = e0p + 7 * CH; es.dz = e0p + 8 * CH;
+  es.wred = e0p + 10 * CH;
+  es.k0 = reinterpret_cast<int*>(gb + lay.ints);
+  es.pidx = es.k0 + CH;
+  const int D = p.D, nY = p.nY, nR = p.nR, P = p.P;
+  const int lane = lt & 31, wg = lt >> 5;
+
+  for (int s = blockIdx.x * lay.G + g; s < nsites; s += gridDim.x * lay.G) {
+    const int iz = min(max((int)pos[s].w, 0), p.nz - 1);
+    const int eb = edge_off[s], E = edge_off[s + 1] - eb;
+    double e_acc = 0.0;
+    group_sync(g);
+    for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? 1.0 : 0.0;
+    // ---- pass 1: A-basis ----
+    for (int c0 = 0; c0 < E; c0 += CH) {
+      const int nc = min(CH, E - c0);
+      group_sync(g);
+      ace_chunk_edges<L, T, false>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, e_acc, status);
+      group_sync(g);
+      for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
+        const int t = idx / nR, n = idx - t * nR;
+        const double* c = channel_coeff(p.R, es.pidx[t], es.k0[t], n);
+        const T u = (T)es.u[t];
+        Rc[t * nR + n] = (T)es.e[t] * ((((T)c[3] * u + (T)c[2]) * u + (T)c[1]) * u + (T)c[0]);
+      }
+      group_sync(g);
+      for (int a = lt; a < D; a += ACE_GROUP) {
+        const int2 nm = s_dens[a];
+        T acc = (T)A[a];
+        for (int t = 0; t < nc; ++t) acc += (T)Rc[t * nR + nm.x] * (T)Yc[t * nY + nm.y];
+        A[a] = acc;
+      }
+    }
+    group_sync(g);
+    // ---- products, energy, adjoints ----
+    const double* w = s_w + (size_t)iz * P;
+    for (int k = lt; k < P; k += ACE_GROUP) {
+      const ushort4 f = s_prods[k];
+      e_acc += w[k] * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
+    }
+    if (want_grad)
+      for (int a = lt; a < D; a += ACE_GROUP) {
+        T acc = T(0);
+        for (int q = s_toff[a]; q < s_toff[a + 1]; ++q) {
+          const ushort4 tm = s_terms[q];
+          acc += (T)w[tm.x] * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
+        }
+        dA[a] = acc;
+      }
+    double wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // ---- pass 2: pullback ----
+    if (want_grad) {
+      for (int c0 = 0; c0 < E; c0 += CH) {
+        const int nc = min(CH, E - c0);
+        group_sync(g);
+        double dummy = 0.0;
+        ace_chunk_edges<L, T, true>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, dummy, status);
+        group_sync(g);
+        for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
+          const int t = idx / nR, n = idx - t * nR;
+          EdgeRadial<T> er;
+          er.u = (T)es.u[t];
+          er.e = (T)es.e[t];
+          er.de = (T)es.de[t];
+          er.du = (T)es.du[t];
+          T v, dv;
+          channel_ed<T>(channel_coeff(p.R, es.pidx[t], es.k0[t], n), er, v, dv);
+          Rc[t * nR + n] = v;
+          dRc[t * nR + n] = dv;
+        }
+        group_sync(g);
+        for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
+          const int t = idx / nR, n = idx - t * nR;
+          T acc = T(0);
+          for (int q = s_dnoff[n]; q < s_dnoff[n + 1]; ++q) {
+            const int2 am = s_dn[q];
+            acc += (T)dA[am.x] * (T)Yc[t * nY + am.y];
+          }
+          T1[t * nR + n] = acc;
+        }
+        for (int idx = lt; idx < nc * nY; idx += ACE_GROUP) {
+          const int t = idx / nY, m = idx - t * nY;
+          T acc = T(0);
+          for (int q = s_dmoff[m]; q < s_dmoff[m + 1]; ++q) {
+            const int2 an = s_dm[q];
+            acc += (T)dA[an.x] * (T)Rc[t * nR + an.y];
+          }
+          T2[t * nY + m] = acc;
+        }
+        group_sync(g);
+        // 4 threads per edge (CH <= 32)
+        const int t = lt >> 2, q4 = lt & 3;
+        T s1 = T(0), gx = T(0), gy = T(0), gz = T(0);
+        if (t < nc) {
+          for (int n = q4; n < nR; n += 4) s1 += (T)dRc[t * nR + n] * (T)T1[t * nR + n];
+          for (int m = q4; m < nY; m += 4) {
+            const T t2 = (T)T2[t * nY + m];
+            gx += (T)dYc[(t * nY + m) * 3] * t2;
+            gy += (T)dYc[(t * nY + m) * 3 + 1] * t2;
+            gz += (T)dYc[(t * nY + m) * 3 + 2] * t2;
+          }
+        }
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+          s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+          gx += __shfl_xor_sync(0xffffffffu, gx, o);
+          gy += __shfl_xor_sync(0xffffffffu, gy, o);
+          gz += __shfl_xor_sync(0xffffffffu, gz, o);
+        }
+        if (t < nc && q4 == 0) {
+          const T r = (T)es.r[t];
+          const T dx = (T)es.dx[t], dy = (T)es.dy[t], dz = (T)es.dz[t];
+          const T radial = (s1 + (T)es.dq[t]) / r;
+          const double g0 = (double)(radial * dx + gx), g1 = (double)(radial * dy + gy), g2 = (double)(radial * dz + gz);
+          double* ge = edge_g + 3 * (size_t)(eb + c0 + t);
+          ge[0] = g0;
+          ge[1] = g1;
+          ge[2] = g2;
+          const double dd[3] = {(double)dx, (double)dy, (double)dz}, gg[3] = {g0, g1, g2};
+#pragma unroll
+          for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) wv[a + 3 * b] -= dd[a] * gg[b];
+        }
+      }
+    }
+    // ---- site energy and virial (warp shuffles, then 4 warp partials) ----
+    double vals[10];
+    vals[0] = e_acc;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) vals[k + 1] = wv[k];
+#pragma unroll
+    for (int k = 0; k < 10; ++k)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) vals[k] += __shfl_xor_sync(0xffffffffu, vals[k], o);
+    group_sync(g);
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < 10; ++k) es.wred[wg * 10 + k] = vals[k];
+    group_sync(g);
+    if (lt < 10) {
+      double v = es.wred[lt] + es.wred[10 + lt] + es.wred[20 + lt] + es.wred[30 + lt];
+      if (lt == 0) v += p.ref[iz];
+      site_out[10 * (size_t)s + lt] = v;
+    }
+  }
+}
+
+}  // namespace pfw

@@ -106,3 +106,13 @@ def test_rotation_invariance_gpu(b2model):
     E2, F2, W2 = gpu_ace(h, b2model, s.X @ Rm.T, Rm @ s.H, s.pbc, s.species)
     assert abs(E - E2) <= 1e-10 * abs(E)
     assert np.abs(F2 - F @ Rm.T).max() <= 1e-9
+
+
+def test_mixed_precision_form(b2model):
+    # FP32 site arithmetic, FP64 energy/virial accumulation: stated force RMSE ≤ 1e-3 eV/Å
+    s = WL.b2(nc=8, seed=2)
+    E64, F64, W64 = gpu_ace(lib.Handle(lib.FP64), b2model, s.X, s.H, s.pbc, s.species)
+    E32, F32, W32 = gpu_ace(lib.Handle(lib.MIXED), b2model, s.X, s.H, s.pbc, s.species)
+    rmse = float(np.sqrt(np.mean((F32 - F64) ** 2)))
+    assert rmse <= 1e-3, rmse
+    assert abs(E32 - E64) <= 1e-5 * abs(E64)
