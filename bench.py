@@ -1,23 +1,29 @@
 #!/usr/bin/env python
 """Benchmark of the B200 force-evaluation hot path (one JSON line on rank 0).
 
-Headline workload: Lennard-Jones FCC 40³ (256,000 atoms, a=5.26 Å, σ_disp
-0.1 Å, ε=0.0104 eV, σ=3.4 Å, c=8.5 Å, periodic), plain FP64 E+F+virial.  A
-step is one evaluate! call: the full cell-list rebuild plus the pair kernel
-and the reductions, on synthetic seeded input.
+Headline workload (default): Lennard-Jones FCC 40³ — 256,000 atoms,
+a = 5.26 Å, σ_disp = 0.1 Å, ε = 0.0104 eV, σ = 3.4 Å, c = 8.5 Å, periodic —
+plain FP64 energy + forces + virial.  A step is one evaluate! call: the full
+cell-list rebuild, the pair kernel and the reductions, on seeded synthetic
+input.
 
   value  atoms/s with positions resident in HBM (pfw_set_geometry_device +
-         pfw_evaluate_device per step), per-step CUDA events on the
-         library's launch stream; L2 flushed between steps outside the events
+         pfw_evaluate_device per step), per-step CUDA events on the stream
+         the library launches on; L2 flushed between steps outside the events
   e2e    the same through the reference-facing C ABI with HOST buffers
          (pinned X in, E/F/W out, copies inside the timed region)
+  forms  the other configurations and arithmetic forms, each with atoms/s
+         and, for reduced precision, its error against plain FP64
 
---impl reference times the reference's CPU algorithm (restated in oracle/,
-the reference being a Julia package that cannot run on this machine) with
-all host threads on the same workload.  Under torchrun each GPU evaluates
-its own replica (weak scaling; the single-box path is replicas only).
+--workload selects another configuration as the headline (used to profile
+its kernel).  --impl reference times the reference's CPU algorithm, restated
+in oracle/ because the reference is a Julia package that cannot run on this
+machine, with all host threads on the same workload.  Under torchrun every
+GPU evaluates its own replica (weak scaling; the single-box paths are
+replicas only).
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -36,27 +42,72 @@ METRIC = "atoms/s E+F+virial, plain vs mixed/batched/surrogate at stated force R
 FALLBACK_HBM = 6650.0
 
 
-def parse():
-    p = argparse.ArgumentParser()
-    p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
-    p.add_argument("--warmup", type=int, default=5)
-    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--no-forms", action="store_true")
-    return p.parse_args()
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+class Workload:
+    """One configuration: system, model binding, kernel and algorithmic work."""
 
+    def __init__(self, name):
+        from pfw_b200 import workloads as WL
+        self.name = name
+        self.model_sel = 0
+        self.kind = "pair"
+        if name in ("lj", "lj1m", "lj_shear"):
+            nc = 64 if name == "lj1m" else 40
+            self.sys = WL.lj_fcc(seed=2 if nc == 40 else 3, nc=nc, shear=0.2 if name == "lj_shear" else 0.0)
+            self.params = dict(potential="lennard_jones", epsilon=WL.LJ_EPS, sigma=WL.LJ_SIGMA, cutoff=WL.LJ_CUTOFF)
+            self.pair = ("lj", (WL.LJ_EPS, WL.LJ_SIGMA), WL.LJ_CUTOFF)
+            self.flop_per_pair = 65.0
+            self.kernel = "k_pair64<LJ>"
+            self.config = dict(workload=f"lj_fcc{nc}_{len(self.sys)}" + ("_shear0.2" if name == "lj_shear" else ""),
+                               lattice_a=5.26, displacement_sigma=0.1, **self.params)
+        elif name == "smooth":
+            self.sys = WL.smooth_fcc(seed=1)
+            self.pair = ("smooth", WL.SMOOTH_A, WL.SMOOTH_CUTOFF)
+            self.flop_per_pair = 52.0
+            self.kernel = "k_pair64<SmoothPair>"
+            self.config = dict(workload="smooth_fcc8_2048", potential="SmoothPair", amplitudes=WL.SMOOTH_A.tolist(),
+                               cutoff=WL.SMOOTH_CUTOFF, lattice_a=1.6, displacement_sigma=0.05)
+        elif name in ("ace", "ace_tial"):
+            from pfw_b200 import ace_generate as G
+            from pfw_b200.ace_model import PackedACE, read_resolved
+            self.kind = "ace"
+            self.model_sel = 1
+            self.sys = WL.b2(seed=4, nc=20)
+            if name == "ace":
+                self.ace = read_resolved(G.generate_b2_model())
+                label = "synthetic resolved ACE: 40 radials (n<=8, l<=4), lmax 4, order 3, degree 12"
+            else:
+                d = np.load(os.path.join(ROOT, "tests", "golden", "tial_ace.npz"))
+                self.ace = PackedACE.from_npz_dict(d, "model_")
+                label = "reference TiAl resolved model (lmax 2, 167 products) on the B2 box"
+            self.kernel = "k_ace_sites"
+            self.config = dict(workload=f"ace_b2_20_{len(self.sys)}" + ("_tial" if name == "ace_tial" else ""),
+                               model=label, cutoff=self.ace.cutoff, lattice_a=2.9, displacement_sigma=0.08,
+                               densities=self.ace.ndensity, products=self.ace.nproducts, invariants=self.ace.nbasis)
+        else:
+            raise SystemExit(f"unknown workload {name}")
+        self.n = len(self.sys)
 
-def env_rank():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+    def bind(self, h):
+        if self.kind == "pair":
+            kind, params, c = self.pair
+            if kind == "lj":
+                h.lj(params[0], params[1], c)
+            else:
+                h.smooth(params, c)
+        else:
+            h.ace(self.ace)
 
-
-def workload():
-    from pfw_b200 import workloads as WL
-    s = WL.lj_fcc(seed=2, nc=40)
-    return s, dict(workload="lj_fcc40_256000", atoms=len(s), potential="lennard_jones",
-                   epsilon=WL.LJ_EPS, sigma=WL.LJ_SIGMA, cutoff=WL.LJ_CUTOFF, lattice_a=5.26,
-                   displacement_sigma=0.1, box=list(np.diag(s.H)), periodic=True)
+    def cpu_call(self, nthreads):
+        from oracle import oracle as O
+        s = self.sys
+        if self.kind == "pair":
+            kind, params, c = self.pair
+            return lambda: O.pair_evaluate(s.X, s.H, s.pbc, s.species, kind, params, c, nthreads=nthreads)
+        ace = O.AceOracle(self.ace)
+        return lambda: ace.evaluate(s.X, s.H, s.pbc, s.species, nthreads=nthreads)
 
 
 def measured_peaks():
@@ -68,7 +119,7 @@ def measured_peaks():
 
 
 def profile_traffic(name):
-    """Per-launch DRAM bytes of a kernel, from a committed ncu summary line
+    """Per-launch DRAM bytes of a kernel from a committed ncu summary line
     `traffic_bytes_per_launch = N` in profiles/<name>.md (None if absent)."""
     path = os.path.join(ROOT, "profiles", name + ".md")
     if not os.path.exists(path):
@@ -83,7 +134,7 @@ def profile_traffic(name):
 
 
 class Clocks:
-    """nvidia-smi sampler for the timed region."""
+    """nvidia-smi sampler (200 ms) around the timed region."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -112,69 +163,160 @@ class Clocks:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 7:
                 try:
-                    rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+                    rows.append((float(parts[0]), float(parts[1]), float(parts[2]), parts[3:7]))
                 except ValueError:
                     pass
         os.unlink(self.f.name)
         if not rows:
             return None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for _, _, r in rows for k in range(4) if r[k].lower() == "active"})
-        return dict(sm_mhz=statistics.median(r[0] for r in rows), sm_max_mhz=max(r[1] for r in rows),
-                    samples=len(rows), reasons=reasons)
+        reasons = sorted({names[k] for *_, r in rows for k in range(4) if r[k].lower() == "active"})
+        busy = [r for r in rows if r[2] > 200.0] or rows  # samples with the GPU under load
+        return dict(sm_mhz=statistics.median(r[0] for r in busy), sm_max_mhz=max(r[1] for r in rows),
+                    power_w_max=max(r[2] for r in rows), samples=len(rows), samples_under_load=len(busy),
+                    reasons=reasons)
 
 
-def cpu_baseline(s, seconds=12.0, max_reps=20):
-    """Restated reference CPU algorithm (oracle/, phase-coloured threads) on the
-    full workload, repeated for about `seconds`."""
-    from oracle import oracle as O
-    from pfw_b200 import workloads as WL
+# ---------------------------------------------------------------------------
+# timing helpers
+# ---------------------------------------------------------------------------
+def device_step_fn(h, w, dev, lib):
+    import torch
+    X_dev = torch.from_numpy(w.sys.X).to(dev)
+    sp_dev = torch.from_numpy(w.sys.species).to(dev)
+    E = torch.zeros(1, dtype=torch.float64, device=dev)
+    F = torch.zeros((w.n, 3), dtype=torch.float64, device=dev)
+    W = torch.zeros(9, dtype=torch.float64, device=dev)
+
+    def step():
+        h.set_geometry_device(w.n, ctypes.c_void_p(X_dev.data_ptr()), w.sys.H, w.sys.pbc,
+                              ctypes.c_void_p(sp_dev.data_ptr()))
+        h.evaluate_device(w.model_sel, 7, ctypes.c_void_p(E.data_ptr()), ctypes.c_void_p(F.data_ptr()),
+                          ctypes.c_void_p(W.data_ptr()))
+    step.keep = (X_dev, sp_dev, E, F, W)
+    return step
+
+
+def time_device(h, w, dev, lib, steps, warmup, flush, stream):
+    """Per-step CUDA events on the launch stream; returns (ms list, stage array, launches)."""
+    import torch
+    step = device_step_fn(h, w, dev, lib)
+    for _ in range(max(warmup, 3)):
+        step()
+    h.check(h.L.pfw_set_diagnostics(h.ws, 1))
+    ms_buf = np.zeros(4)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stage = []
+    torch.cuda.synchronize()
+    l0 = h.launches
+    for k in range(steps):
+        flush.zero_()  # L2 flush (256 MB write), outside the step's events
+        starts[k].record(stream)
+        step()
+        ends[k].record(stream)
+        h.L.pfw_stage_times(h.ws, ms_buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 4)
+        stage.append(ms_buf.copy())
+    torch.cuda.synchronize()
+    launches = h.launches - l0
+    h.check(h.L.pfw_set_diagnostics(h.ws, 0))
+    return [a.elapsed_time(b) for a, b in zip(starts, ends)], np.array(stage), launches
+
+
+def e2e_time(h, w, lib, steps):
+    """Wall time per step through the host C ABI (pinned X in, E/F/W out)."""
+    import torch
+    n = w.n
+    Xh = torch.from_numpy(w.sys.X).pin_memory()
+    sph = torch.from_numpy(w.sys.species).pin_memory()
+    Fh = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
+    Eh = np.zeros(1)
+    Wh = np.zeros(9)
+    Hf = np.asarray(w.sys.H).ravel(order="F").copy()
+    pb = np.array([1 if b else 0 for b in w.sys.pbc], np.uint8)
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def step():
+        h.check(h.L.pfw_set_geometry(h.ws, n, ctypes.cast(Xh.data_ptr(), dp), Hf.ctypes.data_as(dp),
+                                     pb.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                     ctypes.cast(sph.data_ptr(), ctypes.POINTER(ctypes.c_int32))))
+        h.check(h.L.pfw_evaluate(h.ws, w.model_sel, 7, Eh.ctypes.data_as(dp), ctypes.cast(Fh.data_ptr(), dp),
+                                 Wh.ctypes.data_as(dp)))
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / steps, float(Eh[0]), Fh.numpy().copy()
+
+
+def cpu_baseline(w, seconds=12.0, max_reps=20):
+    """Restated reference CPU algorithm (oracle/) on the full workload, all host
+    threads, repeated for about `seconds`."""
     nthreads = os.cpu_count() or 1
+    call = w.cpu_call(nthreads)
     times = []
     t0 = time.perf_counter()
     while len(times) < max_reps and (time.perf_counter() - t0) < seconds:
         t = time.perf_counter()
-        O.pair_evaluate(s.X, s.H, s.pbc, s.species, "lj", (WL.LJ_EPS, WL.LJ_SIGMA), WL.LJ_CUTOFF,
-                        nthreads=nthreads)
+        call()
         times.append(time.perf_counter() - t)
     med = statistics.median(times)
-    return dict(value=len(s) / med, unit="atoms/s", cores=nthreads, kind="port",
-                sample=f"full {len(s)}-atom LJ box, {len(times)} evaluate! calls (median), "
+    return dict(value=w.n / med, unit="atoms/s", cores=nthreads, kind="port",
+                sample=f"full {w.n}-atom {w.config['workload']} system, {len(times)} evaluations (median), "
                        f"restated reference CPU algorithm (oracle/), {nthreads} threads")
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="lj", choices=["lj", "lj1m", "lj_shear", "smooth", "ace", "ace_tial"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-forms", action="store_true")
+    return p.parse_args()
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
 def run_reference(args):
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    s, cfg = workload()
-    from oracle import oracle as O
-    from pfw_b200 import workloads as WL
+    w = Workload(args.workload)
     nthreads = os.cpu_count() or 1
-    call = lambda: O.pair_evaluate(s.X, s.H, s.pbc, s.species, "lj", (WL.LJ_EPS, WL.LJ_SIGMA), WL.LJ_CUTOFF,
-                                   nthreads=nthreads)
+    call = w.cpu_call(nthreads)
     for _ in range(args.warmup):
         call()
+    steps = max(args.steps, 1)
     t = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         call()
-    dt = (time.perf_counter() - t) / max(args.steps, 1)
-    v = len(s) / dt
-    cfg = dict(cfg, parallelism="cpu threads", note="reference is Julia (not installable here); "
-               "its CPU algorithm restated in oracle/ is timed")
-    line = dict(impl="reference", metric=METRIC, value=v, unit="atoms/s", n_gpus=args.gpus, steps=args.steps,
+    dt = (time.perf_counter() - t) / steps
+    v = w.n / dt
+    cfg = dict(w.config, atoms=w.n, parallelism="cpu threads",
+               note="reference is a Julia package (not installable here); its CPU algorithm restated in oracle/ is timed")
+    line = dict(impl="reference", metric=METRIC, value=v, unit="atoms/s", n_gpus=args.gpus, steps=steps,
                 warmup=args.warmup, ms_per_step=dt * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f64", data="synthetic", config=cfg,
                 cpu_baseline=dict(value=v, unit="atoms/s", cores=nthreads, kind="port",
-                                  sample=f"full {len(s)}-atom LJ box per step"),
+                                  sample=f"full {w.n}-atom system per step"),
                 e2e=dict(value=v, unit="atoms/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
     return 0
 
 
 def run_b200(args):
-    import ctypes
-
     import torch
 
     from pfw_b200 import lib
@@ -186,123 +328,71 @@ def run_b200(args):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    s, cfg = workload()
-    n = len(s)
+    w = Workload(args.workload)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     h = lib.Handle(lib.FP64, device=local)
     h.check(h.L.pfw_set_stream(h.ws, ctypes.c_void_p(stream.cuda_stream)))
-    h.lj(cfg["epsilon"], cfg["sigma"], cfg["cutoff"])
-    X_dev = torch.from_numpy(s.X).to(dev)
-    sp_dev = torch.from_numpy(s.species).to(dev)
-    E_dev = torch.zeros(1, dtype=torch.float64, device=dev)
-    F_dev = torch.zeros((n, 3), dtype=torch.float64, device=dev)
-    W_dev = torch.zeros(9, dtype=torch.float64, device=dev)
+    w.bind(h)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-
-    def step():
-        h.set_geometry_device(n, ctypes.c_void_p(X_dev.data_ptr()), s.H, s.pbc, ctypes.c_void_p(sp_dev.data_ptr()))
-        h.evaluate_device(lib.MODEL_PAIR, 7, ctypes.c_void_p(E_dev.data_ptr()), ctypes.c_void_p(F_dev.data_ptr()),
-                          ctypes.c_void_p(W_dev.data_ptr()))
-
-    for _ in range(max(args.warmup, 3)):
-        step()
-    h.check(h.L.pfw_set_diagnostics(h.ws, 1))
-    ms_buf = np.zeros(4)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stage = []
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
-    l0 = h.launches
-    for k in range(args.steps):
-        flush.zero_()  # L2 flush (256 MB write), outside the step's events
-        starts[k].record(stream)
-        step()
-        ends[k].record(stream)
-        h.L.pfw_stage_times(h.ws, ms_buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 4)
-        stage.append(ms_buf.copy())
-    torch.cuda.synchronize()
-    launches = h.launches - l0
+    time.sleep(0.25)
+    step_ms, stage, launches = time_device(h, w, dev, lib, args.steps, args.warmup, flush, stream)
     clk = clocks.stop()
-    h.check(h.L.pfw_set_diagnostics(h.ws, 0))
-    step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     ms = sum(step_ms) / len(step_ms)
     if dist:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
-    value = world * n / (ms * 1e-3)
-    stage = np.array(stage)
+    value = world * w.n / (ms * 1e-3)
     kern_ms = float(stage[:, 1].mean())
     geom_ms = float(stage[:, 0].mean())
-
-    # e2e through the host C ABI: pinned X in, E/F/W out, copies timed
-    Xh = torch.from_numpy(s.X).pin_memory()
-    sph = torch.from_numpy(s.species).pin_memory()
-    Fh = torch.zeros((n, 3), dtype=torch.float64).pin_memory()
-    Eh = np.zeros(1)
-    Wh = np.zeros(9)
-    Hf = np.asarray(s.H).ravel(order="F").copy()
-    pb = np.array([1, 1, 1], np.uint8)
-    dp = ctypes.POINTER(ctypes.c_double)
-
-    def e2e_step():
-        h.check(h.L.pfw_set_geometry(h.ws, n, ctypes.cast(Xh.data_ptr(), dp), Hf.ctypes.data_as(dp),
-                                     pb.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
-                                     ctypes.cast(sph.data_ptr(), ctypes.POINTER(ctypes.c_int32))))
-        h.check(h.L.pfw_evaluate(h.ws, lib.MODEL_PAIR, 7, Eh.ctypes.data_as(dp), ctypes.cast(Fh.data_ptr(), dp),
-                                 Wh.ctypes.data_as(dp)))
-
-    for _ in range(3):
-        e2e_step()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_s, E_ref, F_ref = e2e_time(h, w, lib, max(args.steps // 4, 5))
     if dist:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    npairs = h.pair_count()
-    E_ref = float(Eh[0])
-
     line = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        alg_bytes = 49.0 * n  # X 24 B + species 1 B read, F 24 B written per atom
-        achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
         fp64_peak = h.probe_fp64()
-        alg_flops = npairs * 65.0  # 62 flop + 1 sqrt + 2 div per in-cutoff unordered pair
-        traffic = profile_traffic("pair_lj_fp64")
+        cfg = dict(w.config, atoms=w.n, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                   l2="256 MB flush between steps, outside the per-step events", energy_eV=E_ref)
+        if w.kind == "pair":
+            npairs = h.pair_count()
+            alg_bytes = 49.0 * w.n  # X 24 B + species 1 B read, F 24 B written per atom
+            alg_flops = npairs * w.flop_per_pair
+            cfg["unordered_pairs"] = npairs
+            traffic = profile_traffic("pair_lj_fp64") if args.workload == "lj" else None
+        else:
+            alg_bytes = 49.0 * w.n
+            alg_flops = None
+            traffic = profile_traffic("ace_sites_fp64") if args.workload == "ace" else None
+        achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+        roof = dict(bound="hbm", kernel=w.kernel, achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                    peak_source=peak_kind, traffic=traffic, kernel_ms=kern_ms, geometry_ms=geom_ms,
+                    algorithmic_bytes_per_launch=alg_bytes)
+        if alg_flops:
+            tf = alg_flops / (kern_ms * 1e-3) / 1e12
+            roof["fp64_pipe"] = dict(achieved_tflops=tf, peak_tflops=fp64_peak, frac=tf / fp64_peak,
+                                     peak_source="measured DFMA probe (pfw_probe_fp64_peak)",
+                                     algorithmic_flops_per_launch=alg_flops)
         line = dict(
             metric=METRIC, value=value, unit="atoms/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
             ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
-            data="synthetic (seeded FCC lattice, Gaussian displacements)",
-            config=dict(cfg, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
-                        l2="256 MB flush between steps, outside the per-step events",
-                        unordered_pairs=npairs, energy_eV=E_ref),
-            roofline=dict(bound="hbm", kernel="k_pair64<LJ>", achieved=achieved, peak=peak, unit="GB/s",
-                          frac=achieved / peak, peak_source=peak_kind, traffic=traffic,
-                          kernel_ms=kern_ms, geometry_ms=geom_ms, algorithmic_bytes_per_launch=alg_bytes,
-                          fp64_pipe=dict(achieved_tflops=alg_flops / (kern_ms * 1e-3) / 1e12, peak_tflops=fp64_peak,
-                                         frac=alg_flops / (kern_ms * 1e-3) / 1e12 / fp64_peak,
-                                         peak_source="measured DFMA probe (pfw_probe_fp64_peak)",
-                                         algorithmic_flops_per_launch=alg_flops)),
-            e2e=dict(value=world * n / e2e_s, unit="atoms/s", ms_per_step=e2e_s * 1e3, h2d_bytes_per_step=28 * n,
-                     d2h_bytes_per_step=24 * n + 8 + 72, api="pfw_set_geometry + pfw_evaluate (host buffers)"),
+            data="synthetic (seeded lattice, Gaussian displacements)", config=cfg, roofline=roof,
+            e2e=dict(value=world * w.n / e2e_s, unit="atoms/s", ms_per_step=e2e_s * 1e3,
+                     h2d_bytes_per_step=28 * w.n, d2h_bytes_per_step=24 * w.n + 8 + 72,
+                     api="pfw_set_geometry + pfw_evaluate (host buffers, pinned)"),
             gpu_launches=launches, clocks=clk)
         if not args.no_forms:
-            line["forms"] = forms(s, dev)
+            line["forms"] = forms(args, dev, stream, flush, F_ref)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(s)
+            line["cpu_baseline"] = cpu_baseline(w)
     h.close()
     if dist:
         dist.barrier()
@@ -312,49 +402,44 @@ def run_b200(args):
     return 0
 
 
-def forms(s, dev):
-    """Mixed-precision form on the same workload: atoms/s and force error vs FP64."""
-    import torch
-
+def forms(args, dev, stream, flush, F_head):
+    """The other configurations (plain FP64) and the mixed form, each timed with
+    a few device steps; reduced-precision forms report errors vs plain FP64."""
     from pfw_b200 import lib
     out = {}
-    h64 = lib.Handle(lib.FP64, device=dev.index)
-    h64.set_geometry(s.X, s.H, s.pbc, s.species)
-    h64.lj(0.0104, 3.4, 8.5)
-    E64, F64, W64 = h64.evaluate(lib.MODEL_PAIR, 7)
-    h32 = lib.Handle(lib.MIXED, device=dev.index)
-    h32.set_geometry(s.X, s.H, s.pbc, s.species)
-    h32.lj(0.0104, 3.4, 8.5)
-    E32, F32, W32 = h32.evaluate(lib.MODEL_PAIR, 7)
-    import ctypes
-    X_dev = torch.from_numpy(s.X).to(dev)
-    sp_dev = torch.from_numpy(s.species).to(dev)
-    bufs = [torch.zeros(k, dtype=torch.float64, device=dev) for k in (1, 3 * len(s), 9)]
-    stream = torch.cuda.current_stream(dev)
-    h32.check(h32.L.pfw_set_stream(h32.ws, ctypes.c_void_p(stream.cuda_stream)))
-
-    def step():
-        h32.set_geometry_device(len(s), ctypes.c_void_p(X_dev.data_ptr()), s.H, s.pbc,
-                                ctypes.c_void_p(sp_dev.data_ptr()))
-        h32.evaluate_device(lib.MODEL_PAIR, 7, *[ctypes.c_void_p(b.data_ptr()) for b in bufs])
-
-    for _ in range(3):
-        step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(10):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / 10
-    out["mixed_lj"] = dict(value=len(s) / (ms * 1e-3), unit="atoms/s", ms_per_step=ms,
-                           force_rmse=float(np.sqrt(np.mean((F32 - F64) ** 2))),
-                           force_max_err=float(np.abs(F32 - F64).max()), energy_err=abs(E32 - E64),
-                           virial_max_err=float(np.abs(W32 - W64).max()),
-                           note="FP32 pair arithmetic, FP64 wrap/shift, Kahan FP64 E/W; errors vs plain FP64")
-    h32.close()
-    h64.close()
+    steps = 10
+    for name in ("lj1m", "lj_shear", "smooth", "ace", "ace_tial"):
+        if name == args.workload:
+            continue
+        w = Workload(name)
+        h = lib.Handle(lib.FP64, device=dev.index)
+        h.check(h.L.pfw_set_stream(h.ws, ctypes.c_void_p(stream.cuda_stream)))
+        w.bind(h)
+        ms, stage, _ = time_device(h, w, dev, lib, steps, 3, flush, stream)
+        ms = float(np.mean(ms))
+        out[w.config["workload"] + "_fp64"] = dict(value=w.n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms,
+                                                   kernel_ms=float(stage[:, 1].mean()))
+        h.close()
+    for name in ("lj", "ace"):
+        w = Workload(name)
+        h64 = lib.Handle(lib.FP64, device=dev.index)
+        h64.set_geometry(w.sys.X, w.sys.H, w.sys.pbc, w.sys.species)
+        w.bind(h64)
+        E64, F64, W64 = h64.evaluate(w.model_sel, 7)
+        h64.close()
+        h32 = lib.Handle(lib.MIXED, device=dev.index)
+        h32.check(h32.L.pfw_set_stream(h32.ws, ctypes.c_void_p(stream.cuda_stream)))
+        w.bind(h32)
+        h32.set_geometry(w.sys.X, w.sys.H, w.sys.pbc, w.sys.species)
+        E32, F32, W32 = h32.evaluate(w.model_sel, 7)
+        ms, stage, _ = time_device(h32, w, dev, lib, steps, 3, flush, stream)
+        ms = float(np.mean(ms))
+        out[w.config["workload"] + "_mixed"] = dict(
+            value=w.n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms, kernel_ms=float(stage[:, 1].mean()),
+            force_rmse=float(np.sqrt(np.mean((F32 - F64) ** 2))), force_max_err=float(np.abs(F32 - F64).max()),
+            energy_err=abs(E32 - E64), virial_max_err=float(np.abs(W32 - W64).max()),
+            note="FP32 arithmetic, FP64 wrap/shift and FP64 (Kahan) energy/virial accumulation; errors vs plain FP64")
+        h32.close()
     return out
 
 

@@ -39,6 +39,7 @@ struct AceDevice {
   int64_t nedges = 0;
   int n = 0;
   bool evaluated = false;
+  int sched_chunk = 0, sched_groups = 0;  // 0: automatic
 };
 
 // ---------------------------------------------------------------------------
@@ -373,17 +374,37 @@ static AceTables tables_of(AceDevice* a) {
 
 // Largest working set that fits: two 128-thread groups with 32-edge chunks
 // when possible, else smaller chunks / one group.
-static AceLayout choose_layout(const AceTables& p, int device) {
+static AceLayout choose_layout(const AceTables& p, int device, int chunk, int groups) {
   int optin = 0;
   PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   const size_t limit = (size_t)optin;
-  const int cand[][2] = {{32, 2}, {16, 2}, {32, 1}, {16, 1}, {8, 1}};
+  if (chunk > 0) {
+    AceLayout lay;
+    lay.make(p, chunk, groups);
+    if (lay.total > limit) throw Error(PFW_EINVAL, "ACE schedule does not fit in shared memory");
+    return lay;
+  }
+  const int cand[][2] = {{32, 2}, {16, 3}, {16, 2}, {32, 1}, {16, 1}, {8, 1}};
   for (auto& c : cand) {
     AceLayout lay;
     lay.make(p, c[0], c[1]);
     if (lay.total <= limit) return lay;
   }
   throw Error(PFW_EINVAL, "ACE model too large for the site kernel's shared memory");
+}
+
+void ace_set_schedule(pfw_ws* ws, int chunk, int groups) {
+  AceDevice* a = ws->ace;
+  if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
+  if (chunk == 0 && groups == 0) {
+    a->sched_chunk = a->sched_groups = 0;
+    return;
+  }
+  if (!(chunk == 8 || chunk == 16 || chunk == 32) || groups < 1 || groups > ACE_MAX_GROUPS)
+    throw Error(PFW_EINVAL, "ACE schedule: chunk must be 8, 16 or 32 and groups 1..4");
+  choose_layout(tables_of(a), ws->opt.device, chunk, groups);  // validates the fit
+  a->sched_chunk = chunk;
+  a->sched_groups = groups;
 }
 
 template <int L, class T>
@@ -478,7 +499,7 @@ void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   double* out = static_cast<double*>(a->site_out.ensure(sizeof(double) * 10 * std::max(n, 1)));
   double* Esite = static_cast<double*>(a->site_E_orig.ensure(sizeof(double) * std::max(n, 1)));
   const AceTables p = tables_of(a);
-  const AceLayout lay = choose_layout(p, ws->opt.device);
+  const AceLayout lay = choose_layout(p, ws->opt.device, a->sched_chunk, a->sched_groups);
   ws->stage_begin(1);
   if (n > 0) {
     const int* off = a->edge_off.as<int>();

@@ -168,6 +168,57 @@ __device__ __forceinline__ Jet<T, G> jscale(T s, const Jet<T, G>& b) {
 
 constexpr int ACE_LMAX = 6;
 
+// The harmonics of one azimuthal order m ≥ 0 (all l in m..L): the same
+// recurrences as angular_blocks.jl:49-77 evaluated m-major, so each value is
+// computed from the same operands by the same formula:
+//   cos/sin(mφ):  c_{k+1} = c_k x - s_k y,  s_{k+1} = s_k x + c_k y  (c_0 → 1/√2 for m = 0)
+//   Q_mm = -(2m-1) Q_{m-1,m-1},  Q_{m+1,m} = (2m+1) z Q_mm,
+//   Q_lm = ((2l-1) z Q_{l-1,m} - (l+m-1) r² Q_{l-2,m}) / (l-m)
+// emit(index, Jet) receives Y_lm at l*l+l+m and, for m > 0, Y_l,-m at l*l+l-m.
+template <class T, bool Grad, int L, class Emit>
+__device__ __forceinline__ void harmonics_m(const double* __restrict__ F, T r, T dx, T dy, T dz, int m,
+                                            Emit&& emit) {
+  using J = Jet<T, Grad>;
+  const T ir = T(1) / r;
+  const T ux = dx * ir, uy = dy * ir, uz = dz * ir;
+  const J x = {ux, Grad ? (T(1) - ux * ux) * ir : T(0), Grad ? (-ux * uy) * ir : T(0), Grad ? (-ux * uz) * ir : T(0)};
+  const J y = {uy, Grad ? (-uy * ux) * ir : T(0), Grad ? (T(1) - uy * uy) * ir : T(0), Grad ? (-uy * uz) * ir : T(0)};
+  const J z = {uz, Grad ? (-uz * ux) * ir : T(0), Grad ? (-uz * uy) * ir : T(0), Grad ? (T(1) - uz * uz) * ir : T(0)};
+  const J r2 = jadd(jadd(jmul(x, x), jmul(y, y)), jmul(z, z));
+  J cs = {T(1), T(0), T(0), T(0)}, sn = {T(0), T(0), T(0), T(0)};
+  J q = {T(1), T(0), T(0), T(0)};  // Q_kk along the diagonal
+#pragma unroll
+  for (int k = 1; k <= L; ++k) {
+    if (k > m) break;
+    const J c2 = jsub(jmul(cs, x), jmul(sn, y));
+    const J s2 = jadd(jmul(sn, x), jmul(cs, y));
+    cs = c2;
+    sn = s2;
+    q = jscale(T(-(2 * k - 1)), q);
+  }
+  if (m == 0) cs = {T(0.70710678118654752440), T(0), T(0), T(0)};
+  J qm2 = q, qm1 = q;
+#pragma unroll
+  for (int l = 0; l <= L; ++l) {
+    if (l < m) continue;
+    J ql;
+    if (l == m) {
+      ql = q;
+    } else if (l == m + 1) {
+      ql = jscale(T(2 * m + 1), jmul(z, qm1));
+    } else {
+      const J a = jscale(T(2 * l - 1), jmul(z, qm1));
+      const J b = jscale(T(l + m - 1), jmul(r2, qm2));
+      ql = jscale(T(1) / T(l - m), jsub(a, b));
+    }
+    const T Fl = (T)F[l * (L + 1) + m];
+    emit(l * l + l + m, jscale(Fl, jmul(ql, cs)));
+    if (m > 0) emit(l * l + l - m, jscale(Fl, jmul(ql, sn)));
+    qm2 = qm1;
+    qm1 = ql;
+  }
+}
+
 // BlockAngular harmonics of direction d (angular_blocks.jl:36-81).  Calls
 // emit(index, Jet) for every component in l*l+l+m order; with Grad=false the
 // gradients are not formed.  F: normalisation [(L+1)*(L+1)] as F[l*(L+1)+m].

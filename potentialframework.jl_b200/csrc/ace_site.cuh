@@ -1,7 +1,8 @@
 // ace_site.cuh — the persistent ACE site kernel.
 //
 // One CTA per SM slot holds the model's product, adjoint-term and density
-// tables and the precontracted weights in shared memory (loaded once), and
+// tables in shared memory (loaded once; the precontracted weights are read
+// through L1), and
 // runs G groups of 128 threads; each group evaluates one site at a time
 // (sites strided over the grid), with its own A/dA vectors and an edge-chunk
 // working set of CH edges:
@@ -22,6 +23,7 @@
 namespace pfw {
 
 constexpr int ACE_GROUP = 128;
+constexpr int ACE_MAX_GROUPS = 4;
 
 struct AceTables {
   RadialDev R, Q;
@@ -44,7 +46,8 @@ struct AceTables {
 // shared-memory layout (byte offsets), computed identically on host and device
 struct AceLayout {
   int CH, G;
-  size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, weights, tables_end;
+  int RS, YS;  // odd row strides of the per-edge R and Y tables (bank-conflict padding)
+  size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, tables_end;
   size_t group_bytes, total;
   // group-relative double offsets
   int A, dA, Y, dY, R, dR, T1, T2, esc, ints;
@@ -61,17 +64,18 @@ struct AceLayout {
     dn = o; o = align16(o + sizeof(int2) * t.D);
     dm_off = o; o = align16(o + sizeof(int) * (t.nY + 1));
     dm = o; o = align16(o + sizeof(int2) * t.D);
-    weights = o; o = align16(o + sizeof(double) * t.nz * t.P);
     tables_end = o;
+    RS = t.nR | 1;
+    YS = t.nY | 1;
     int d = 0;
     A = d; d += t.D + 1;
     dA = d; d += t.D + 1;
-    Y = d; d += CH * t.nY;
-    dY = d; d += CH * t.nY * 3;
-    R = d; d += CH * t.nR;
-    dR = d; d += CH * t.nR;
-    T1 = d; d += CH * t.nR;
-    T2 = d; d += CH * t.nY;
+    Y = d; d += CH * YS;
+    dY = d; d += CH * YS * 3;
+    R = d; d += CH * RS;
+    dR = d; d += CH * RS;
+    T1 = d; d += CH * RS;
+    T2 = d; d += CH * YS;
     esc = d; d += CH * 10 + 4 * 10;  // per-edge scalars, then warp partials
     ints = d; d += CH;               // 2 ints per edge
     group_bytes = align16(sizeof(double) * d);
@@ -90,58 +94,69 @@ struct EdgeScalars {
   int *k0, *pidx;
 };
 
+// Per-edge set-up of one chunk, four threads per edge (lt = 4t + q):
+// q = 0 the R-family transform/interval/envelope, q = 1 the pair radials,
+// and harmonics split by azimuthal order m ≡ q (mod 4).
 template <int L, class T, bool Grad>
 __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbase, const AceLayout& lay,
                                                 const EdgeScalars<T>& es, const double4* __restrict__ edge_d, int e0,
                                                 int nc, int iz, int lt, double& e_acc, int* status) {
-  if (lt >= nc) return;
-  const double4 d = edge_d[e0 + lt];
+  const int t = lt >> 2, q = lt & 3;
+  if (t >= nc) return;
+  const double4 d = edge_d[e0 + t];
   const int zj = min(max((int)d.w, 0), p.nz - 1);
   const int pidx = iz * p.nz + zj;
   const T dx = (T)d.x, dy = (T)d.y, dz = (T)d.z;
   const T r0 = sqrt(dx * dx + dy * dy + dz * dz);
-  if (!(r0 > T(0))) atomicOr(status, 2);
   const T r = r0 > T(0) ? r0 : T(1);
-  es.r[lt] = r;
-  es.dx[lt] = dx;
-  es.dy[lt] = dy;
-  es.dz[lt] = dz;
-  const EdgeRadial<T> er = edge_radial<T>(p.R, pidx, r);
-  es.k0[lt] = er.k0;
-  es.pidx[lt] = pidx;
-  es.u[lt] = er.u;
-  es.e[lt] = er.e;
-  es.de[lt] = er.de;
-  es.du[lt] = er.du;
-  double qe = 0.0;
-  T qd = T(0);
-  if (p.nQ > 0 && p.pair_ok[zj]) {
-    const EdgeRadial<T> eq = edge_radial<T>(p.Q, pidx, r);
-    if (!eq.ok) atomicOr(status, 2);
-    const double* wp = p.wpair + (size_t)iz * p.nQ;
-    for (int n = 0; n < p.nQ; ++n) {
-      T v, dv;
-      channel_ed<T>(channel_coeff(p.Q, pidx, eq.k0, n), eq, v, dv);
-      qe += (double)v * wp[n];
-      qd += (T)wp[n] * dv;
+  if (q == 0) {
+    if (!(r0 > T(0))) atomicOr(status, 2);
+    es.r[t] = r;
+    es.dx[t] = dx;
+    es.dy[t] = dy;
+    es.dz[t] = dz;
+    const EdgeRadial<T> er = edge_radial<T>(p.R, pidx, r);
+    es.k0[t] = er.k0;
+    es.pidx[t] = pidx;
+    es.u[t] = er.u;
+    es.e[t] = er.e;
+    es.de[t] = er.de;
+    es.du[t] = er.du;
+  } else if (q == 1) {
+    double qe = 0.0;
+    T qd = T(0);
+    if (p.nQ > 0 && p.pair_ok[zj]) {
+      const EdgeRadial<T> eq = edge_radial<T>(p.Q, pidx, r);
+      if (!eq.ok) atomicOr(status, 2);
+      const double* wp = p.wpair + (size_t)iz * p.nQ;
+      for (int n = 0; n < p.nQ; ++n) {
+        T v, dv;
+        channel_ed<T>(channel_coeff(p.Q, pidx, eq.k0, n), eq, v, dv);
+        qe += (double)v * wp[n];
+        qd += (T)wp[n] * dv;
+      }
     }
+    if (!Grad) e_acc += qe;
+    es.dq[t] = qd;
   }
-  if (!Grad) e_acc += qe;
-  es.dq[lt] = qd;
-  double* Yt = gbase + lay.Y + lt * p.nY;
-  double* dYt = gbase + lay.dY + lt * p.nY * 3;
-  harmonics<T, Grad, L>(p.Fnorm, r, dx, dy, dz, [&](int idx, const Jet<T, Grad>& j) {
-    Yt[idx] = j.v;
-    if constexpr (Grad) {
-      dYt[3 * idx] = j.gx;
-      dYt[3 * idx + 1] = j.gy;
-      dYt[3 * idx + 2] = j.gz;
-    }
-  });
+  double* Yt = gbase + lay.Y + t * lay.YS;
+  double* dYt = gbase + lay.dY + t * lay.YS * 3;
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    if ((m & 3) != q) continue;
+    harmonics_m<T, Grad, L>(p.Fnorm, r, dx, dy, dz, m, [&](int idx, const Jet<T, Grad>& j) {
+      Yt[idx] = j.v;
+      if constexpr (Grad) {
+        dYt[3 * idx] = j.gx;
+        dYt[3 * idx + 1] = j.gy;
+        dYt[3 * idx + 2] = j.gz;
+      }
+    });
+  }
 }
 
 template <int L, class T>
-__global__ void __launch_bounds__(2 * ACE_GROUP)
+__global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
     k_ace_sites(AceTables p, AceLayout lay, int nsites, const int* __restrict__ edge_off,
                 const double4* __restrict__ edge_d, const double4* __restrict__ pos, double* __restrict__ edge_g,
                 double* __restrict__ site_out, int want_grad, int* __restrict__ status) {
@@ -155,7 +170,6 @@ __global__ void __launch_bounds__(2 * ACE_GROUP)
   int2* s_dn = reinterpret_cast<int2*>(smem + lay.dn);
   int* s_dmoff = reinterpret_cast<int*>(smem + lay.dm_off);
   int2* s_dm = reinterpret_cast<int2*>(smem + lay.dm);
-  double* s_w = reinterpret_cast<double*>(smem + lay.weights);
   for (int k = threadIdx.x; k < p.P; k += blockDim.x) s_prods[k] = p.prods[k];
   for (int k = threadIdx.x; k < p.T; k += blockDim.x) s_terms[k] = p.terms[k];
   for (int k = threadIdx.x; k <= p.D; k += blockDim.x) s_toff[k] = p.term_off[k];
@@ -166,7 +180,6 @@ __global__ void __launch_bounds__(2 * ACE_GROUP)
   }
   for (int k = threadIdx.x; k <= p.nR; k += blockDim.x) s_dnoff[k] = p.dn_off[k];
   for (int k = threadIdx.x; k <= p.nY; k += blockDim.x) s_dmoff[k] = p.dm_off[k];
-  for (int k = threadIdx.x; k < p.nz * p.P; k += blockDim.x) s_w[k] = p.weights[k];
   __syncthreads();
 
   const int g = threadIdx.x / ACE_GROUP, lt = threadIdx.x % ACE_GROUP;
@@ -188,7 +201,7 @@ __global__ void __launch_bounds__(2 * ACE_GROUP)
   es.wred = e0p + 10 * CH;
   es.k0 = reinterpret_cast<int*>(gb + lay.ints);
   es.pidx = es.k0 + CH;
-  const int D = p.D, nY = p.nY, nR = p.nR, P = p.P;
+  const int D = p.D, nY = p.nY, nR = p.nR, P = p.P, RS = lay.RS, YS = lay.YS;
   const int lane = lt & 31, wg = lt >> 5;
 
   for (int s = blockIdx.x * lay.G + g; s < nsites; s += gridDim.x * lay.G) {
@@ -207,29 +220,29 @@ __global__ void __launch_bounds__(2 * ACE_GROUP)
         const int t = idx / nR, n = idx - t * nR;
         const double* c = channel_coeff(p.R, es.pidx[t], es.k0[t], n);
         const T u = (T)es.u[t];
-        Rc[t * nR + n] = (T)es.e[t] * ((((T)c[3] * u + (T)c[2]) * u + (T)c[1]) * u + (T)c[0]);
+        Rc[t * RS + n] = (T)es.e[t] * ((((T)c[3] * u + (T)c[2]) * u + (T)c[1]) * u + (T)c[0]);
       }
       group_sync(g);
       for (int a = lt; a < D; a += ACE_GROUP) {
         const int2 nm = s_dens[a];
         T acc = (T)A[a];
-        for (int t = 0; t < nc; ++t) acc += (T)Rc[t * nR + nm.x] * (T)Yc[t * nY + nm.y];
+        for (int t = 0; t < nc; ++t) acc += (T)Rc[t * RS + nm.x] * (T)Yc[t * YS + nm.y];
         A[a] = acc;
       }
     }
     group_sync(g);
     // ---- products, energy, adjoints ----
-    const double* w = s_w + (size_t)iz * P;
+    const double* __restrict__ w = p.weights + (size_t)iz * P;
     for (int k = lt; k < P; k += ACE_GROUP) {
       const ushort4 f = s_prods[k];
-      e_acc += w[k] * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
+      e_acc += __ldg(w + k) * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
     }
     if (want_grad)
       for (int a = lt; a < D; a += ACE_GROUP) {
         T acc = T(0);
         for (int q = s_toff[a]; q < s_toff[a + 1]; ++q) {
           const ushort4 tm = s_terms[q];
-          acc += (T)w[tm.x] * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
+          acc += (T)__ldg(w + tm.x) * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
         }
         dA[a] = acc;
       }
@@ -251,8 +264,8 @@ __global__ void __launch_bounds__(2 * ACE_GROUP)
           er.du = (T)es.du[t];
           T v, dv;
           channel_ed<T>(channel_coeff(p.R, es.pidx[t], es.k0[t], n), er, v, dv);
-          Rc[t * nR + n] = v;
-          dRc[t * nR + n] = dv;
+          Rc[t * RS + n] = v;
+          dRc[t * RS + n] = dv;
         }
         group_sync(g);
         for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
@@ -260,30 +273,30 @@ __global__ void __launch_bounds__(2 * ACE_GROUP)
           T acc = T(0);
           for (int q = s_dnoff[n]; q < s_dnoff[n + 1]; ++q) {
             const int2 am = s_dn[q];
-            acc += (T)dA[am.x] * (T)Yc[t * nY + am.y];
+            acc += (T)dA[am.x] * (T)Yc[t * YS + am.y];
           }
-          T1[t * nR + n] = acc;
+          T1[t * RS + n] = acc;
         }
         for (int idx = lt; idx < nc * nY; idx += ACE_GROUP) {
           const int t = idx / nY, m = idx - t * nY;
           T acc = T(0);
           for (int q = s_dmoff[m]; q < s_dmoff[m + 1]; ++q) {
             const int2 an = s_dm[q];
-            acc += (T)dA[an.x] * (T)Rc[t * nR + an.y];
+            acc += (T)dA[an.x] * (T)Rc[t * RS + an.y];
           }
-          T2[t * nY + m] = acc;
+          T2[t * YS + m] = acc;
         }
         group_sync(g);
         // 4 threads per edge (CH <= 32)
         const int t = lt >> 2, q4 = lt & 3;
         T s1 = T(0), gx = T(0), gy = T(0), gz = T(0);
         if (t < nc) {
-          for (int n = q4; n < nR; n += 4) s1 += (T)dRc[t * nR + n] * (T)T1[t * nR + n];
+          for (int n = q4; n < nR; n += 4) s1 += (T)dRc[t * RS + n] * (T)T1[t * RS + n];
           for (int m = q4; m < nY; m += 4) {
-            const T t2 = (T)T2[t * nY + m];
-            gx += (T)dYc[(t * nY + m) * 3] * t2;
-            gy += (T)dYc[(t * nY + m) * 3 + 1] * t2;
-            gz += (T)dYc[(t * nY + m) * 3 + 2] * t2;
+            const T t2 = (T)T2[t * YS + m];
+            gx += (T)dYc[(t * YS + m) * 3] * t2;
+            gy += (T)dYc[(t * YS + m) * 3 + 1] * t2;
+            gz += (T)dYc[(t * YS + m) * 3 + 2] * t2;
           }
         }
 #pragma unroll

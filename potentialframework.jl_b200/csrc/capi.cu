@@ -166,6 +166,10 @@ pfw_status pfw_ace_model_load(pfw_ws* ws, const pfw_ace_tables* tables) {
   });
 }
 
+pfw_status pfw_ace_set_schedule(pfw_ws* ws, int32_t chunk, int32_t groups) {
+  return guarded(ws, [&] { pfw::ace_set_schedule(ws, chunk, groups); });
+}
+
 pfw_status pfw_evaluate_device(pfw_ws* ws, int32_t model, uint32_t request, double* E_dev, double* F_dev,
                                double* W_dev) {
   return guarded(ws, [&] {

@@ -431,6 +431,8 @@ void prepare(pfw_ws* ws, double cutoff) {
   if (P.valid && P.cutoff == cutoff) return;
   const int n = ws->n;
   const int nsys = (int)ws->systems.size();
+  // neighbour lists pack sorted indices in 24 bits
+  if (n >= (1 << 24)) throw Error(PFW_EINVAL, "at most 16,777,215 atoms per evaluation");
   cudaStream_t st = ws->stream;
   P.sys.resize(nsys);
   bool any_open = false, any_image = false;

@@ -54,10 +54,14 @@ __device__ __forceinline__ void write_cell_parts(double* cellpart, int cell, int
   }
 }
 
+#ifndef PFW_PAIR_MINBLOCKS
+#define PFW_PAIR_MINBLOCKS 1
+#endif
+
 // Plain FP64 path.  MODE 0: displacement = (x_j - x_i) + cell shift;
 // MODE 1: per-pair minimum image (small boxes).
 template <int KIND, int MODE>
-__global__ void __launch_bounds__(PAIR_WARPS * 32)
+__global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
     k_pair64(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
              const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
              double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
@@ -98,7 +102,10 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32)
           en = aq2 * q;
           coef = -6.0 * aq2 * prm.invc2;
         } else {
-          const double ir2 = __drcp_rn(r2);
+          // 1/r² by two Newton steps y ← y(2 - r²y) from an FP32 seed (≈1 ulp)
+          double ir2 = (double)__frcp_rn((float)r2);
+          ir2 = fma(ir2, fma(-r2, ir2, 1.0), ir2);
+          ir2 = fma(ir2, fma(-r2, ir2, 1.0), ir2);
           const double s2 = prm.sigma2 * ir2;
           const double s6 = s2 * s2 * s2;
           en = prm.eps4 * (s6 * s6 - s6) - prm.shift;

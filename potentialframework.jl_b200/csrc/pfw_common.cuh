@@ -114,8 +114,20 @@ __device__ __forceinline__ void stencil_entry(const SysGeom& g, const int key[3]
         other[a] = 0;
         e.s[a] = off[a];
       } else {
-        other[a] = imod(v, g.pdims[a]);
-        e.s[a] = ifld(v, g.pdims[a]);
+        // other = mod(v, dims), s = fld(v, dims) without integer division:
+        // |off| <= radius, so a few steps at most
+        const int dm = g.pdims[a];
+        int s = 0;
+        while (v < 0) {
+          v += dm;
+          --s;
+        }
+        while (v >= dm) {
+          v -= dm;
+          ++s;
+        }
+        other[a] = v;
+        e.s[a] = s;
       }
     } else {
       if (g.brute) v = 0;

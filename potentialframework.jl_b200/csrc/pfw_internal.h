@@ -130,6 +130,7 @@ int64_t neighbour_build(pfw_ws* ws, double cutoff);
 void neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);
 // ace.cu
 void ace_load(pfw_ws* ws, const pfw_ace_tables* t);
+void ace_set_schedule(pfw_ws* ws, int chunk, int groups);
 void ace_free(pfw_ws* ws);
 void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev);
 void ace_site_energies(pfw_ws* ws, double* host);

@@ -1,44 +1,83 @@
 // traverse.cuh — warp-per-home-cell traversal of all directed neighbours.
 //
-// Lanes are the home cell's atoms (chunks of 32).  For each stencil
-// cell-image the warp stages up to 32 neighbour atoms in shared memory twice:
-// exact FP64 (double4 x,y,z,species) and FP32 coordinates relative to the
-// home cell's first atom with the image shift already applied in FP64.
-//
-//   phase A (FP32 pipe)  every lane tests all staged atoms with r² computed in
-//                        FP32 against c²·(1 + 2⁻¹⁰) and keeps a 32-bit mask;
-//   phase B (FP64 pipe)  only masked candidates are re-tested with the exact
-//                        reference arithmetic (NeighbourList/geometry.jl:5-19)
-//                        and, when r² < c², visited.
+// Lanes are the home cell's atoms (chunks of 32).  The warp first resolves up
+// to 32 stencil cell-images at once (one per lane: neighbour cell, image
+// shift, atom range) and concatenates their atoms into one flat list.  That
+// list is staged 32 atoms at a time in shared memory as packed FP32 pairs
+// relative to the home cell's first atom (each atom's image shift applied in
+// FP64 first), and each lane runs the candidate test on two neighbours per
+// packed instruction (__ffma2_rn) against c²·(1 + 2⁻¹⁰).  Survivors are
+// appended to the lane's own list; when any list could overflow, or at the
+// end of a stencil block, the lists are drained: each lane walks its list,
+// re-tests with the exact reference arithmetic
+// (NeighbourList/geometry.jl:5-19) and calls visit for pairs with r² < c².
 //
 // The FP32 test can only reject pairs whose exact r² exceeds c²: with
 // coordinates relative to a point at most R away, |r²₃₂ - r²| ≤ c²·(4e-7·R/c
-// + 2e-7), far inside the 2⁻¹⁰ guard for any R < 1000 c.  So the visited set
-// is exactly the reference's.  visit(i, j, pi, pj, se, d) runs on the lane
-// owning sorted atom i, in a fixed order (stencil entry, then the neighbour
-// cell's sorted order).
+// + 2e-7), far inside the 2⁻¹⁰ guard for any R < 1000 c.  The visited set is
+// therefore exactly the reference's, and visit(i, j, pi, pj, se, d, r2) runs
+// on the lane owning sorted atom i in a fixed order (stencil entry, then the
+// neighbour cell's sorted order).
 #pragma once
 #include "pfw_common.cuh"
 
 namespace pfw {
 
-// Compile-time tuning knobs (both variants are exact):
-//   PFW_PREFILTER       1: FP32 guard-band prefilter before the exact test
-//   PFW_PHASEA_DYNAMIC  1: prefilter loop bounded by the staged count
-#ifndef PFW_PREFILTER
-#define PFW_PREFILTER 1
-#endif
-#ifndef PFW_PHASEA_DYNAMIC
-#define PFW_PHASEA_DYNAMIC 1
-#endif
-
 constexpr int TRAVERSE_STAGE = 32;
+constexpr int LIST_K = 64;   // list capacity per lane
+constexpr int LIST_NE = 32;  // stencil entries per block (one per lane)
 constexpr float PREFILTER_GUARD = 1.0f + 1.0f / 1024.0f;
 
+#ifndef PFW_DRAIN_UNROLL
+#define PFW_DRAIN_UNROLL 1
+#endif
+
 struct WarpStage {
-  double4 p64[TRAVERSE_STAGE];
-  float4 p32[TRAVERSE_STAGE];
+  float2 x2[TRAVERSE_STAGE / 2], y2[TRAVERSE_STAGE / 2], z2[TRAVERSE_STAGE / 2];
+  int sj[TRAVERSE_STAGE];           // staged atom: sorted index
+  int sk[TRAVERSE_STAGE];           // staged atom: stencil entry slot
+  int start[LIST_NE + 1];           // flat-list offsets of the entries
+  StencilEntry ent[LIST_NE];
+  unsigned int list[LIST_K][32];    // [slot][lane]: j | entry << 24
 };
+
+// Walk the lane's list: PFW_DRAIN_UNROLL neighbour loads are issued before
+// any of them is used, so their latencies overlap.
+template <int MODE, class Visit>
+__device__ __forceinline__ void drain_lists(const SysGeom& g, const double4* __restrict__ pos, WarpStage& stage,
+                                            int lane, bool have, int i, const double4& pi, int& cnt, Visit& visit) {
+  constexpr int U = PFW_DRAIN_UNROLL;
+  __syncwarp();
+  if (have) {
+    for (int q0 = 0; q0 < cnt; q0 += U) {
+      unsigned item[U];
+      double4 pj[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        item[u] = stage.list[min(q0 + u, cnt - 1)][lane];
+        pj[u] = pos[item[u] & 0xFFFFFFu];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (q0 + u >= cnt) break;
+        const int j = (int)(item[u] & 0xFFFFFFu);
+        const StencilEntry& se = stage.ent[item[u] >> 24];
+        double d[3];
+        if (MODE == 0) {
+          d[0] = xadd(xsub(pj[u].x, pi.x), se.sh[0]);
+          d[1] = xadd(xsub(pj[u].y, pi.y), se.sh[1]);
+          d[2] = xadd(xsub(pj[u].z, pi.z), se.sh[2]);
+        } else {
+          displacement(g, se, pi.x, pi.y, pi.z, pj[u].x, pj[u].y, pj[u].z, d);
+        }
+        const double r2 = xr2(d[0], d[1], d[2]);
+        if (r2 < g.c2) visit(i, j, pi, pj[u], se, d, r2);
+      }
+    }
+  }
+  cnt = 0;
+  __syncwarp();
+}
 
 template <int MODE, class Visit>
 __device__ __forceinline__ void warp_traverse_cell(const SysGeom& g, int cell, const int* __restrict__ cell_start,
@@ -49,73 +88,115 @@ __device__ __forceinline__ void warp_traverse_cell(const SysGeom& g, int cell, c
   const int local = cell - g.cell_begin;
   const int key[3] = {local / (g.dims[1] * g.dims[2]), (local / g.dims[2]) % g.dims[1], local % g.dims[2]};
   const int cnt0 = stencil_count(g, 0), cnt1 = stencil_count(g, 1), cnt2 = stencil_count(g, 2);
-  const double c2 = g.c2;
-  const float c2hi = (float)c2 * PREFILTER_GUARD;
+  const int nstencil = cnt0 * cnt1 * cnt2;
+  const float c2hi = (float)g.c2 * PREFILTER_GUARD;
   const double4 ref = pos[b];
   for (int i0 = b; i0 < e; i0 += 32) {
     const int i = i0 + lane;
     const bool have = i < e;
     const double4 pi = have ? pos[i] : ref;
-    const float xi = (float)(pi.x - ref.x), yi = (float)(pi.y - ref.y), zi = (float)(pi.z - ref.z);
-    for (int t0 = 0; t0 < cnt0; ++t0)
-      for (int t1 = 0; t1 < cnt1; ++t1)
-        for (int t2 = 0; t2 < cnt2; ++t2) {
+    const float2 nx = make_float2(-(float)(pi.x - ref.x), -(float)(pi.x - ref.x));
+    const float2 ny = make_float2(-(float)(pi.y - ref.y), -(float)(pi.y - ref.y));
+    const float2 nz = make_float2(-(float)(pi.z - ref.z), -(float)(pi.z - ref.z));
+    int cnt = 0;
+    for (int s0 = 0; s0 < nstencil; s0 += LIST_NE) {
+      // ---- resolve up to 32 stencil entries, one per lane ----
+      __syncwarp();
+      int len = 0, jb = 0;
+      {
+        const int k = s0 + lane;
+        StencilEntry se;
+        se.cell = -1;
+        if (k < nstencil) {
+          const int t0 = k / (cnt1 * cnt2), t1 = (k / cnt2) % cnt1, t2 = k % cnt2;
           const int off[3] = {stencil_offset(g, 0, t0), stencil_offset(g, 1, t1), stencil_offset(g, 2, t2)};
-          StencilEntry se;
           stencil_entry(g, key, off, se);
-          if (se.cell < 0) continue;
-          const int jb = cell_start[se.cell], je = cell_start[se.cell + 1];
-          for (int j0 = jb; j0 < je; j0 += TRAVERSE_STAGE) {
-            const int nj = min(TRAVERSE_STAGE, je - j0);
-            __syncwarp();
-            if (lane < nj) {
-              const double4 q = pos[j0 + lane];
-              stage.p64[lane] = q;
-              if (MODE == 0)
-                stage.p32[lane] = make_float4((float)((q.x + se.sh[0]) - ref.x), (float)((q.y + se.sh[1]) - ref.y),
-                                              (float)((q.z + se.sh[2]) - ref.z), 0.f);
-            } else if (MODE == 0) {
-              stage.p32[lane] = make_float4(1e30f, 1e30f, 1e30f, 0.f);
-            }
-            __syncwarp();
-            if (!have) continue;
-            unsigned mask;
-            if (MODE == 0 && PFW_PREFILTER) {
-              mask = 0u;
-#if PFW_PHASEA_DYNAMIC
-#pragma unroll 4
-              for (int t = 0; t < nj; ++t) {
-#else
-#pragma unroll
-              for (int t = 0; t < TRAVERSE_STAGE; ++t) {
-#endif
-                const float4 q = stage.p32[t];
-                const float dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                mask |= (r2 < c2hi ? 1u : 0u) << t;
-              }
-            } else {
-              mask = nj == 32 ? 0xffffffffu : ((1u << nj) - 1u);
-            }
-            while (mask) {
-              const int t = __ffs(mask) - 1;
-              mask &= mask - 1u;
-              const int j = j0 + t;
-              if (se.zero && j == i) continue;
-              const double4 pj = stage.p64[t];
-              double d[3];
-              if (MODE == 0) {
-                d[0] = xadd(xsub(pj.x, pi.x), se.sh[0]);
-                d[1] = xadd(xsub(pj.y, pi.y), se.sh[1]);
-                d[2] = xadd(xsub(pj.z, pi.z), se.sh[2]);
-              } else {
-                displacement(g, se, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, d);
-              }
-              const double r2 = xr2(d[0], d[1], d[2]);
-              if (r2 < c2) visit(i, j, pi, pj, se, d, r2);
-            }
+          if (se.cell >= 0) {
+            jb = cell_start[se.cell];
+            len = cell_start[se.cell + 1] - jb;
           }
         }
+        stage.ent[lane] = se;
+      }
+      int incl = len;  // inclusive warp scan of the entry lengths
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      stage.start[lane] = incl - len;
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      if (lane == 31) stage.start[32] = total;
+      const int jb_lane = jb;
+      __syncwarp();
+      // ---- stage the flat list 32 atoms at a time ----
+      for (int f0 = 0; f0 < total; f0 += TRAVERSE_STAGE) {
+        const int nj = min(TRAVERSE_STAGE, total - f0);
+        __syncwarp();
+        {
+          float px = 1e30f, py = 1e30f, pz = 1e30f;
+          int jj = -1, kk = 0;
+          if (lane < nj) {
+            const int f = f0 + lane;
+            int lo = 0, hi = 31;  // last entry with start <= f
+            while (lo < hi) {
+              const int mid = (lo + hi + 1) >> 1;
+              if (stage.start[mid] <= f) lo = mid;
+              else hi = mid - 1;
+            }
+            kk = lo;
+          }
+          // atom index of the flat position: entry kk's first atom + offset
+          const int jbk = __shfl_sync(0xffffffffu, jb_lane, kk);
+          if (lane < nj) {
+            jj = jbk + (f0 + lane - stage.start[kk]);
+            if (MODE == 0) {
+              const double4 q = pos[jj];
+              const StencilEntry& se = stage.ent[kk];
+              px = (float)((q.x + se.sh[0]) - ref.x);
+              py = (float)((q.y + se.sh[1]) - ref.y);
+              pz = (float)((q.z + se.sh[2]) - ref.z);
+            }
+          }
+          if (MODE == 0) {
+            reinterpret_cast<float*>(stage.x2)[lane] = px;
+            reinterpret_cast<float*>(stage.y2)[lane] = py;
+            reinterpret_cast<float*>(stage.z2)[lane] = pz;
+          }
+          stage.sj[lane] = jj;
+          stage.sk[lane] = kk;
+        }
+        __syncwarp();
+        unsigned mask;
+        if (MODE == 0) {
+          mask = 0u;
+          const float2 lim = make_float2(c2hi, c2hi);
+          const int npair = (nj + 1) >> 1;
+#pragma unroll 4
+          for (int u = 0; u < npair; ++u) {
+            const float2 dx = __fadd2_rn(stage.x2[u], nx);
+            const float2 dy = __fadd2_rn(stage.y2[u], ny);
+            const float2 dz = __fadd2_rn(stage.z2[u], nz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            mask |= ((r2.x < lim.x ? 1u : 0u) | (r2.y < lim.y ? 2u : 0u)) << (2 * u);
+          }
+        } else {
+          mask = nj == 32 ? 0xffffffffu : ((1u << nj) - 1u);
+        }
+        if (!have) mask = 0u;
+        while (mask) {
+          const int t = __ffs(mask) - 1;
+          mask &= mask - 1u;
+          const int j = stage.sj[t], k = stage.sk[t];
+          if (j == i && stage.ent[k].zero) continue;  // the zero-shift self pair
+          stage.list[cnt++][lane] = (unsigned)j | ((unsigned)k << 24);
+        }
+        if (__reduce_max_sync(0xffffffffu, cnt) > LIST_K - TRAVERSE_STAGE)
+          drain_lists<MODE>(g, pos, stage, lane, have, i, pi, cnt, visit);
+      }
+      // entries are reused by the next block: drain what refers to them
+      drain_lists<MODE>(g, pos, stage, lane, have, i, pi, cnt, visit);
+    }
   }
 }
 

@@ -76,6 +76,7 @@ def load():
     L.pfw_pair_model_smooth.argtypes = [vp, C.c_int32, dp, C.c_double]
     L.pfw_pair_model_lj.argtypes = [vp, C.c_double, C.c_double, C.c_double]
     L.pfw_ace_model_load.argtypes = [vp, C.POINTER(pfw_ace_tables)]
+    L.pfw_ace_set_schedule.argtypes = [vp, C.c_int32, C.c_int32]
     L.pfw_evaluate.argtypes = [vp, C.c_int32, C.c_uint32, dp, dp, dp]
     L.pfw_evaluate_device.argtypes = [vp, C.c_int32, C.c_uint32, vp, vp, vp]
     L.pfw_site_energies.argtypes = [vp, dp]
@@ -154,6 +155,9 @@ class Handle:
         self._ace_tables = packed.tables()
         self._ace_packed = packed
         self.check(self.L.pfw_ace_model_load(self.ws, C.byref(self._ace_tables)))
+
+    def ace_schedule(self, chunk=0, groups=0):
+        self.check(self.L.pfw_ace_set_schedule(self.ws, int(chunk), int(groups)))
 
     def evaluate(self, model=MODEL_PAIR, request=7):
         E = np.zeros(1)
