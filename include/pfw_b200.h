@@ -168,6 +168,50 @@ pfw_status pfw_last_pair_count(pfw_ws* ws, int64_t* npairs);
 pfw_status pfw_neighbour_count(pfw_ws* ws, double cutoff, int64_t* total);
 pfw_status pfw_neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);
 
+/* ---- batches of independent systems ------------------------------------ */
+/* Replaces a loop of evaluate! / energy_forces_virial calls over independent
+ * structures, such as the training set of design_matrix (ACE/fitting.jl:18-67),
+ * with one launch over all of them.  nsys systems; their atoms are
+ * concatenated system after system: system s owns atoms
+ * [atom_offsets[s], atom_offsets[s+1]) (atom_offsets[0] = 0, nsys+1 entries).
+ * H holds 9 doubles per system (column-major, columns = cell vectors), pbc 3
+ * flags per system.  X (3×N) and species (N) are host arrays for
+ * pfw_set_batch and device arrays for pfw_set_batch_device; offsets, H and
+ * pbc are always host arrays.  Replaces the single-system geometry. */
+pfw_status pfw_set_batch(pfw_ws* ws, int32_t nsys, const int64_t* atom_offsets, const double* X,
+                         const double* H, const uint8_t* pbc, const int32_t* species);
+pfw_status pfw_set_batch_device(pfw_ws* ws, int32_t nsys, const int64_t* atom_offsets, const double* X_dev,
+                                const double* H, const uint8_t* pbc, const int32_t* species_dev);
+/* New positions (3×N, same systems, cells and species) for the next
+ * evaluation; on_device != 0: X is device memory (queued, no sync).  A
+ * captured batch graph stays valid. */
+pfw_status pfw_batch_update_positions(pfw_ws* ws, const double* X, int32_t on_device);
+/* Per-structure fitting features of the loaded ACE model: nz·(nB + nQ)
+ * values per system, laid out [Σ_i B_i of species block z (nB each, z =
+ * 0..nz-1), then Σ_{i,j} Q[j,:] of species block z (nQ each)] — the energy
+ * row of design_matrix (ACE/fitting.jl:28-29) without the reference
+ * energies. */
+pfw_status pfw_ace_feature_count(pfw_ws* ws, int32_t* nfeat);
+/* Batch evaluation.  E: nsys, F: 3×N (original order), W: 9 per system,
+ * features: nfeat per system (ACE only; NULL skips them).  Any output may be
+ * NULL when not requested.  Host outputs, synchronous. */
+pfw_status pfw_evaluate_batch(pfw_ws* ws, int32_t model, uint32_t request, double* E, double* F,
+                              double* W, double* features);
+/* Same with DEVICE outputs; still checks device status before returning. */
+pfw_status pfw_evaluate_batch_device(pfw_ws* ws, int32_t model, uint32_t request, double* E_dev,
+                                     double* F_dev, double* W_dev, double* features_dev);
+/* ACE batch through a CUDA graph: the first call (and any call after the
+ * batch, model, schedule, request or output pointers changed) evaluates
+ * eagerly to plan, sizes the environment buffers with 25 % headroom and
+ * captures cell lists + environments + site kernel + force gather + per-system
+ * outputs as one graph on the workspace stream; every call then launches the
+ * graph and returns without synchronising.  Requires fully periodic systems.
+ * pfw_batch_graph_sync waits and reports device status: PFW_ECAPACITY when
+ * moved positions outgrew the headroom (call again: it re-plans). */
+pfw_status pfw_batch_graph_launch(pfw_ws* ws, uint32_t request, double* E_dev, double* F_dev,
+                                  double* W_dev, double* features_dev);
+pfw_status pfw_batch_graph_sync(pfw_ws* ws);
+
 /* ---- device peak probe ------------------------------------------------- */
 /* Measured FP64 FMA throughput of the current device (TFLOP/s), used as the
  * FP64-pipe roofline denominator. */

@@ -10,10 +10,15 @@
 //                 CSR over sorted centres; edge displacement X_j - X_i + H·S
 //                 from the ORIGINAL coordinates (environments.jl:97-102)
 //   k_edge_rev    index of the reverse edge (j→i, -S) of every edge
-//   k_ace_sites   persistent site kernel (ace_site.cuh)
+//   k_ace_sites   persistent site kernel (ace_site.cuh) over work units (one
+//                 site, or one system of a batch)
 //   k_ace_gather  F_k = Σ_{e∈out(k)} g_e - g_{rev(e)}  (reduce_site!,
 //                 NeighbourList/execution.jl:256-273, without a racing scatter)
 //   k_ace_reduce  E and the 3×3 virial from per-site partials
+//
+// Batches of systems evaluate with one unit per system, so energies, virials
+// and the per-structure fitting features (ACE/fitting.jl:28-29) come out per
+// system; the batch path can be captured once as a CUDA graph and replayed.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -25,6 +30,19 @@
 
 namespace pfw {
 
+// What a captured batch graph was recorded for.
+struct GraphKey {
+  uint64_t geometry_version = ~0ull;
+  uint64_t alloc_epoch = ~0ull;
+  const void *E = nullptr, *F = nullptr, *W = nullptr, *feat = nullptr;
+  uint32_t req = 0;
+  int chunk = 0, groups = 0, precision = 0;
+  bool operator==(const GraphKey& o) const {
+    return geometry_version == o.geometry_version && alloc_epoch == o.alloc_epoch && E == o.E && F == o.F && W == o.W && feat == o.feat &&
+           req == o.req && chunk == o.chunk && groups == o.groups && precision == o.precision;
+  }
+};
+
 struct AceDevice {
   int nz = 0, lmax = 0, nY = 0, nR = 0, nQ = 0, D = 0, P = 0, T = 0, nB = 0, max_order = 0;
   double cutoff = 0;
@@ -32,14 +50,20 @@ struct AceDevice {
   DevBuf r_len, r_nodes, r_coeff, r_tr, r_pow, r_envk, r_env;
   DevBuf q_len, q_nodes, q_coeff, q_tr, q_pow, q_envk, q_env;
   DevBuf density, dn_off, dn, dm_off, dm, prods, term_off, terms, weights, wpair, ref, pair_ok, Fnorm;
-  DevBuf c_rows, c_cols, c_vals;
-  int ncoupling = 0;
+  DevBuf crow_off, crow_k, crow_val;
   // per evaluation
   DevBuf edge_count, edge_off, edge_j, edge_d, edge_S, edge_rev, edge_g, site_out, site_E_orig, status;
+  DevBuf unit_begin, unit_out;
   int64_t nedges = 0;
+  int cap = 0;  // edge capacity of the buffers
   int n = 0;
   bool evaluated = false;
   int sched_chunk = 0, sched_groups = 0;  // 0: automatic
+  // captured batch evaluation
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  GraphKey graph_key{};
+  uint64_t graph_kernels = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -67,12 +91,13 @@ __global__ void __launch_bounds__(128)
   if (cur >= 0) count[cur] = cnt;
 }
 
+// Writes edges below `cap` only; an edge past the capacity sets status bit 8.
 template <int MODE>
 __global__ void __launch_bounds__(128)
     k_edge_fill(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
                 const double4* __restrict__ pos, const int* __restrict__ perm, const int* __restrict__ wind,
-                const double* __restrict__ X, int ncells, const int* __restrict__ off, int* __restrict__ ej,
-                int4* __restrict__ eS, double4* __restrict__ ed) {
+                const double* __restrict__ X, int ncells, const int* __restrict__ off, int cap, int* __restrict__ ej,
+                int4* __restrict__ eS, double4* __restrict__ ed, int* __restrict__ status) {
   __shared__ WarpStage stage[4];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * 4 + warp;
@@ -91,6 +116,11 @@ __global__ void __launch_bounds__(128)
                                wi[0] = wind[3 * a]; wi[1] = wind[3 * a + 1]; wi[2] = wind[3 * a + 2];
                                xi[0] = X[3 * a]; xi[1] = X[3 * a + 1]; xi[2] = X[3 * a + 2];
                              }
+                             if (o >= cap) {
+                               atomicOr(status, 8);
+                               ++o;
+                               return;
+                             }
                              const int b = perm[j];
                              const int wj[3] = {wind[3 * b], wind[3 * b + 1], wind[3 * b + 2]};
                              int S[3];
@@ -107,16 +137,18 @@ __global__ void __launch_bounds__(128)
 }
 
 // Reverse edge of e = (i→j, S): the entry (j→i, -S) of j's list.
-__global__ void k_edge_rev(int n, const int* __restrict__ off, const int* __restrict__ ej, const int4* __restrict__ eS,
-                           int* __restrict__ rev, int* __restrict__ status) {
+__global__ void k_edge_rev(int n, const int* __restrict__ off, int cap, const int* __restrict__ ej,
+                           const int4* __restrict__ eS, int* __restrict__ rev, int* __restrict__ status) {
   const int i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (i >= n) return;
-  for (int e = off[i] + lane; e < off[i + 1]; e += 32) {
+  const int e1 = min(off[i + 1], cap);
+  for (int e = min(off[i], cap) + lane; e < e1; e += 32) {
     const int j = ej[e];
     const int4 s = eS[e];
     int found = -1;
-    for (int f = off[j]; f < off[j + 1]; ++f) {
+    const int f1 = min(off[j + 1], cap);
+    for (int f = min(off[j], cap); f < f1; ++f) {
       if (ej[f] == i) {
         const int4 t = eS[f];
         if (t.x == -s.x && t.y == -s.y && t.z == -s.z) {
@@ -130,15 +162,14 @@ __global__ void k_edge_rev(int n, const int* __restrict__ off, const int* __rest
   }
 }
 
-
-
 // F_k = Σ_{e ∈ out(k)} g_e - g_rev(e), written in original order.
-__global__ void k_ace_gather(int n, const int* __restrict__ off, const int* __restrict__ rev,
+__global__ void k_ace_gather(int n, const int* __restrict__ off, int cap, const int* __restrict__ rev,
                              const double* __restrict__ g, const int* __restrict__ perm, double* __restrict__ F) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   double f0 = 0, f1 = 0, f2 = 0;
-  for (int e = off[k]; e < off[k + 1]; ++e) {
+  const int e1 = min(off[k + 1], cap);
+  for (int e = min(off[k], cap); e < e1; ++e) {
     const int r = rev[e];
     f0 += g[3 * (size_t)e] - g[3 * (size_t)r];
     f1 += g[3 * (size_t)e + 1] - g[3 * (size_t)r + 1];
@@ -176,6 +207,28 @@ __global__ void k_ace_reduce(int n, const double* __restrict__ site_out, const i
   }
 }
 
+__global__ void k_iota(int n, int* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k <= n) out[k] = k;
+}
+
+// Units of a batch: the sorted sites of system s start at its first cell.
+__global__ void k_system_units(int nsys, const SysGeom* __restrict__ sys, const int* __restrict__ cell_start,
+                               int n, int* __restrict__ unit_begin) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsys) unit_begin[s] = cell_start[sys[s].cell_begin];
+  if (s == 0) unit_begin[nsys] = n;
+}
+
+// Per-unit [E, W(9)] → caller layout E[s], W[9s..9s+8].
+__global__ void k_unit_outputs(int nunits, const double* __restrict__ unit_out, double* __restrict__ E,
+                               double* __restrict__ W) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nunits) return;
+  if (E) E[s] = unit_out[10 * (size_t)s];
+  if (W)
+    for (int k = 0; k < 9; ++k) W[9 * (size_t)s + k] = unit_out[10 * (size_t)s + 1 + k];
+}
 
 // ---------------------------------------------------------------------------
 // host
@@ -211,15 +264,24 @@ static RadialDev upload_family(const pfw_radial_family& f, int nz, DevBuf& len, 
   return d;
 }
 
+static void release_graph(AceDevice* a) {
+  if (a->graph_exec) cudaGraphExecDestroy(a->graph_exec);
+  if (a->graph) cudaGraphDestroy(a->graph);
+  a->graph_exec = nullptr;
+  a->graph = nullptr;
+  a->graph_key = GraphKey{};
+}
+
 void ace_free(pfw_ws* ws) {
   if (!ws->ace) return;
   AceDevice* a = ws->ace;
+  release_graph(a);
   DevBuf* bufs[] = {&a->r_len, &a->r_nodes, &a->r_coeff, &a->r_tr, &a->r_pow, &a->r_envk, &a->r_env,
                     &a->q_len, &a->q_nodes, &a->q_coeff, &a->q_tr, &a->q_pow, &a->q_envk, &a->q_env,
                     &a->density, &a->dn_off, &a->dn, &a->dm_off, &a->dm, &a->prods, &a->term_off, &a->terms,
-                    &a->weights, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm, &a->c_rows, &a->c_cols, &a->c_vals,
+                    &a->weights, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm, &a->crow_off, &a->crow_k, &a->crow_val,
                     &a->edge_count, &a->edge_off, &a->edge_j, &a->edge_d, &a->edge_S, &a->edge_rev, &a->edge_g,
-                    &a->site_out, &a->site_E_orig, &a->status};
+                    &a->site_out, &a->site_E_orig, &a->status, &a->unit_begin, &a->unit_out};
   for (auto* b : bufs) b->release();
   delete a;
   ws->ace = nullptr;
@@ -315,15 +377,31 @@ void ace_load(pfw_ws* ws, const pfw_ace_tables* t) {
   upload(a->prods, prods.data(), prods.size(), st);
   upload(a->term_off, toff.data(), toff.size(), st);
   upload(a->terms, terms.data(), terms.size(), st);
-  // precontracted weights w[z][k] = Σ_b C[b,k]·WB[z][b] (ACE/cpu.jl:265-268)
+  // precontracted weights w[z][k] = Σ_b C[b,k]·WB[z][b] (ACE/cpu.jl:265-268) and
+  // the coupling by invariant row (fitting features B = C·P)
   std::vector<double> wts((size_t)nz * a->P, 0.0);
-  for (int z = 0; z < nz; ++z)
+  std::vector<int> roff(a->nB + 1, 0);
+  for (int e = 0; e < t->ncoupling; ++e) {
+    const int r = t->coupling_rows[e], c = t->coupling_cols[e];
+    if (r < 0 || r >= a->nB || c < 0 || c >= a->P) throw Error(PFW_EINVAL, "invalid coupling entry");
+    roff[r + 1]++;
+    for (int z = 0; z < nz; ++z) wts[(size_t)z * a->P + c] += t->coupling_vals[e] * t->WB[(size_t)z * a->nB + r];
+  }
+  for (int b = 0; b < a->nB; ++b) roff[b + 1] += roff[b];
+  std::vector<int> rk(t->ncoupling);
+  std::vector<double> rv(t->ncoupling);
+  {
+    std::vector<int> fill(roff.begin(), roff.end() - 1);
     for (int e = 0; e < t->ncoupling; ++e) {
-      const int r = t->coupling_rows[e], c = t->coupling_cols[e];
-      if (r < 0 || r >= a->nB || c < 0 || c >= a->P) throw Error(PFW_EINVAL, "invalid coupling entry");
-      wts[(size_t)z * a->P + c] += t->coupling_vals[e] * t->WB[(size_t)z * a->nB + r];
+      const int q = fill[t->coupling_rows[e]]++;
+      rk[q] = t->coupling_cols[e];
+      rv[q] = t->coupling_vals[e];
     }
+  }
   upload(a->weights, wts.data(), wts.size(), st);
+  upload(a->crow_off, roff.data(), roff.size(), st);
+  upload(a->crow_k, rk.data(), rk.size(), st);
+  upload(a->crow_val, rv.data(), rv.size(), st);
   upload(a->wpair, t->Wpair, (size_t)nz * a->nQ, st);
   upload(a->ref, t->reference, nz, st);
   std::vector<int> pok(nz);
@@ -338,10 +416,6 @@ void ace_load(pfw_ws* ws, const pfw_ace_tables* t) {
     for (int m = 1; m <= l; ++m) F[l * (L + 1) + m] = -F[l * (L + 1) + m - 1] / std::sqrt((double)((l + m) * (l + 1 - m)));
   }
   upload(a->Fnorm, F.data(), F.size(), st);
-  upload(a->c_rows, t->coupling_rows, t->ncoupling, st);
-  upload(a->c_cols, t->coupling_cols, t->ncoupling, st);
-  upload(a->c_vals, t->coupling_vals, t->ncoupling, st);
-  a->ncoupling = t->ncoupling;
   PFW_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -356,6 +430,7 @@ static AceTables tables_of(AceDevice* a) {
   p.D = a->D;
   p.P = a->P;
   p.T = a->T;
+  p.nB = a->nB;
   p.prods = a->prods.as<ushort4>();
   p.term_off = a->term_off.as<int>();
   p.terms = a->terms.as<ushort4>();
@@ -365,6 +440,9 @@ static AceTables tables_of(AceDevice* a) {
   p.dm_off = a->dm_off.as<int>();
   p.dm = a->dm.as<int2>();
   p.weights = a->weights.as<double>();
+  p.crow_off = a->crow_off.as<int>();
+  p.crow_k = a->crow_k.as<int>();
+  p.crow_val = a->crow_val.as<double>();
   p.wpair = a->wpair.as<double>();
   p.ref = a->ref.as<double>();
   p.pair_ok = a->pair_ok.as<int>();
@@ -372,22 +450,22 @@ static AceTables tables_of(AceDevice* a) {
   return p;
 }
 
-// Largest working set that fits: two 128-thread groups with 32-edge chunks
-// when possible, else smaller chunks / one group.
-static AceLayout choose_layout(const AceTables& p, int device, int chunk, int groups) {
+// Largest working set that fits (or the tuned schedule): site groups of 128
+// threads per CTA and edges per chunk.
+static AceLayout choose_layout(const AceTables& p, int device, int chunk, int groups, int feat) {
   int optin = 0;
   PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   const size_t limit = (size_t)optin;
   if (chunk > 0) {
     AceLayout lay;
-    lay.make(p, chunk, groups);
-    if (lay.total > limit) throw Error(PFW_EINVAL, "ACE schedule does not fit in shared memory");
-    return lay;
+    lay.make(p, chunk, groups, feat);
+    if (lay.total <= limit) return lay;
+    if (!feat) throw Error(PFW_EINVAL, "ACE schedule does not fit in shared memory");
   }
   const int cand[][2] = {{32, 2}, {16, 3}, {16, 2}, {32, 1}, {16, 1}, {8, 1}};
   for (auto& c : cand) {
     AceLayout lay;
-    lay.make(p, c[0], c[1]);
+    lay.make(p, c[0], c[1], feat);
     if (lay.total <= limit) return lay;
   }
   throw Error(PFW_EINVAL, "ACE model too large for the site kernel's shared memory");
@@ -398,84 +476,178 @@ void ace_set_schedule(pfw_ws* ws, int chunk, int groups) {
   if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
   if (chunk == 0 && groups == 0) {
     a->sched_chunk = a->sched_groups = 0;
+    release_graph(a);
     return;
   }
   if (!(chunk == 8 || chunk == 16 || chunk == 32) || groups < 1 || groups > ACE_MAX_GROUPS)
     throw Error(PFW_EINVAL, "ACE schedule: chunk must be 8, 16 or 32 and groups 1..4");
-  choose_layout(tables_of(a), ws->opt.device, chunk, groups);  // validates the fit
+  choose_layout(tables_of(a), ws->opt.device, chunk, groups, 0);  // validates the fit
   a->sched_chunk = chunk;
   a->sched_groups = groups;
+  release_graph(a);
 }
 
+struct SiteLaunch {
+  int nunits;
+  const int* unit_begin;
+  int cap;
+  const int* off;
+  const double4* ed;
+  const double4* pos;
+  double* g;
+  double* unit_out;
+  double* unit_feat;
+  int want_grad;
+  int* status;
+};
+
 template <int L, class T>
-static void launch_sites(const AceTables& p, const AceLayout& lay, int n, cudaStream_t st, int device, const int* off,
-                         const double4* ed, const double4* pos, double* g, double* out, int want_grad, int* status) {
+static void launch_sites(const AceTables& p, const AceLayout& lay, const SiteLaunch& s, cudaStream_t st, int device) {
   auto kern = k_ace_sites<L, T>;
   PFW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total));
   int sms = 0, per_sm = 0;
   PFW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   PFW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ACE_GROUP * lay.G, lay.total));
   per_sm = std::max(per_sm, 1);
-  const int blocks = std::max(1, std::min(sms * per_sm, (n + lay.G - 1) / lay.G));
-  kern<<<blocks, ACE_GROUP * lay.G, lay.total, st>>>(p, lay, n, off, ed, pos, g, out, want_grad, status);
+  const int blocks = std::max(1, std::min(sms * per_sm, (s.nunits + lay.G - 1) / lay.G));
+  kern<<<blocks, ACE_GROUP * lay.G, lay.total, st>>>(p, lay, s.nunits, s.unit_begin, s.cap, s.off, s.ed, s.pos, s.g,
+                                                     s.unit_out, s.unit_feat, s.want_grad, s.status);
 }
 
-// Build the directed environments of the current geometry (sorted centres).
-static void build_edges(pfw_ws* ws, AceDevice* a) {
+template <class T>
+static void dispatch_sites(int lmax, const AceTables& p, const AceLayout& lay, const SiteLaunch& s, cudaStream_t st,
+                           int device) {
+  switch (lmax) {
+    case 0: launch_sites<0, T>(p, lay, s, st, device); break;
+    case 1: launch_sites<1, T>(p, lay, s, st, device); break;
+    case 2: launch_sites<2, T>(p, lay, s, st, device); break;
+    case 3: launch_sites<3, T>(p, lay, s, st, device); break;
+    case 4: launch_sites<4, T>(p, lay, s, st, device); break;
+    case 5: launch_sites<5, T>(p, lay, s, st, device); break;
+    default: launch_sites<6, T>(p, lay, s, st, device); break;
+  }
+}
+
+static bool shift_mode(const Prepared& P) {
+  for (auto& g : P.sys)
+    if (g.minimum_image && !g.fast_shift) return false;
+  return true;
+}
+
+// count + scan of the environments (no host synchronisation)
+static void edges_count_launch(pfw_ws* ws, AceDevice* a) {
   const Prepared& P = ws->prep;
   cudaStream_t st = ws->stream;
   const int n = P.n;
-  int* count = static_cast<int*>(a->edge_count.ensure(sizeof(int) * std::max(n, 1)));
-  int* off = static_cast<int*>(a->edge_off.ensure(sizeof(int) * (n + 1)));
+  int* count = a->edge_count.as<int>();
   PFW_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * std::max(n, 1), st));
-  bool shift = true;
-  for (auto& g : P.sys)
-    if (g.minimum_image && !g.fast_shift) shift = false;
   const dim3 grid(grid_for(P.ncells, 4)), block(128);
   if (P.ncells > 0) {
-    if (shift) k_edge_count<0><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(),
-                                                          ws->cell_start.as<int>(), ws->pos.as<double4>(), P.ncells, count);
-    else k_edge_count<1><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(),
-                                                   ws->cell_start.as<int>(), ws->pos.as<double4>(), P.ncells, count);
+    if (shift_mode(P))
+      k_edge_count<0><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(),
+                                              ws->cell_start.as<int>(), ws->pos.as<double4>(), P.ncells, count);
+    else
+      k_edge_count<1><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(),
+                                              ws->cell_start.as<int>(), ws->pos.as<double4>(), P.ncells, count);
     ws->launches += 1;
   }
-  exclusive_scan_i32(ws, count, off, n);
-  int total = 0;
-  PFW_CUDA(cudaMemcpyAsync(&total, off + n, sizeof(int), cudaMemcpyDeviceToHost, st));
-  PFW_CUDA(cudaStreamSynchronize(st));
-  a->nedges = total;
-  int* ej = static_cast<int*>(a->edge_j.ensure(sizeof(int) * std::max(total, 1)));
-  int4* eS = static_cast<int4*>(a->edge_S.ensure(sizeof(int4) * std::max(total, 1)));
-  double4* ed = static_cast<double4*>(a->edge_d.ensure(sizeof(double4) * std::max(total, 1)));
-  int* rev = static_cast<int*>(a->edge_rev.ensure(sizeof(int) * std::max(total, 1)));
-  int* status = static_cast<int*>(a->status.ensure(sizeof(int) * 4));
-  if (P.ncells > 0 && total > 0) {
-    if (shift)
+  exclusive_scan_i32(ws, count, a->edge_off.as<int>(), n);
+}
+
+// fill + reverse index up to the buffer capacity (no host synchronisation)
+static void edges_fill_launch(pfw_ws* ws, AceDevice* a) {
+  const Prepared& P = ws->prep;
+  cudaStream_t st = ws->stream;
+  const int n = P.n;
+  const dim3 grid(grid_for(P.ncells, 4)), block(128);
+  int* status = a->status.as<int>();
+  if (P.ncells > 0 && a->cap > 0) {
+    if (shift_mode(P))
       k_edge_fill<0><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(), ws->cell_start.as<int>(),
                                              ws->pos.as<double4>(), ws->perm.as<int>(), ws->wind.as<int>(),
-                                             ws->X.as<double>(), P.ncells, off, ej, eS, ed);
+                                             ws->X.as<double>(), P.ncells, a->edge_off.as<int>(), a->cap,
+                                             a->edge_j.as<int>(), a->edge_S.as<int4>(), a->edge_d.as<double4>(), status);
     else
       k_edge_fill<1><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(), ws->cell_start.as<int>(),
                                              ws->pos.as<double4>(), ws->perm.as<int>(), ws->wind.as<int>(),
-                                             ws->X.as<double>(), P.ncells, off, ej, eS, ed);
-    k_edge_rev<<<grid_for(n, 4), 128, 0, st>>>(n, off, ej, eS, rev, status);
+                                             ws->X.as<double>(), P.ncells, a->edge_off.as<int>(), a->cap,
+                                             a->edge_j.as<int>(), a->edge_S.as<int4>(), a->edge_d.as<double4>(), status);
+    k_edge_rev<<<grid_for(n, 4), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_j.as<int>(),
+                                               a->edge_S.as<int4>(), a->edge_rev.as<int>(), status);
     ws->launches += 2;
   }
 }
 
-template <class T>
-static void dispatch_sites(int lmax, const AceTables& p, const AceLayout& lay, int n, cudaStream_t st, int device,
-                           const int* off, const double4* ed, const double4* pos, double* g, double* out,
-                           int want_grad, int* status) {
-  switch (lmax) {
-    case 0: launch_sites<0, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
-    case 1: launch_sites<1, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
-    case 2: launch_sites<2, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
-    case 3: launch_sites<3, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
-    case 4: launch_sites<4, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
-    case 5: launch_sites<5, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
-    default: launch_sites<6, T>(p, lay, n, st, device, off, ed, pos, g, out, want_grad, status); break;
+static void ensure_edge_buffers(AceDevice* a, int cap) {
+  a->cap = cap;
+  a->edge_j.ensure(sizeof(int) * std::max(cap, 1));
+  a->edge_S.ensure(sizeof(int4) * std::max(cap, 1));
+  a->edge_d.ensure(sizeof(double4) * std::max(cap, 1));
+  a->edge_rev.ensure(sizeof(int) * std::max(cap, 1));
+  a->edge_g.ensure(sizeof(double) * 3 * std::max(cap, 1));
+}
+
+// Eager environments: count, read the total back, size the buffers, fill.
+static void build_edges(pfw_ws* ws, AceDevice* a) {
+  const int n = ws->prep.n;
+  a->edge_count.ensure(sizeof(int) * std::max(n, 1));
+  a->edge_off.ensure(sizeof(int) * (n + 1));
+  a->status.ensure(sizeof(int) * 4);
+  edges_count_launch(ws, a);
+  int total = 0;
+  PFW_CUDA(cudaMemcpyAsync(&total, a->edge_off.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, ws->stream));
+  PFW_CUDA(cudaStreamSynchronize(ws->stream));
+  a->nedges = total;
+  ensure_edge_buffers(a, total);
+  edges_fill_launch(ws, a);
+}
+
+// Site kernel, force gather and the per-unit outputs (no host synchronisation).
+static void sites_launch(pfw_ws* ws, AceDevice* a, uint32_t req, int nunits, const AceLayout& lay, double* F_dev,
+                         double* feat) {
+  cudaStream_t st = ws->stream;
+  const int n = ws->prep.n;
+  const bool want_grad = (req & (PFW_REQ_FORCES | PFW_REQ_VIRIAL)) != 0;
+  const AceTables p = tables_of(a);
+  SiteLaunch s;
+  s.nunits = nunits;
+  s.unit_begin = a->unit_begin.as<int>();
+  s.cap = a->cap;
+  s.off = a->edge_off.as<int>();
+  s.ed = a->edge_d.as<double4>();
+  s.pos = ws->pos.as<double4>();
+  s.g = a->edge_g.as<double>();
+  s.unit_out = a->unit_out.as<double>();
+  s.unit_feat = feat;
+  s.want_grad = want_grad;
+  s.status = a->status.as<int>();
+  ws->stage_begin(1);
+  if (nunits > 0) {
+    if (ws->opt.precision == PFW_PRECISION_MIXED) dispatch_sites<float>(a->lmax, p, lay, s, st, ws->opt.device);
+    else dispatch_sites<double>(a->lmax, p, lay, s, st, ws->opt.device);
+    ws->launches += 1;
   }
+  ws->stage_end(1);
+  ws->stage_begin(2);
+  if (F_dev && n > 0) {
+    if (want_grad) {
+      k_ace_gather<<<grid_for(n, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(), s.g,
+                                                     ws->perm.as<int>(), F_dev);
+      ws->launches += 1;
+    } else {
+      PFW_CUDA(cudaMemsetAsync(F_dev, 0, sizeof(double) * 3 * n, st));
+    }
+  }
+}
+
+static void ace_check(pfw_ws* ws, AceDevice* a) {
+  int hs[4];
+  PFW_CUDA(cudaMemcpyAsync(hs, a->status.ptr, sizeof(hs), cudaMemcpyDeviceToHost, ws->stream));
+  PFW_CUDA(cudaStreamSynchronize(ws->stream));
+  PFW_CUDA(cudaGetLastError());
+  if (hs[0] & 2) throw Error(PFW_EDOMAIN, "coincident physical atoms have undefined harmonics / pair envelope");
+  if (hs[0] & 8) throw Error(PFW_ECAPACITY, "neighbour environments outgrew the planned capacity; re-plan");
+  if (hs[0] & 4) throw Error(PFW_EINVAL, "internal: reverse edge not found");
 }
 
 void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev) {
@@ -488,52 +660,136 @@ void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   ws->stage_begin(0);
   prepare(ws, a->cutoff);
   ws->stage_end(0);
-  int* status = static_cast<int*>(a->status.ensure(sizeof(int) * 4));
-  PFW_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, st));
+  a->status.ensure(sizeof(int) * 4);
+  PFW_CUDA(cudaMemsetAsync(a->status.ptr, 0, sizeof(int) * 4, st));
   build_edges(ws, a);
   ws->stage_end(3);
   const int n = ws->prep.n;
   a->n = n;
-  const bool want_grad = (req & (PFW_REQ_FORCES | PFW_REQ_VIRIAL)) != 0;
-  double* g = static_cast<double*>(a->edge_g.ensure(sizeof(double) * 3 * std::max<int64_t>(a->nedges, 1)));
-  double* out = static_cast<double*>(a->site_out.ensure(sizeof(double) * 10 * std::max(n, 1)));
+  // one unit per site: unit_out holds the site partials
+  int* ub = static_cast<int*>(a->unit_begin.ensure(sizeof(int) * (n + 1)));
+  a->unit_out.ensure(sizeof(double) * 10 * std::max(n, 1));
   double* Esite = static_cast<double*>(a->site_E_orig.ensure(sizeof(double) * std::max(n, 1)));
-  const AceTables p = tables_of(a);
-  const AceLayout lay = choose_layout(p, ws->opt.device, a->sched_chunk, a->sched_groups);
-  ws->stage_begin(1);
-  if (n > 0) {
-    const int* off = a->edge_off.as<int>();
-    const double4* ed = a->edge_d.as<double4>();
-    const double4* pos = ws->pos.as<double4>();
-    if (ws->opt.precision == PFW_PRECISION_MIXED)
-      dispatch_sites<float>(a->lmax, p, lay, n, st, ws->opt.device, off, ed, pos, g, out, want_grad, status);
-    else
-      dispatch_sites<double>(a->lmax, p, lay, n, st, ws->opt.device, off, ed, pos, g, out, want_grad, status);
-    ws->launches += 1;
-  }
-  ws->stage_end(1);
-  ws->stage_begin(2);
-  if (F_dev && n > 0) {
-    if (want_grad) {
-      k_ace_gather<<<grid_for(n, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->edge_rev.as<int>(), g,
-                                                     ws->perm.as<int>(), F_dev);
-      ws->launches += 1;
-    } else {
-      PFW_CUDA(cudaMemsetAsync(F_dev, 0, sizeof(double) * 3 * n, st));
-    }
-  }
+  k_iota<<<grid_for(n + 1, 256), 256, 0, st>>>(n, ub);
+  ws->launches += 1;
+  const AceLayout lay = choose_layout(tables_of(a), ws->opt.device, a->sched_chunk, a->sched_groups, 0);
+  sites_launch(ws, a, req, n, lay, F_dev, nullptr);
   double* E = E_dev ? E_dev : static_cast<double*>(ws->out_E.ensure(sizeof(double)));
   double* W = W_dev ? W_dev : static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
-  k_ace_reduce<<<1, 256, 0, st>>>(n, out, ws->perm.as<int>(), E, W, Esite);
+  k_ace_reduce<<<1, 256, 0, st>>>(n, a->unit_out.as<double>(), ws->perm.as<int>(), E, W, Esite);
   ws->launches += 1;
   ws->stage_end(2);
   a->evaluated = true;
-  int hs[4];
-  PFW_CUDA(cudaMemcpyAsync(hs, status, sizeof(hs), cudaMemcpyDeviceToHost, st));
-  PFW_CUDA(cudaStreamSynchronize(st));
-  PFW_CUDA(cudaGetLastError());
-  if (hs[0] & 2) throw Error(PFW_EDOMAIN, "coincident physical atoms have undefined harmonics / pair envelope");
-  if (hs[0] & 4) throw Error(PFW_EINVAL, "internal: reverse edge not found");
+  ace_check(ws, a);
+}
+
+int ace_feature_count(pfw_ws* ws) {
+  AceDevice* a = ws->ace;
+  if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
+  return a->nz * (a->nB + a->nQ);
+}
+
+// Batch of systems, one unit per system.  Eager: plan, build, evaluate.
+void ace_evaluate_batch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev) {
+  AceDevice* a = ws->ace;
+  if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
+  if (ws->max_species >= a->nz) throw Error(PFW_EINVAL, "ACE model has no element channel for a species");
+  cudaStream_t st = ws->stream;
+  ws->prep.valid = false;
+  prepare(ws, a->cutoff);
+  a->status.ensure(sizeof(int) * 4);
+  PFW_CUDA(cudaMemsetAsync(a->status.ptr, 0, sizeof(int) * 4, st));
+  build_edges(ws, a);
+  const int nsys = ws->prep.nsys, n = ws->prep.n;
+  a->n = n;
+  int* ub = static_cast<int*>(a->unit_begin.ensure(sizeof(int) * (nsys + 1)));
+  a->unit_out.ensure(sizeof(double) * 10 * std::max(nsys, 1));
+  const bool feat = feat_dev != nullptr;
+  k_system_units<<<grid_for(nsys + 1, 128), 128, 0, st>>>(nsys, ws->sysgeom.as<SysGeom>(), ws->cell_start.as<int>(), n, ub);
+  const AceLayout lay = choose_layout(tables_of(a), ws->opt.device, a->sched_chunk, a->sched_groups, feat);
+  sites_launch(ws, a, req, nsys, lay, F_dev, feat_dev);
+  k_unit_outputs<<<grid_for(nsys, 128), 128, 0, st>>>(nsys, a->unit_out.as<double>(), E_dev, W_dev);
+  ws->launches += 2;
+  ws->stage_end(2);
+  ace_check(ws, a);
+}
+
+// Batch evaluation replayed from a CUDA graph.  The first call (or a call
+// after the batch, model, schedule or outputs changed) plans with an eager
+// run, sizes the environment buffers with 25 % headroom and captures the
+// device-only sequence — cell-list build, environments, site kernel, force
+// gather, per-system outputs — on the workspace stream; later calls launch
+// the graph.  Positions may change between replays (pfw_batch_update_positions):
+// an environment that outgrows the headroom raises PFW_ECAPACITY at the next
+// pfw_batch_graph_sync.
+void ace_batch_graph(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev) {
+  AceDevice* a = ws->ace;
+  if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
+  GraphKey key;
+  key.geometry_version = ws->geometry_version;
+  key.alloc_epoch = g_alloc_epoch.load();
+  key.E = E_dev;
+  key.F = F_dev;
+  key.W = W_dev;
+  key.feat = feat_dev;
+  key.req = req;
+  key.chunk = a->sched_chunk;
+  key.groups = a->sched_groups;
+  key.precision = ws->opt.precision;
+  cudaStream_t st = ws->stream;
+  if (!a->graph_exec || !(a->graph_key == key)) {
+    release_graph(a);
+    for (const auto& hs : ws->systems)
+      if (!hs.pbc[0] || !hs.pbc[1] || !hs.pbc[2])
+        throw Error(PFW_EINVAL, "graph batches require fully periodic systems");
+    ace_evaluate_batch(ws, req, E_dev, F_dev, W_dev, feat_dev);  // plan and validate
+    ensure_edge_buffers(a, (int)std::min<int64_t>((int64_t)(a->nedges * 1.25) + 4096, INT32_MAX / 4));
+    const int nsys = ws->prep.nsys, n = ws->prep.n;
+    const bool feat = feat_dev != nullptr;
+    const AceLayout lay = choose_layout(tables_of(a), ws->opt.device, a->sched_chunk, a->sched_groups, feat);
+    const bool diag = ws->diag;
+    ws->diag = false;
+    const uint64_t launches0 = ws->launches;
+    PFW_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      PFW_CUDA(cudaMemsetAsync(a->status.ptr, 0, sizeof(int) * 4, st));
+      prepare_launch(ws, true);
+      edges_count_launch(ws, a);
+      edges_fill_launch(ws, a);
+      k_system_units<<<grid_for(nsys + 1, 128), 128, 0, st>>>(nsys, ws->sysgeom.as<SysGeom>(),
+                                                              ws->cell_start.as<int>(), n, a->unit_begin.as<int>());
+      sites_launch(ws, a, req, nsys, lay, F_dev, feat_dev);
+      k_unit_outputs<<<grid_for(nsys, 128), 128, 0, st>>>(nsys, a->unit_out.as<double>(), E_dev, W_dev);
+      ws->launches += 2;
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      ws->diag = diag;
+      throw;
+    }
+    PFW_CUDA(cudaStreamEndCapture(st, &a->graph));
+    ws->diag = diag;
+    a->graph_kernels = ws->launches - launches0;
+    ws->launches = launches0;
+    PFW_CUDA(cudaGraphInstantiate(&a->graph_exec, a->graph, 0));
+    a->graph_key = key;
+    a->graph_key.alloc_epoch = g_alloc_epoch.load();  // after the planning run's allocations
+  }
+  PFW_CUDA(cudaGraphLaunch(a->graph_exec, st));
+  ws->launches += a->graph_kernels;  // kernels replayed by the graph
+}
+
+void ace_batch_graph_sync(pfw_ws* ws) {
+  AceDevice* a = ws->ace;
+  if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
+  prepare_check(ws);
+  try {
+    ace_check(ws, a);
+  } catch (const Error& e) {
+    if (e.code == PFW_ECAPACITY) release_graph(a);  // the next launch re-plans
+    throw;
+  }
 }
 
 void ace_site_energies(pfw_ws* ws, double* host) {

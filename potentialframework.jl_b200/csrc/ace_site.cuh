@@ -37,6 +37,10 @@ struct AceTables {
   const int* dm_off;              // [nY+1]
   const int2* dm;                 // [D] (a, n)
   const double* weights;          // [nz][P]
+  int nB;                         // invariants (fitting features)
+  const int* crow_off;            // [nB+1] coupling rows (CSR)
+  const int* crow_k;              // product of each stored entry
+  const double* crow_val;         //   and its value
   const double* wpair;            // [nz][nQ]
   const double* ref;              // [nz]
   const int* pair_ok;             // [nz]
@@ -47,14 +51,18 @@ struct AceTables {
 struct AceLayout {
   int CH, G;
   int RS, YS;  // odd row strides of the per-edge R and Y tables (bank-conflict padding)
+  int feat;    // 1: per-unit fitting features are accumulated
+  int nfeat;   // nz * (nB + nQ)
   size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, tables_end;
   size_t group_bytes, total;
   // group-relative double offsets
-  int A, dA, Y, dY, R, dR, T1, T2, esc, ints;
+  int A, dA, Y, dY, R, dR, T1, T2, esc, F, QV, ints;
   __host__ __device__ static size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
-  __host__ __device__ void make(const AceTables& t, int ch, int g) {
+  __host__ __device__ void make(const AceTables& t, int ch, int g, int with_feat = 0) {
     CH = ch;
     G = g;
+    feat = with_feat;
+    nfeat = t.nz * (t.nB + t.nQ);
     size_t o = 0;
     prods = o; o = align16(o + sizeof(ushort4) * t.P);
     terms = o; o = align16(o + sizeof(ushort4) * t.T);
@@ -77,6 +85,8 @@ struct AceLayout {
     T1 = d; d += CH * RS;
     T2 = d; d += CH * YS;
     esc = d; d += CH * 10 + 4 * 10;  // per-edge scalars, then warp partials
+    F = d; d += feat ? nfeat : 0;     // unit feature accumulator
+    QV = d; d += feat ? CH * t.nQ : 0;  // pair radial values of the chunk
     ints = d; d += CH;               // 2 ints per edge
     group_bytes = align16(sizeof(double) * d);
     total = tables_end + group_bytes * G;
@@ -125,6 +135,7 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   } else if (q == 1) {
     double qe = 0.0;
     T qd = T(0);
+    double* qv = (!Grad && lay.feat) ? gbase + lay.QV + t * p.nQ : nullptr;
     if (p.nQ > 0 && p.pair_ok[zj]) {
       const EdgeRadial<T> eq = edge_radial<T>(p.Q, pidx, r);
       if (!eq.ok) atomicOr(status, 2);
@@ -134,7 +145,10 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
         channel_ed<T>(channel_coeff(p.Q, pidx, eq.k0, n), eq, v, dv);
         qe += (double)v * wp[n];
         qd += (T)wp[n] * dv;
+        if (qv) qv[n] = v;
       }
+    } else if (qv) {
+      for (int n = 0; n < p.nQ; ++n) qv[n] = 0.0;
     }
     if (!Grad) e_acc += qe;
     es.dq[t] = qd;
@@ -157,9 +171,10 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
 
 template <int L, class T>
 __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
-    k_ace_sites(AceTables p, AceLayout lay, int nsites, const int* __restrict__ edge_off,
-                const double4* __restrict__ edge_d, const double4* __restrict__ pos, double* __restrict__ edge_g,
-                double* __restrict__ site_out, int want_grad, int* __restrict__ status) {
+    k_ace_sites(AceTables p, AceLayout lay, int nunits, const int* __restrict__ unit_begin, int cap,
+                const int* __restrict__ edge_off, const double4* __restrict__ edge_d, const double4* __restrict__ pos,
+                double* __restrict__ edge_g, double* __restrict__ unit_out, double* __restrict__ unit_feat,
+                int want_grad, int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem[];
   // ---- stage the model tables once per CTA ----
   ushort4* s_prods = reinterpret_cast<ushort4*>(smem + lay.prods);
@@ -204,10 +219,19 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
   const int D = p.D, nY = p.nY, nR = p.nR, P = p.P, RS = lay.RS, YS = lay.YS;
   const int lane = lt & 31, wg = lt >> 5;
 
-  for (int s = blockIdx.x * lay.G + g; s < nsites; s += gridDim.x * lay.G) {
+  double* Facc = gb + lay.F;
+  const double* QVc = gb + lay.QV;
+  for (int unit = blockIdx.x * lay.G + g; unit < nunits; unit += gridDim.x * lay.G) {
+   double e_acc = 0.0;
+   double wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+   if (lay.feat) {
+     group_sync(g);
+     for (int k = lt; k < lay.nfeat; k += ACE_GROUP) Facc[k] = 0.0;
+   }
+   for (int s = unit_begin[unit]; s < unit_begin[unit + 1]; ++s) {
     const int iz = min(max((int)pos[s].w, 0), p.nz - 1);
-    const int eb = edge_off[s], E = edge_off[s + 1] - eb;
-    double e_acc = 0.0;
+    const int eb = min(edge_off[s], cap), E = min(edge_off[s + 1], cap) - eb;
+    if (lt == 0) e_acc += p.ref[iz];
     group_sync(g);
     for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? 1.0 : 0.0;
     // ---- pass 1: A-basis ----
@@ -216,6 +240,12 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
       group_sync(g);
       ace_chunk_edges<L, T, false>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, e_acc, status);
       group_sync(g);
+      if (lay.feat)  // Σ_j Q[j,n] of the centre's species block (fitting.jl:29)
+        for (int n = lt; n < p.nQ; n += ACE_GROUP) {
+          double acc = 0.0;
+          for (int t = 0; t < nc; ++t) acc += QVc[t * p.nQ + n];
+          Facc[p.nz * p.nB + iz * p.nQ + n] += acc;
+        }
       for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
         const int t = idx / nR, n = idx - t * nR;
         const double* c = channel_coeff(p.R, es.pidx[t], es.k0[t], n);
@@ -246,7 +276,15 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         }
         dA[a] = acc;
       }
-    double wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (lay.feat)  // B = C·P of the centre's species block (fitting.jl:28)
+      for (int b = lt; b < p.nB; b += ACE_GROUP) {
+        double acc = 0.0;
+        for (int q = p.crow_off[b]; q < p.crow_off[b + 1]; ++q) {
+          const ushort4 f = s_prods[p.crow_k[q]];
+          acc += p.crow_val[q] * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
+        }
+        Facc[iz * p.nB + b] += acc;
+      }
     // ---- pass 2: pullback ----
     if (want_grad) {
       for (int c0 = 0; c0 < E; c0 += CH) {
@@ -323,7 +361,8 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         }
       }
     }
-    // ---- site energy and virial (warp shuffles, then 4 warp partials) ----
+   }  // sites of the unit
+    // ---- unit energy and virial (warp shuffles, then 4 warp partials) ----
     double vals[10];
     vals[0] = e_acc;
 #pragma unroll
@@ -337,11 +376,9 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
 #pragma unroll
       for (int k = 0; k < 10; ++k) es.wred[wg * 10 + k] = vals[k];
     group_sync(g);
-    if (lt < 10) {
-      double v = es.wred[lt] + es.wred[10 + lt] + es.wred[20 + lt] + es.wred[30 + lt];
-      if (lt == 0) v += p.ref[iz];
-      site_out[10 * (size_t)s + lt] = v;
-    }
+    if (lt < 10) unit_out[10 * (size_t)unit + lt] = es.wred[lt] + es.wred[10 + lt] + es.wred[20 + lt] + es.wred[30 + lt];
+    if (lay.feat)
+      for (int k = lt; k < lay.nfeat; k += ACE_GROUP) unit_feat[(size_t)lay.nfeat * unit + k] = Facc[k];
   }
 }
 

@@ -3,7 +3,9 @@
 // Every entry point catches internal errors and returns a pfw_status with
 // the message kept in the workspace (pfw_last_error).  Nothing here falls
 // back to a CPU computation: a missing device is an error.
+#include <algorithm>
 #include <cmath>
+#include <vector>
 #include <cstdio>
 #include <new>
 
@@ -47,6 +49,7 @@ void upload_geometry(pfw_ws* ws, int64_t n, const double* X, const double* H, co
   hs.natoms = (int32_t)n;
   ws->systems.assign(1, hs);
   ws->n = (int32_t)n;
+  ws->geometry_version += 1;
   cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   ws->X.ensure(sizeof(double) * 3 * std::max<int64_t>(n, 1));
   ws->species.ensure(sizeof(int32_t) * std::max<int64_t>(n, 1));
@@ -64,6 +67,60 @@ void upload_geometry(pfw_ws* ws, int64_t n, const double* X, const double* H, co
   ws->prep.valid = false;
   ws->nb_total = -1;
   ws->last_pairs = -1;
+}
+
+void upload_batch(pfw_ws* ws, int32_t nsys, const int64_t* offsets, const double* X, const double* H,
+                  const uint8_t* pbc, const int32_t* species, bool device_ptrs) {
+  if (nsys < 1) throw Error(PFW_EINVAL, "a batch needs at least one system");
+  if (!offsets || !H || !pbc) throw Error(PFW_EINVAL, "offsets, cells and pbc are required");
+  if (offsets[0] != 0) throw Error(PFW_EINVAL, "atom offsets must start at 0");
+  for (int32_t s = 0; s < nsys; ++s)
+    if (offsets[s + 1] < offsets[s]) throw Error(PFW_EINVAL, "atom offsets must be nondecreasing");
+  const int64_t n = offsets[nsys];
+  if (n > (int64_t)INT32_MAX / 4) throw Error(PFW_EINVAL, "atom count out of range");
+  if (n > 0 && (!X || !species)) throw Error(PFW_EINVAL, "positions and species are required");
+  std::vector<pfw::HostSystem> systems(nsys);
+  for (int32_t s = 0; s < nsys; ++s) {
+    pfw::HostSystem& hs = systems[s];
+    for (int k = 0; k < 9; ++k) hs.H[k] = H[9 * (size_t)s + k];
+    for (int a = 0; a < 3; ++a) hs.pbc[a] = pbc[3 * (size_t)s + a] ? 1 : 0;
+    hs.atom_begin = (int32_t)offsets[s];
+    hs.natoms = (int32_t)(offsets[s + 1] - offsets[s]);
+  }
+  int32_t max_species = 0;
+  if (!device_ptrs)
+    for (int64_t i = 0; i < n; ++i) {
+      if (species[i] < 0) throw Error(PFW_EINVAL, "species channels must be nonnegative");
+      max_species = std::max(max_species, species[i]);
+    }
+  cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  ws->X.ensure(sizeof(double) * 3 * std::max<int64_t>(n, 1));
+  ws->species.ensure(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  if (n > 0) {
+    PFW_CUDA(cudaMemcpyAsync(ws->X.ptr, X, sizeof(double) * 3 * n, kind, ws->stream));
+    PFW_CUDA(cudaMemcpyAsync(ws->species.ptr, species, sizeof(int32_t) * n, kind, ws->stream));
+  }
+  ws->systems.swap(systems);
+  ws->n = (int32_t)n;
+  ws->max_species = max_species;
+  ws->geometry_version += 1;
+  ws->prep.valid = false;
+  ws->nb_total = -1;
+  ws->last_pairs = -1;
+}
+
+// Batch evaluation on device outputs (no host synchronisation for pairs).
+void evaluate_batch_device(pfw_ws* ws, int32_t model, uint32_t request, double* E, double* F, double* W,
+                           double* feat) {
+  if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+  if (model == PFW_MODEL_PAIR) {
+    if (feat) throw Error(PFW_EINVAL, "fitting features exist for ACE models only");
+    pfw::pair_evaluate(ws, request, E, F, W, true);
+  } else if (model == PFW_MODEL_ACE) {
+    pfw::ace_evaluate_batch(ws, request, E, F, W, feat);
+  } else {
+    throw Error(PFW_EINVAL, "unknown model selector");
+  }
 }
 
 }  // namespace
@@ -99,6 +156,7 @@ pfw_status pfw_ws_create(const pfw_options* opts, pfw_ws** out) {
     delete ws;
     return PFW_ECUDA;
   }
+  ws->own_stream = ws->stream;
   *out = ws;
   return PFW_OK;
 }
@@ -111,10 +169,12 @@ void pfw_ws_destroy(pfw_ws* ws) {
   pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
                          &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
                          &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
-                         &ws->minmax, &ws->cellpart, &ws->out_E, &ws->out_F, &ws->out_W, &ws->counters,
+                         &ws->minmax, &ws->cellpart, &ws->out_E, &ws->out_F, &ws->out_W, &ws->out_feat, &ws->counters,
                          &ws->nb_count, &ws->nb_offsets, &ws->nb_j, &ws->nb_S, &ws->nb_R};
   for (auto* b : bufs) b->release();
-  if (ws->stream) cudaStreamDestroy(ws->stream);
+  for (auto& e : ws->ev)
+    if (e) cudaEventDestroy(e);
+  if (ws->own_stream) cudaStreamDestroy(ws->own_stream);
   delete ws;
 }
 
@@ -210,6 +270,87 @@ pfw_status pfw_evaluate(pfw_ws* ws, int32_t model, uint32_t request, double* E, 
     if (W)
       for (int k = 0; k < 9; ++k) W[k] = hW[k];
   });
+}
+
+pfw_status pfw_set_batch(pfw_ws* ws, int32_t nsys, const int64_t* atom_offsets, const double* X, const double* H,
+                         const uint8_t* pbc, const int32_t* species) {
+  return guarded(ws, [&] { upload_batch(ws, nsys, atom_offsets, X, H, pbc, species, false); });
+}
+
+pfw_status pfw_set_batch_device(pfw_ws* ws, int32_t nsys, const int64_t* atom_offsets, const double* X_dev,
+                                const double* H, const uint8_t* pbc, const int32_t* species_dev) {
+  return guarded(ws, [&] { upload_batch(ws, nsys, atom_offsets, X_dev, H, pbc, species_dev, true); });
+}
+
+pfw_status pfw_batch_update_positions(pfw_ws* ws, const double* X, int32_t on_device) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    if (ws->n > 0 && !X) throw Error(PFW_EINVAL, "positions required");
+    if (ws->n > 0)
+      PFW_CUDA(cudaMemcpyAsync(ws->X.ptr, X, sizeof(double) * 3 * ws->n,
+                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ws->stream));
+    if (!on_device) PFW_CUDA(cudaStreamSynchronize(ws->stream));
+    ws->prep.valid = false;
+    ws->nb_total = -1;
+  });
+}
+
+pfw_status pfw_ace_feature_count(pfw_ws* ws, int32_t* nfeat) {
+  return guarded(ws, [&] {
+    if (!nfeat) throw Error(PFW_EINVAL, "null output");
+    *nfeat = pfw::ace_feature_count(ws);
+  });
+}
+
+pfw_status pfw_evaluate_batch_device(pfw_ws* ws, int32_t model, uint32_t request, double* E_dev, double* F_dev,
+                                     double* W_dev, double* features_dev) {
+  return guarded(ws, [&] {
+    evaluate_batch_device(ws, model, request, E_dev, F_dev, W_dev, features_dev);
+    PFW_CUDA(cudaStreamSynchronize(ws->stream));
+    PFW_CUDA(cudaGetLastError());
+  });
+}
+
+pfw_status pfw_evaluate_batch(pfw_ws* ws, int32_t model, uint32_t request, double* E, double* F, double* W,
+                              double* features) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    const int n = ws->n, nsys = (int)ws->systems.size();
+    const int nfeat = (features && model == PFW_MODEL_ACE) ? pfw::ace_feature_count(ws) : 0;
+    double* dE = static_cast<double*>(ws->out_E.ensure(sizeof(double) * nsys));
+    double* dW = static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9 * nsys));
+    double* dF = (request & PFW_REQ_FORCES) ? static_cast<double*>(ws->out_F.ensure(sizeof(double) * 3 * std::max(n, 1)))
+                                            : nullptr;
+    double* dX = features ? static_cast<double*>(ws->out_feat.ensure(sizeof(double) * std::max(nfeat, 1) * nsys))
+                          : nullptr;
+    evaluate_batch_device(ws, model, request, dE, dF, dW, dX);
+    std::vector<double> hE(nsys), hW(9 * (size_t)nsys);
+    PFW_CUDA(cudaMemcpyAsync(hE.data(), dE, sizeof(double) * nsys, cudaMemcpyDeviceToHost, ws->stream));
+    PFW_CUDA(cudaMemcpyAsync(hW.data(), dW, sizeof(double) * 9 * nsys, cudaMemcpyDeviceToHost, ws->stream));
+    if (F && dF && n > 0)
+      PFW_CUDA(cudaMemcpyAsync(F, dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ws->stream));
+    if (features && dX && nfeat > 0)
+      PFW_CUDA(cudaMemcpyAsync(features, dX, sizeof(double) * nfeat * nsys, cudaMemcpyDeviceToHost, ws->stream));
+    PFW_CUDA(cudaStreamSynchronize(ws->stream));
+    bool finite = true;
+    for (double v : hE) finite = finite && std::isfinite(v);
+    for (double v : hW) finite = finite && std::isfinite(v);
+    if (!finite) throw Error(PFW_EDOMAIN, "nonfinite energy/virial (coincident atoms with a singular model?)");
+    if (E) std::copy(hE.begin(), hE.end(), E);
+    if (W) std::copy(hW.begin(), hW.end(), W);
+  });
+}
+
+pfw_status pfw_batch_graph_launch(pfw_ws* ws, uint32_t request, double* E_dev, double* F_dev, double* W_dev,
+                                  double* features_dev) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    pfw::ace_batch_graph(ws, request, E_dev, F_dev, W_dev, features_dev);
+  });
+}
+
+pfw_status pfw_batch_graph_sync(pfw_ws* ws) {
+  return guarded(ws, [&] { pfw::ace_batch_graph_sync(ws); });
 }
 
 pfw_status pfw_site_energies(pfw_ws* ws, double* energies) {

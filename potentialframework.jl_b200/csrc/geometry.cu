@@ -424,11 +424,13 @@ void exclusive_scan_i64(pfw_ws* ws, const int32_t* in, int64_t* out, int64_t n) 
 // ---------------------------------------------------------------------------
 // prepare: cell list of the current geometry for a cutoff
 // ---------------------------------------------------------------------------
-void prepare(pfw_ws* ws, double cutoff) {
+// Host decisions, buffer sizing and (only when a system has an open axis) the
+// wrap + min/max pass that fixes the open-axis grid.  Returns true when that
+// pass already wrapped the positions.
+bool prepare_plan(pfw_ws* ws, double cutoff) {
   if (!(std::isfinite(cutoff) && cutoff > 0)) throw Error(PFW_EINVAL, "cutoff must be finite and positive (Å)");
   if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
   Prepared& P = ws->prep;
-  if (P.valid && P.cutoff == cutoff) return;
   const int n = ws->n;
   const int nsys = (int)ws->systems.size();
   // neighbour lists pack sorted indices in 24 bits
@@ -443,23 +445,22 @@ void prepare(pfw_ws* ws, double cutoff) {
     if (!P.sys[s].minimum_image) any_image = true;
   }
   SysGeom* dsys = static_cast<SysGeom*>(ws->sysgeom.ensure(sizeof(SysGeom) * nsys));
-  PFW_CUDA(cudaMemcpyAsync(dsys, P.sys.data(), sizeof(SysGeom) * nsys, cudaMemcpyHostToDevice, st));
-  int* atom_sys = static_cast<int*>(ws->atom_sys.ensure(sizeof(int) * std::max(n, 1)));
-  double* wrapped = static_cast<double*>(ws->wrapped.ensure(sizeof(double) * 3 * std::max(n, 1)));
-  double* bincoord = static_cast<double*>(ws->bincoord.ensure(sizeof(double) * 3 * std::max(n, 1)));
-  int* wind = static_cast<int*>(ws->wind.ensure(sizeof(int) * 3 * std::max(n, 1)));
-  // counters: int flags [0..7] (0: bad input, 4: largest cell), u64 pair count at byte 32
-  int* bad = static_cast<int*>(ws->counters.ensure(64));
-  PFW_CUDA(cudaMemsetAsync(bad, 0, sizeof(int) * 8, st));
-  if (n > 0) {
-    k_atom_sys<<<grid_for(n, 256), 256, 0, st>>>(dsys, nsys, n, atom_sys);
-    k_wrap<<<grid_for(n, 256), 256, 0, st>>>(n, ws->X.as<double>(), atom_sys, dsys, wrapped, bincoord, wind, bad);
-    ws->launches += 2;
-  }
+  ws->atom_sys.ensure(sizeof(int) * std::max(n, 1));
+  ws->wrapped.ensure(sizeof(double) * 3 * std::max(n, 1));
+  ws->bincoord.ensure(sizeof(double) * 3 * std::max(n, 1));
+  ws->wind.ensure(sizeof(int) * 3 * std::max(n, 1));
+  ws->counters.ensure(64);  // int flags [0..7] (0: bad input, 4: largest cell), u64 pair count at byte 32
+  bool wrapped_done = false;
   if (any_open && n > 0) {
+    PFW_CUDA(cudaMemcpyAsync(dsys, P.sys.data(), sizeof(SysGeom) * nsys, cudaMemcpyHostToDevice, st));
+    int* bad = ws->counters.as<int>();
+    PFW_CUDA(cudaMemsetAsync(bad, 0, sizeof(int) * 8, st));
+    k_atom_sys<<<grid_for(n, 256), 256, 0, st>>>(dsys, nsys, n, ws->atom_sys.as<int>());
+    k_wrap<<<grid_for(n, 256), 256, 0, st>>>(n, ws->X.as<double>(), ws->atom_sys.as<int>(), dsys,
+                                             ws->wrapped.as<double>(), ws->bincoord.as<double>(), ws->wind.as<int>(), bad);
     double* mm = static_cast<double*>(ws->minmax.ensure(sizeof(double) * 6 * nsys));
-    k_open_minmax<<<nsys, 256, 0, st>>>(dsys, bincoord, mm);
-    ws->launches += 1;
+    k_open_minmax<<<nsys, 256, 0, st>>>(dsys, ws->bincoord.as<double>(), mm);
+    ws->launches += 3;
     std::vector<double> h(6 * nsys);
     PFW_CUDA(cudaMemcpyAsync(h.data(), mm, sizeof(double) * 6 * nsys, cudaMemcpyDeviceToHost, st));
     PFW_CUDA(cudaStreamSynchronize(st));
@@ -477,6 +478,7 @@ void prepare(pfw_ws* ws, double cutoff) {
         g.dims[a] = (int32_t)q + 1;
       }
     }
+    wrapped_done = true;
   }
   int64_t ncells = 0;
   for (int s = 0; s < nsys; ++s) {
@@ -492,39 +494,84 @@ void prepare(pfw_ws* ws, double cutoff) {
   P.nsys = nsys;
   P.n = n;
   P.any_image = any_image;
-  int* count = static_cast<int*>(ws->cell_count.ensure(sizeof(int) * (ncells + 1)));
-  int* cell_start = static_cast<int*>(ws->cell_start.ensure(sizeof(int) * (ncells + 1)));
-  int* cellid = static_cast<int*>(ws->cellid.ensure(sizeof(int) * std::max(n, 1)));
-  int* slot = static_cast<int*>(ws->slot.ensure(sizeof(int) * std::max(n, 1)));
-  int* tmp = static_cast<int*>(ws->tmp_idx.ensure(sizeof(int) * std::max(n, 1)));
-  int* perm = static_cast<int*>(ws->perm.ensure(sizeof(int) * std::max(n, 1)));
-  int* inverse = static_cast<int*>(ws->inverse.ensure(sizeof(int) * std::max(n, 1)));
-  double4* pos = static_cast<double4*>(ws->pos.ensure(sizeof(double4) * std::max(n, 1)));
-  int* cell_sys = static_cast<int*>(ws->cell_sys.ensure(sizeof(int) * std::max<int64_t>(ncells, 1)));
+  P.cutoff = cutoff;
+  ws->cell_count.ensure(sizeof(int) * (ncells + 1));
+  ws->cell_start.ensure(sizeof(int) * (ncells + 1));
+  ws->cellid.ensure(sizeof(int) * std::max(n, 1));
+  ws->slot.ensure(sizeof(int) * std::max(n, 1));
+  ws->tmp_idx.ensure(sizeof(int) * std::max(n, 1));
+  ws->perm.ensure(sizeof(int) * std::max(n, 1));
+  ws->inverse.ensure(sizeof(int) * std::max(n, 1));
+  ws->pos.ensure(sizeof(double4) * std::max(n, 1));
+  ws->cell_sys.ensure(sizeof(int) * std::max<int64_t>(ncells, 1));
+  const int64_t nb = (std::max<int64_t>(ncells, n) + 4095) / 4096 + 1;
+  ws->scan_tmp.ensure(sizeof(int64_t) * (nb + 1));
+  return wrapped_done;
+}
+
+// Device work of the cell-list build on planned buffers: no allocation and no
+// host synchronisation, so it can be captured in a CUDA graph.
+void prepare_launch(pfw_ws* ws, bool wrap) {
+  const Prepared& P = ws->prep;
+  const int n = P.n, nsys = P.nsys;
+  const int64_t ncells = P.ncells;
+  cudaStream_t st = ws->stream;
+  const SysGeom* dsys = ws->sysgeom.as<SysGeom>();
+  int* bad = ws->counters.as<int>();
+  int* atom_sys = ws->atom_sys.as<int>();
+  double* bincoord = ws->bincoord.as<double>();
+  int* count = ws->cell_count.as<int>();
+  int* cell_start = ws->cell_start.as<int>();
+  if (wrap) {
+    PFW_CUDA(cudaMemsetAsync(bad, 0, sizeof(int) * 8, st));
+    if (n > 0) {
+      k_atom_sys<<<grid_for(n, 256), 256, 0, st>>>(dsys, nsys, n, atom_sys);
+      k_wrap<<<grid_for(n, 256), 256, 0, st>>>(n, ws->X.as<double>(), atom_sys, dsys, ws->wrapped.as<double>(),
+                                               bincoord, ws->wind.as<int>(), bad);
+      ws->launches += 2;
+    }
+  }
   PFW_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (ncells + 1), st));
   if (n > 0) {
-    k_key_count<<<grid_for(n, 256), 256, 0, st>>>(n, atom_sys, dsys, bincoord, cellid, slot, count, bad);
+    k_key_count<<<grid_for(n, 256), 256, 0, st>>>(n, atom_sys, dsys, bincoord, ws->cellid.as<int>(),
+                                                  ws->slot.as<int>(), count, bad);
     ws->launches += 1;
   }
   exclusive_scan_i32(ws, count, cell_start, ncells);
   if (n > 0) {
-    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, cellid, slot, cell_start, tmp);
-    k_cell_rank<<<grid_for((int64_t)ncells * 32, 256), 256, 0, st>>>((int)ncells, cell_start, tmp, perm);
-    k_gather<<<grid_for(n, 256), 256, 0, st>>>(n, perm, wrapped, ws->species.as<int>(), pos, inverse);
+    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, ws->cellid.as<int>(), ws->slot.as<int>(), cell_start,
+                                                 ws->tmp_idx.as<int>());
+    k_cell_rank<<<grid_for((int64_t)ncells * 32, 256), 256, 0, st>>>((int)ncells, cell_start, ws->tmp_idx.as<int>(),
+                                                                      ws->perm.as<int>());
+    k_gather<<<grid_for(n, 256), 256, 0, st>>>(n, ws->perm.as<int>(), ws->wrapped.as<double>(),
+                                               ws->species.as<int>(), ws->pos.as<double4>(), ws->inverse.as<int>());
     ws->launches += 3;
   }
   if (ncells > 0) {
-    k_cell_sys<<<grid_for(ncells, 256), 256, 0, st>>>(dsys, nsys, (int)ncells, cell_sys, cell_start, bad + 4);
+    k_cell_sys<<<grid_for(ncells, 256), 256, 0, st>>>(dsys, nsys, (int)ncells, ws->cell_sys.as<int>(), cell_start,
+                                                      bad + 4);
     ws->launches += 1;
   }
+  PFW_CUDA(cudaGetLastError());
+}
+
+// Synchronise and turn the device flags of the build into errors.
+void prepare_check(pfw_ws* ws) {
   int hbad[8];
-  PFW_CUDA(cudaMemcpyAsync(hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, st));
-  PFW_CUDA(cudaStreamSynchronize(st));
+  PFW_CUDA(cudaMemcpyAsync(hbad, ws->counters.ptr, sizeof(hbad), cudaMemcpyDeviceToHost, ws->stream));
+  PFW_CUDA(cudaStreamSynchronize(ws->stream));
   PFW_CUDA(cudaGetLastError());
   if (hbad[0] == 1) throw Error(PFW_EINVAL, "positions must be finite");
   if (hbad[0] == 2) throw Error(PFW_EINVAL, "atom outside the open-axis cell grid");
-  P.max_cell = hbad[4];
-  P.cutoff = cutoff;
+  ws->prep.max_cell = hbad[4];
+}
+
+void prepare(pfw_ws* ws, double cutoff) {
+  Prepared& P = ws->prep;
+  if (P.valid && P.cutoff == cutoff) return;
+  const bool wrapped = prepare_plan(ws, cutoff);
+  prepare_launch(ws, !wrapped);
+  prepare_check(ws);
   P.valid = true;
 }
 

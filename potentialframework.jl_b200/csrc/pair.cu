@@ -283,7 +283,38 @@ __global__ void k_reduce_parts(const double* __restrict__ parts, int nparts, int
   }
 }
 
-void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev) {
+// Per-system reduction of a batch: block s sums the cells of system s.
+__global__ void k_reduce_systems(const double* __restrict__ parts, const SysGeom* __restrict__ sys, int stride,
+                                 double* __restrict__ E, double* __restrict__ W) {
+  __shared__ double sh[7][128];
+  const int s = blockIdx.x;
+  const int c0 = sys[s].cell_begin, c1 = c0 + sys[s].ncells;
+  Kahan acc[7];
+  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 7; ++k) acc[k].add(parts[(size_t)stride * c + k]);
+#pragma unroll
+  for (int k = 0; k < 7; ++k) sh[k][threadIdx.x] = acc[k].s - acc[k].c;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+#pragma unroll
+      for (int k = 0; k < 7; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (E) E[s] = sh[0][0];
+    if (W) {
+      double* w = W + 9 * (size_t)s;
+      w[0] = sh[1][0]; w[4] = sh[2][0]; w[8] = sh[3][0];
+      w[3] = w[1] = sh[4][0];
+      w[6] = w[2] = sh[5][0];
+      w[7] = w[5] = sh[6][0];
+    }
+  }
+}
+
+void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system) {
   const PairModel& m = ws->pair;
   if (m.kind < 0) throw Error(PFW_ESTATE, "no pair model loaded");
   if (m.kind == 0 && ws->max_species >= m.nz)
@@ -343,7 +374,11 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   double* E = E_dev ? E_dev : static_cast<double*>(ws->out_E.ensure(sizeof(double)));
   double* W = W_dev ? W_dev : static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
   ws->stage_begin(2);
-  k_reduce_parts<<<1, 256, 0, st>>>(parts, ncells, 8, E, W);
+  if (per_system) {
+    if (P.nsys > 0) k_reduce_systems<<<P.nsys, 128, 0, st>>>(parts, dsys, 8, E_dev, W_dev);
+  } else {
+    k_reduce_parts<<<1, 256, 0, st>>>(parts, ncells, 8, E, W);
+  }
   ws->stage_end(2);
   ws->launches += 1;
   PFW_CUDA(cudaGetLastError());

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -25,12 +26,17 @@ struct Error : std::runtime_error {
       throw ::pfw::Error(PFW_ECUDA, std::string(#call) + ": " + cudaGetErrorString(_e));           \
   } while (0)
 
+// Bumped by every device reallocation in the process: a captured CUDA graph
+// recorded at an older epoch may hold freed pointers and is re-captured.
+inline std::atomic<uint64_t> g_alloc_epoch{0};
+
 // Growable device buffer (never shrinks; contents not preserved on growth).
 struct DevBuf {
   void* ptr = nullptr;
   size_t cap = 0;
   void* ensure(size_t bytes) {
     if (bytes > cap) {
+      g_alloc_epoch.fetch_add(1);
       if (ptr) cudaFree(ptr);
       ptr = nullptr;
       size_t want = bytes < 256 ? 256 : bytes + bytes / 4;
@@ -86,6 +92,7 @@ struct pfw_ws {
   int32_t n = 0;
   int32_t max_species = 0;  // largest species channel of host-uploaded geometry
   std::vector<pfw::HostSystem> systems;
+  uint64_t geometry_version = 0;  // bumped when the systems (count, sizes, cells) change
   pfw::DevBuf X, species, atom_sys;  // X: 3n doubles
   // prepared geometry
   pfw::Prepared prep;
@@ -93,7 +100,7 @@ struct pfw_ws {
       perm, inverse, pos, pos32, scan_tmp, minmax;
   // pair evaluation
   pfw::PairModel pair;
-  pfw::DevBuf cellpart, out_E, out_F, out_W, counters;
+  pfw::DevBuf cellpart, out_E, out_F, out_W, out_feat, counters;
   int64_t last_pairs = -1;
   // neighbour snapshot
   pfw::DevBuf nb_count, nb_offsets, nb_j, nb_S, nb_R;
@@ -121,10 +128,14 @@ struct pfw_ws {
 namespace pfw {
 // geometry.cu
 void prepare(pfw_ws* ws, double cutoff);
+bool prepare_plan(pfw_ws* ws, double cutoff);  // host plan; true if it already wrapped (open axes)
+void prepare_launch(pfw_ws* ws, bool wrap);    // device-only build, capturable
+void prepare_check(pfw_ws* ws);                // synchronise, raise on device flags
 void exclusive_scan_i32(pfw_ws* ws, const int32_t* in, int32_t* out, int64_t n);  // out has n+1 entries
 void exclusive_scan_i64(pfw_ws* ws, const int32_t* in, int64_t* out, int64_t n);
 // pair.cu
-void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev);
+// per_system: E[s] and W[9s..] for every system of a batch
+void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system = false);
 // snapshot.cu
 int64_t neighbour_build(pfw_ws* ws, double cutoff);
 void neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);
@@ -134,6 +145,10 @@ void ace_set_schedule(pfw_ws* ws, int chunk, int groups);
 void ace_free(pfw_ws* ws);
 void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev);
 void ace_site_energies(pfw_ws* ws, double* host);
+int ace_feature_count(pfw_ws* ws);
+void ace_evaluate_batch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev);
+void ace_batch_graph(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev);
+void ace_batch_graph_sync(pfw_ws* ws);
 double probe_fp64(pfw_ws* ws);
 
 inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }

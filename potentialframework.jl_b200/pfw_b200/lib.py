@@ -86,6 +86,18 @@ def load():
     L.pfw_probe_fp64_peak.argtypes = [vp, dp]
     L.pfw_launch_count.argtypes = [vp]
     L.pfw_launch_count.restype = C.c_uint64
+    L.pfw_set_stream.argtypes = [vp, vp]
+    L.pfw_set_diagnostics.argtypes = [vp, C.c_int32]
+    L.pfw_stage_times.argtypes = [vp, dp, C.c_int32]
+    L.pfw_stage_times.restype = C.c_int32
+    L.pfw_set_batch.argtypes = [vp, C.c_int32, i64p, dp, dp, u8p, i32p]
+    L.pfw_set_batch_device.argtypes = [vp, C.c_int32, i64p, vp, dp, u8p, vp]
+    L.pfw_batch_update_positions.argtypes = [vp, vp, C.c_int32]
+    L.pfw_ace_feature_count.argtypes = [vp, i32p]
+    L.pfw_evaluate_batch.argtypes = [vp, C.c_int32, C.c_uint32, dp, dp, dp, dp]
+    L.pfw_evaluate_batch_device.argtypes = [vp, C.c_int32, C.c_uint32, vp, vp, vp, vp]
+    L.pfw_batch_graph_launch.argtypes = [vp, C.c_uint32, vp, vp, vp, vp]
+    L.pfw_batch_graph_sync.argtypes = [vp]
     _lib = L
     return L
 
@@ -191,6 +203,68 @@ class Handle:
         self.check(self.L.pfw_neighbour_fill(self.ws, ptr(offs, C.c_int64), ptr(j, C.c_int32), ptr(S, C.c_int32),
                                              ptr(R, C.c_double)))
         return offs, j, S, R
+
+    # --- batches of independent systems --------------------------------
+    @staticmethod
+    def _batch_arrays(systems):
+        offs = np.zeros(len(systems) + 1, np.int64)
+        offs[1:] = np.cumsum([len(s.species) for s in systems])
+        H = np.concatenate([np.asarray(s.H, np.float64).reshape(3, 3).ravel(order="F") for s in systems])
+        pbc = np.array([[1 if b else 0 for b in s.pbc] for s in systems], np.uint8).ravel()
+        return offs, H, pbc
+
+    def set_batch(self, systems):
+        """systems: sequence of workloads.System-like objects (X n×3, H with columns = cell vectors, pbc, species)."""
+        offs, H, pbc = self._batch_arrays(systems)
+        X = np.ascontiguousarray(np.concatenate([np.asarray(s.X, np.float64).reshape(-1, 3) for s in systems]))
+        sp = np.ascontiguousarray(np.concatenate([np.asarray(s.species, np.int32) for s in systems]))
+        self.check(self.L.pfw_set_batch(self.ws, len(systems), ptr(offs, C.c_int64), ptr(X, C.c_double),
+                                        ptr(H, C.c_double), ptr(pbc, C.c_uint8), ptr(sp, C.c_int32)))
+        self.n = int(offs[-1])
+        self.nsys = len(systems)
+        self.batch_offsets = offs
+
+    def set_batch_device(self, systems, X_dev_ptr, species_dev_ptr):
+        offs, H, pbc = self._batch_arrays(systems)
+        self.check(self.L.pfw_set_batch_device(self.ws, len(systems), ptr(offs, C.c_int64), X_dev_ptr,
+                                               ptr(H, C.c_double), ptr(pbc, C.c_uint8), species_dev_ptr))
+        self.n = int(offs[-1])
+        self.nsys = len(systems)
+        self.batch_offsets = offs
+
+    def batch_update_positions(self, X=None, X_dev_ptr=None):
+        if X_dev_ptr is not None:
+            self.check(self.L.pfw_batch_update_positions(self.ws, X_dev_ptr, 1))
+        else:
+            X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
+            self.check(self.L.pfw_batch_update_positions(self.ws, X.ctypes.data, 0))
+
+    def feature_count(self):
+        v = np.zeros(1, np.int32)
+        self.check(self.L.pfw_ace_feature_count(self.ws, ptr(v, C.c_int32)))
+        return int(v[0])
+
+    def evaluate_batch(self, model=MODEL_ACE, request=7, features=False):
+        """Per-system E [nsys], F [N×3], W [nsys×3×3] and (ACE) fitting features [nsys×nfeat]."""
+        E = np.zeros(self.nsys)
+        W = np.zeros((self.nsys, 9))
+        F = np.zeros((self.n, 3)) if request & REQ_F else None
+        X = np.zeros((self.nsys, self.feature_count())) if features else None
+        self.check(self.L.pfw_evaluate_batch(self.ws, model, request, ptr(E, C.c_double), ptr(F, C.c_double),
+                                             ptr(W, C.c_double), ptr(X, C.c_double)))
+        return E, F, W.reshape(self.nsys, 3, 3).transpose(0, 2, 1), X
+
+    def evaluate_batch_device(self, model, request, E_ptr, F_ptr, W_ptr, feat_ptr=None):
+        self.check(self.L.pfw_evaluate_batch_device(self.ws, model, request, E_ptr, F_ptr, W_ptr, feat_ptr))
+
+    def batch_graph_launch(self, request, E_ptr, F_ptr, W_ptr, feat_ptr=None):
+        self.check(self.L.pfw_batch_graph_launch(self.ws, request, E_ptr, F_ptr, W_ptr, feat_ptr))
+
+    def batch_graph_sync(self):
+        self.check(self.L.pfw_batch_graph_sync(self.ws))
+
+    def set_stream(self, stream_ptr):
+        self.check(self.L.pfw_set_stream(self.ws, stream_ptr))
 
     def probe_fp64(self):
         v = np.zeros(1)

@@ -16,6 +16,7 @@ sizes and value distributions:
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 
@@ -116,45 +117,75 @@ def random_triclinic_cell(rng, lo=6.0, hi=14.0, amin=70.0, amax=110.0):
         return np.stack([v1, v2, v3], axis=1)
 
 
-def batched(seed=5, nsys=4096, nmin=8, nmax=256, dmin=1.6, max_density=0.11):
-    """4096 periodic triclinic systems; n log-uniform on [nmin, nmax]; uniform
-    fractional positions with hard-core rejection at dmin; cells are redrawn
-    until n/V <= max_density Å⁻³."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for s in range(nsys):
-        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
-        while True:
-            H = random_triclinic_cell(rng)
-            V = abs(np.linalg.det(H))
-            if n / V <= max_density:
-                break
-        X = _hardcore(rng, H, n, dmin)
-        species = np.zeros(n, np.int32)
-        species[rng.permutation(n)[: n // 2]] = 1
-        out.append(System(X, H, (True, True, True), species, f"batch{s}"))
-    return out
+def _batched_system(args):
+    seq, nmin, nmax, dmin, max_density, s = args
+    rng = np.random.default_rng(seq)
+    n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+    while True:
+        H = random_triclinic_cell(rng)
+        V = abs(np.linalg.det(H))
+        if n / V <= max_density:
+            break
+    X = _hardcore(rng, H, n, dmin)
+    species = np.zeros(n, np.int32)
+    species[rng.permutation(n)[: n // 2]] = 1
+    return System(X, H, (True, True, True), species, f"batch{s}")
 
 
-def _hardcore(rng, H, n, dmin, max_tries=200000):
-    Hinv = np.linalg.inv(H)
-    pts = []
-    tries = 0
-    shifts = np.array([[i, j, k] for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)], dtype=np.float64)
+def batched(seed=5, nsys=4096, nmin=8, nmax=256, dmin=1.6, max_density=0.11, workers=None):
+    """Periodic triclinic systems (4096 by default); n log-uniform on
+    [nmin, nmax]; uniform fractional positions with hard-core rejection at
+    dmin; cells are redrawn until n/V <= max_density Å⁻³.  System s draws from
+    its own stream (SeedSequence(seed).spawn), so the set does not depend on
+    `workers` (processes, spawned; default: all cores for large batches)."""
+    seqs = np.random.SeedSequence(seed).spawn(nsys)
+    args = [(seqs[s], nmin, nmax, dmin, max_density, s) for s in range(nsys)]
+    if workers is None:
+        workers = min(os.cpu_count() or 1, 32) if nsys >= 256 else 1
+    if workers <= 1:
+        return [_batched_system(a) for a in args]
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(_batched_system, args, chunksize=max(1, nsys // (8 * workers)))
+
+
+_SHIFTS = np.array([[i, j, k] for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)], dtype=np.float64)
+
+
+def _min_image_d2(H, a, b):
+    """Squared minimum-image distances between fractional points a (p,3) and b (m,3)."""
+    df = a[:, None, :] - b[None, :, :]
+    df -= np.round(df)
+    d0 = df @ H.T
+    Sc = _SHIFTS @ H.T
+    # |d0 + S|² = |d0|² + 2 d0·S + |S|², minimised over the 27 shifts
+    d2 = (d0 * d0).sum(axis=2)[:, :, None] + 2.0 * (d0 @ Sc.T) + (Sc * Sc).sum(axis=1)[None, None, :]
+    return d2.min(axis=2)
+
+
+def _hardcore(rng, H, n, dmin, batch=64, max_rounds=4000):
+    """Random sequential adsorption in fractional coordinates: candidates are
+    drawn `batch` at a time and accepted in draw order when they stay dmin
+    (minimum image) from every accepted point; dmin shrinks by 10 % after
+    max_rounds rounds without completing."""
+    pts = np.empty((0, 3))
+    rounds = 0
     while len(pts) < n:
-        tries += 1
-        if tries > max_tries:
+        rounds += 1
+        if rounds > max_rounds:
             dmin *= 0.9
-            tries = 0
-        f = rng.uniform(0, 1, 3)
-        ok = True
-        if pts:
-            P = np.array(pts)
-            df = P - f
-            df -= np.round(df)
-            d = (df[:, None, :] + shifts[None]) @ H.T
-            if np.min(np.einsum("ijk,ijk->ij", d, d)) < dmin * dmin:
-                ok = False
-        if ok:
-            pts.append(f)
-    return np.array(pts) @ H.T
+            rounds = 0
+        d2min = dmin * dmin
+        cand = rng.uniform(0, 1, (batch, 3))
+        if len(pts):
+            cand = cand[_min_image_d2(H, cand, pts).min(axis=1) >= d2min]
+        fresh = []
+        for c in cand:
+            if len(pts) + len(fresh) >= n:
+                break
+            if fresh and _min_image_d2(H, c[None], np.array(fresh)).min() < d2min:
+                continue
+            fresh.append(c)
+        if fresh:
+            pts = np.concatenate([pts, np.array(fresh)])
+    return pts @ H.T
