@@ -11,16 +11,18 @@
 //                 from the ORIGINAL coordinates (environments.jl:97-102)
 //   k_edge_rev    index of the reverse edge (j→i, -S) of every edge
 //   k_ace_sites   persistent site kernel (ace_site.cuh) over work units (one
-//                 site, or one system of a batch)
+//                 site, or up to 16 sites of one system of a batch)
 //   k_ace_gather  F_k = Σ_{e∈out(k)} g_e - g_{rev(e)}  (reduce_site!,
 //                 NeighbourList/execution.jl:256-273, without a racing scatter)
 //   k_ace_reduce  E and the 3×3 virial from per-site partials
 //
-// Batches of systems evaluate with one unit per system, so energies, virials
-// and the per-structure fitting features (ACE/fitting.jl:28-29) come out per
-// system; the batch path can be captured once as a CUDA graph and replayed.
+// Batches of systems evaluate in units that never span two systems, summed
+// per system in a fixed order, so energies, virials and the per-structure
+// fitting features (ACE/fitting.jl:28-29) come out per system; the batch path
+// can be captured once as a CUDA graph and replayed.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "ace_math.cuh"
@@ -38,8 +40,8 @@ struct GraphKey {
   uint32_t req = 0;
   int chunk = 0, groups = 0, precision = 0;
   bool operator==(const GraphKey& o) const {
-    return geometry_version == o.geometry_version && alloc_epoch == o.alloc_epoch && E == o.E && F == o.F && W == o.W && feat == o.feat &&
-           req == o.req && chunk == o.chunk && groups == o.groups && precision == o.precision;
+    return geometry_version == o.geometry_version && alloc_epoch == o.alloc_epoch && E == o.E && F == o.F &&
+           W == o.W && feat == o.feat && req == o.req && chunk == o.chunk && groups == o.groups && precision == o.precision;
   }
 };
 
@@ -53,7 +55,13 @@ struct AceDevice {
   DevBuf crow_off, crow_k, crow_val;
   // per evaluation
   DevBuf edge_count, edge_off, edge_j, edge_d, edge_S, edge_rev, edge_g, site_out, site_E_orig, status;
-  DevBuf unit_begin, unit_out;
+  DevBuf unit_begin, unit_out;  // single system: one unit per site
+  // batch: units of at most BATCH_UNIT_SITES sites, never spanning two systems
+  DevBuf batch_units, batch_sys_units, batch_out, batch_feat;
+  uint64_t batch_version = ~0ull;
+  int batch_nunits = 0;
+  std::vector<int> h_batch_units, h_batch_sys_units;
+  std::vector<SysGeom> graph_sys;  // cell-list plan the graph was captured with
   int64_t nedges = 0;
   int cap = 0;  // edge capacity of the buffers
   int n = 0;
@@ -212,22 +220,29 @@ __global__ void k_iota(int n, int* __restrict__ out) {
   if (k <= n) out[k] = k;
 }
 
-// Units of a batch: the sorted sites of system s start at its first cell.
-__global__ void k_system_units(int nsys, const SysGeom* __restrict__ sys, const int* __restrict__ cell_start,
-                               int n, int* __restrict__ unit_begin) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < nsys) unit_begin[s] = cell_start[sys[s].cell_begin];
-  if (s == 0) unit_begin[nsys] = n;
-}
-
-// Per-unit [E, W(9)] → caller layout E[s], W[9s..9s+8].
-__global__ void k_unit_outputs(int nunits, const double* __restrict__ unit_out, double* __restrict__ E,
-                               double* __restrict__ W) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nunits) return;
-  if (E) E[s] = unit_out[10 * (size_t)s];
-  if (W)
-    for (int k = 0; k < 9; ++k) W[9 * (size_t)s + k] = unit_out[10 * (size_t)s + 1 + k];
+// Per-system totals of a batch: the units of system s, summed in unit order
+// (deterministic), give E[s], W[9s..9s+8] and the fitting features.
+__global__ void k_system_reduce(int nsys, const int* __restrict__ sys_units, const double* __restrict__ unit_out,
+                                const double* __restrict__ unit_feat, int nfeat, double* __restrict__ E,
+                                double* __restrict__ W, double* __restrict__ feat) {
+  const int s = blockIdx.x;
+  if (s >= nsys) return;
+  const int u0 = sys_units[s], u1 = sys_units[s + 1];
+  const int ncol = 10 + (feat ? nfeat : 0);
+  for (int k = threadIdx.x; k < ncol; k += blockDim.x) {
+    double acc = 0.0;
+    if (k < 10)
+      for (int u = u0; u < u1; ++u) acc += unit_out[10 * (size_t)u + k];
+    else
+      for (int u = u0; u < u1; ++u) acc += unit_feat[(size_t)nfeat * u + (k - 10)];
+    if (k == 0) {
+      if (E) E[s] = acc;
+    } else if (k < 10) {
+      if (W) W[9 * (size_t)s + k - 1] = acc;
+    } else {
+      feat[(size_t)nfeat * s + k - 10] = acc;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -281,7 +296,8 @@ void ace_free(pfw_ws* ws) {
                     &a->density, &a->dn_off, &a->dn, &a->dm_off, &a->dm, &a->prods, &a->term_off, &a->terms,
                     &a->weights, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm, &a->crow_off, &a->crow_k, &a->crow_val,
                     &a->edge_count, &a->edge_off, &a->edge_j, &a->edge_d, &a->edge_S, &a->edge_rev, &a->edge_g,
-                    &a->site_out, &a->site_E_orig, &a->status, &a->unit_begin, &a->unit_out};
+                    &a->site_out, &a->site_E_orig, &a->status, &a->unit_begin, &a->unit_out,
+                    &a->batch_units, &a->batch_sys_units, &a->batch_out, &a->batch_feat};
   for (auto* b : bufs) b->release();
   delete a;
   ws->ace = nullptr;
@@ -603,22 +619,22 @@ static void build_edges(pfw_ws* ws, AceDevice* a) {
 }
 
 // Site kernel, force gather and the per-unit outputs (no host synchronisation).
-static void sites_launch(pfw_ws* ws, AceDevice* a, uint32_t req, int nunits, const AceLayout& lay, double* F_dev,
-                         double* feat) {
+static void sites_launch(pfw_ws* ws, AceDevice* a, uint32_t req, int nunits, const int* unit_begin,
+                         double* unit_out, double* unit_feat, const AceLayout& lay, double* F_dev) {
   cudaStream_t st = ws->stream;
   const int n = ws->prep.n;
   const bool want_grad = (req & (PFW_REQ_FORCES | PFW_REQ_VIRIAL)) != 0;
   const AceTables p = tables_of(a);
   SiteLaunch s;
   s.nunits = nunits;
-  s.unit_begin = a->unit_begin.as<int>();
+  s.unit_begin = unit_begin;
   s.cap = a->cap;
   s.off = a->edge_off.as<int>();
   s.ed = a->edge_d.as<double4>();
   s.pos = ws->pos.as<double4>();
   s.g = a->edge_g.as<double>();
-  s.unit_out = a->unit_out.as<double>();
-  s.unit_feat = feat;
+  s.unit_out = unit_out;
+  s.unit_feat = unit_feat;
   s.want_grad = want_grad;
   s.status = a->status.as<int>();
   ws->stage_begin(1);
@@ -673,7 +689,7 @@ void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   k_iota<<<grid_for(n + 1, 256), 256, 0, st>>>(n, ub);
   ws->launches += 1;
   const AceLayout lay = choose_layout(tables_of(a), ws->opt.device, a->sched_chunk, a->sched_groups, 0);
-  sites_launch(ws, a, req, n, lay, F_dev, nullptr);
+  sites_launch(ws, a, req, n, ub, a->unit_out.as<double>(), nullptr, lay, F_dev);
   double* E = E_dev ? E_dev : static_cast<double*>(ws->out_E.ensure(sizeof(double)));
   double* W = W_dev ? W_dev : static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
   k_ace_reduce<<<1, 256, 0, st>>>(n, a->unit_out.as<double>(), ws->perm.as<int>(), E, W, Esite);
@@ -689,7 +705,45 @@ int ace_feature_count(pfw_ws* ws) {
   return a->nz * (a->nB + a->nQ);
 }
 
-// Batch of systems, one unit per system.  Eager: plan, build, evaluate.
+// Sites per work unit of a batch: small enough that large systems spread over
+// many site groups, large enough that a unit's feature partials stay few.
+constexpr int BATCH_UNIT_SITES = 16;
+
+// Work units of the current batch.  In sorted order the sites of system s
+// are [atom_begin_s, atom_begin_s + natoms_s) (its cells follow those of
+// system s-1), so the units depend only on the atom counts.
+static void plan_units(pfw_ws* ws, AceDevice* a) {
+  if (a->batch_version == ws->geometry_version) return;
+  auto& ub = a->h_batch_units;
+  auto& su = a->h_batch_sys_units;
+  ub.clear();
+  su.clear();
+  for (const auto& hs : ws->systems) {
+    su.push_back((int)ub.size());
+    for (int k = 0; k < hs.natoms; k += BATCH_UNIT_SITES) ub.push_back(hs.atom_begin + k);
+  }
+  su.push_back((int)ub.size());
+  a->batch_nunits = (int)ub.size();
+  ub.push_back(ws->n);
+  upload(a->batch_units, ub.data(), ub.size(), ws->stream);
+  upload(a->batch_sys_units, su.data(), su.size(), ws->stream);
+  a->batch_version = ws->geometry_version;
+}
+
+// Site kernel, force gather and per-system totals of a planned batch
+// (device work only; capturable).
+static void batch_launch(pfw_ws* ws, AceDevice* a, uint32_t req, const AceLayout& lay, double* E_dev,
+                         double* F_dev, double* W_dev, double* feat_dev) {
+  const int nsys = (int)ws->systems.size(), nu = a->batch_nunits;
+  const int nfeat = a->nz * (a->nB + a->nQ);
+  double* feat_part = feat_dev ? a->batch_feat.as<double>() : nullptr;
+  sites_launch(ws, a, req, nu, a->batch_units.as<int>(), a->batch_out.as<double>(), feat_part, lay, F_dev);
+  k_system_reduce<<<nsys, 128, 0, ws->stream>>>(nsys, a->batch_sys_units.as<int>(), a->batch_out.as<double>(),
+                                                 feat_part, nfeat, E_dev, W_dev, feat_dev);
+  ws->launches += 1;
+}
+
+// Batch of systems.  Eager: plan, build, evaluate.
 void ace_evaluate_batch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev) {
   AceDevice* a = ws->ace;
   if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
@@ -700,16 +754,13 @@ void ace_evaluate_batch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
   a->status.ensure(sizeof(int) * 4);
   PFW_CUDA(cudaMemsetAsync(a->status.ptr, 0, sizeof(int) * 4, st));
   build_edges(ws, a);
-  const int nsys = ws->prep.nsys, n = ws->prep.n;
-  a->n = n;
-  int* ub = static_cast<int*>(a->unit_begin.ensure(sizeof(int) * (nsys + 1)));
-  a->unit_out.ensure(sizeof(double) * 10 * std::max(nsys, 1));
-  const bool feat = feat_dev != nullptr;
-  k_system_units<<<grid_for(nsys + 1, 128), 128, 0, st>>>(nsys, ws->sysgeom.as<SysGeom>(), ws->cell_start.as<int>(), n, ub);
-  const AceLayout lay = choose_layout(tables_of(a), ws->opt.device, a->sched_chunk, a->sched_groups, feat);
-  sites_launch(ws, a, req, nsys, lay, F_dev, feat_dev);
-  k_unit_outputs<<<grid_for(nsys, 128), 128, 0, st>>>(nsys, a->unit_out.as<double>(), E_dev, W_dev);
-  ws->launches += 2;
+  a->n = ws->prep.n;
+  plan_units(ws, a);
+  const size_t nu = std::max(a->batch_nunits, 1);
+  a->batch_out.ensure(sizeof(double) * 10 * nu);
+  if (feat_dev) a->batch_feat.ensure(sizeof(double) * (size_t)ace_feature_count(ws) * nu);
+  const AceLayout lay = choose_layout(tables_of(a), ws->opt.device, a->sched_chunk, a->sched_groups, feat_dev != nullptr);
+  batch_launch(ws, a, req, lay, E_dev, F_dev, W_dev, feat_dev);
   ws->stage_end(2);
   ace_check(ws, a);
 }
@@ -737,14 +788,16 @@ void ace_batch_graph(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, dou
   key.groups = a->sched_groups;
   key.precision = ws->opt.precision;
   cudaStream_t st = ws->stream;
-  if (!a->graph_exec || !(a->graph_key == key)) {
+  const auto& ps = ws->prep.sys;
+  const bool same_plan = a->graph_sys.size() == ps.size() &&
+                         (ps.empty() || std::memcmp(a->graph_sys.data(), ps.data(), sizeof(SysGeom) * ps.size()) == 0);
+  if (!a->graph_exec || !(a->graph_key == key) || !same_plan) {
     release_graph(a);
     for (const auto& hs : ws->systems)
       if (!hs.pbc[0] || !hs.pbc[1] || !hs.pbc[2])
         throw Error(PFW_EINVAL, "graph batches require fully periodic systems");
     ace_evaluate_batch(ws, req, E_dev, F_dev, W_dev, feat_dev);  // plan and validate
     ensure_edge_buffers(a, (int)std::min<int64_t>((int64_t)(a->nedges * 1.25) + 4096, INT32_MAX / 4));
-    const int nsys = ws->prep.nsys, n = ws->prep.n;
     const bool feat = feat_dev != nullptr;
     const AceLayout lay = choose_layout(tables_of(a), ws->opt.device, a->sched_chunk, a->sched_groups, feat);
     const bool diag = ws->diag;
@@ -756,11 +809,7 @@ void ace_batch_graph(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, dou
       prepare_launch(ws, true);
       edges_count_launch(ws, a);
       edges_fill_launch(ws, a);
-      k_system_units<<<grid_for(nsys + 1, 128), 128, 0, st>>>(nsys, ws->sysgeom.as<SysGeom>(),
-                                                              ws->cell_start.as<int>(), n, a->unit_begin.as<int>());
-      sites_launch(ws, a, req, nsys, lay, F_dev, feat_dev);
-      k_unit_outputs<<<grid_for(nsys, 128), 128, 0, st>>>(nsys, a->unit_out.as<double>(), E_dev, W_dev);
-      ws->launches += 2;
+      batch_launch(ws, a, req, lay, E_dev, F_dev, W_dev, feat_dev);
     } catch (...) {
       cudaGraph_t g = nullptr;
       cudaStreamEndCapture(st, &g);
@@ -775,6 +824,7 @@ void ace_batch_graph(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, dou
     PFW_CUDA(cudaGraphInstantiate(&a->graph_exec, a->graph, 0));
     a->graph_key = key;
     a->graph_key.alloc_epoch = g_alloc_epoch.load();  // after the planning run's allocations
+    a->graph_sys = ws->prep.sys;
   }
   PFW_CUDA(cudaGraphLaunch(a->graph_exec, st));
   ws->launches += a->graph_kernels;  // kernels replayed by the graph
