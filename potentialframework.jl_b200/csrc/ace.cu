@@ -14,7 +14,7 @@
 //                 site, or up to 16 sites of one system of a batch)
 //   k_ace_gather  F_k = Σ_{e∈out(k)} g_e - g_{rev(e)}  (reduce_site!,
 //                 NeighbourList/execution.jl:256-273, without a racing scatter)
-//   k_ace_reduce  E and the 3×3 virial from per-site partials
+//   reduce_site_parts  E and the 3×3 virial from per-site partials (reduce.cu)
 //
 // Batches of systems evaluate in units that never span two systems, summed
 // per system in a fixed order, so energies, virials and the per-structure
@@ -189,30 +189,11 @@ __global__ void k_ace_gather(int n, const int* __restrict__ off, int cap, const 
   F[3 * o + 2] = f2;
 }
 
-// Per-site [E, W(9)] → totals; site energies in original order.
-__global__ void k_ace_reduce(int n, const double* __restrict__ site_out, const int* __restrict__ perm,
-                             double* __restrict__ E, double* __restrict__ W, double* __restrict__ Esite) {
-  __shared__ double sh[10][256];
-  Kahan acc[10];
-  for (int s = threadIdx.x; s < n; s += blockDim.x) {
-#pragma unroll
-    for (int k = 0; k < 10; ++k) acc[k].add(site_out[10 * (size_t)s + k]);
-    if (Esite) Esite[perm[s]] = site_out[10 * (size_t)s];
-  }
-#pragma unroll
-  for (int k = 0; k < 10; ++k) sh[k][threadIdx.x] = acc[k].s - acc[k].c;
-  __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if (threadIdx.x < st)
-#pragma unroll
-      for (int k = 0; k < 10; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    if (E) E[0] = sh[0][0];
-    if (W)
-      for (int k = 0; k < 9; ++k) W[k] = sh[k + 1][0];
-  }
+// Site energies in original order.
+__global__ void k_site_energies(int n, const double* __restrict__ site_out, const int* __restrict__ perm,
+                                double* __restrict__ Esite) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) Esite[perm[s]] = site_out[10 * (size_t)s];
 }
 
 __global__ void k_iota(int n, int* __restrict__ out) {
@@ -692,8 +673,11 @@ void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   sites_launch(ws, a, req, n, ub, a->unit_out.as<double>(), nullptr, lay, F_dev);
   double* E = E_dev ? E_dev : static_cast<double*>(ws->out_E.ensure(sizeof(double)));
   double* W = W_dev ? W_dev : static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
-  k_ace_reduce<<<1, 256, 0, st>>>(n, a->unit_out.as<double>(), ws->perm.as<int>(), E, W, Esite);
-  ws->launches += 1;
+  if (n > 0) {
+    k_site_energies<<<grid_for(n, 256), 256, 0, st>>>(n, a->unit_out.as<double>(), ws->perm.as<int>(), Esite);
+    ws->launches += 1;
+  }
+  reduce_site_parts(ws, a->unit_out.as<double>(), n, E, W);
   ws->stage_end(2);
   a->evaluated = true;
   ace_check(ws, a);

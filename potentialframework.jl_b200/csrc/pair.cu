@@ -4,13 +4,13 @@
 // pair callbacks of PairPotentials/models.jl:138-176 (PreparedSmooth) and
 // lennard_jones.jl:5-33 (LennardJonesRadial).
 //
-// Decomposition: one warp owns one home cell.  Lanes are the home cell's
-// atoms (chunks of 32); for each stencil cell-image the warp stages the
-// neighbour cell's sorted positions (double4 x,y,z,species) in shared memory
-// and every lane walks them as a broadcast.  Each lane accumulates the force
-// on ITS atom only (full directed list), so forces are written once, in
-// place, with no racing scatter; E and W take half of every directed pair.
-// Per-cell partials (E, 6 virial components) are reduced deterministically.
+// Decomposition: one warp owns one home cell and walks every directed
+// neighbour of its atoms with the shared traversal (traverse.cuh: stencil
+// entries resolved per lane, FP32x2 prefilter, per-lane candidate lists,
+// exact FP64 re-test).  Each lane accumulates the force on ITS atom only
+// (full directed list), so forces are written once, in place, with no racing
+// scatter; E and W take half of every directed pair.  Per-cell partials (E, 6
+// virial components) are reduced deterministically (reduce.cu).
 #include <algorithm>
 #include <cmath>
 
@@ -54,8 +54,10 @@ __device__ __forceinline__ void write_cell_parts(double* cellpart, int cell, int
   }
 }
 
+// 5 resident 4-warp blocks per SM: 96 registers/thread and 5 × 42 KB of
+// candidate lists fit one SM; measured faster than register-limited 4.
 #ifndef PFW_PAIR_MINBLOCKS
-#define PFW_PAIR_MINBLOCKS 1
+#define PFW_PAIR_MINBLOCKS 5
 #endif
 
 // Plain FP64 path.  MODE 0: displacement = (x_j - x_i) + cell shift;
@@ -124,163 +126,98 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
   write_cell_parts(cellpart, cell, lane, acc_e, w, np, npairs);
 }
 
-// Mixed form: candidate test and pair arithmetic in FP32 on coordinates
-// relative to the home cell's first atom, the FP64 wrap/image shift applied
-// before the conversion; energy and virial per neighbour chunk folded into
-// Kahan-compensated FP64 accumulators.
-template <int KIND>
-__global__ void __launch_bounds__(PAIR_WARPS * 32)
+// Mixed form: the same traversal and the same FP64 cutoff decision as the
+// plain path (so the neighbour set is the reference's), with the pair
+// arithmetic in FP32 on the FP64 displacement rounded to FP32.  Forces
+// accumulate per atom in FP32; energy and virial terms accumulate in FP32
+// over at most MIXED_CHUNK pairs and are then folded into Kahan-compensated
+// FP64 accumulators.
+constexpr int MIXED_CHUNK = 16;
+
+#ifndef PFW_PAIR32_MINBLOCKS
+#define PFW_PAIR32_MINBLOCKS 4
+#endif
+
+template <int KIND, int MODE>
+__global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
     k_pair32(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
              const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
              double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
-  __shared__ float4 stage[PAIR_WARPS][32];
+  __shared__ WarpStage stage[PAIR_WARPS];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * PAIR_WARPS + warp;
   if (cell >= ncells) return;
   const SysGeom& g = sysv[cell_sys[cell]];
-  const int b = cell_start[cell], e = cell_start[cell + 1];
   Kahan ke, kw[6];
+  float ce = 0.f, cw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  int cn = 0;
   unsigned long long np = 0;
-  if (b < e) {
-    const int local = cell - g.cell_begin;
-    const int key[3] = {local / (g.dims[1] * g.dims[2]), (local / g.dims[2]) % g.dims[1], local % g.dims[2]};
-    const int cnt0 = stencil_count(g, 0), cnt1 = stencil_count(g, 1), cnt2 = stencil_count(g, 2);
-    const bool rint_path = g.minimum_image && !g.fast_shift;
-    const double4 ref = pos[b];
-    const float c2 = (float)g.c2;
-    const float invc2 = (float)prm.invc2, eps4 = (float)prm.eps4, eps24 = (float)prm.eps24,
-                sigma2 = (float)prm.sigma2, shift = (float)prm.shift;
-    const float L0 = (float)g.L[0], L1 = (float)g.L[1], L2 = (float)g.L[2];
-    for (int i0 = b; i0 < e; i0 += 32) {
-      const int i = i0 + lane;
-      const bool have = i < e;
-      const double4 pd = have ? pos[i] : ref;
-      const float xi = (float)(pd.x - ref.x), yi = (float)(pd.y - ref.y), zi_ = (float)(pd.z - ref.z);
-      float arow[4] = {0, 0, 0, 0};
-      if (KIND == 0) {
-        const int zi = min(max((int)pd.w, 0), prm.nz - 1);
+  int cur = -1;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  float arow[4] = {0.f, 0.f, 0.f, 0.f};
+  const bool want_f = prm.want_f;
+  const float invc2 = (float)prm.invc2, eps4 = (float)prm.eps4, eps24 = (float)prm.eps24,
+              sigma2 = (float)prm.sigma2, shift = (float)prm.shift;
+  auto fold = [&]() {
+    ke.add((double)ce);
 #pragma unroll
-        for (int z = 0; z < 4; ++z) arow[z] = z < prm.nz ? (float)prm.A[zi * prm.nz + z] : 0.f;
-      }
-      float fx = 0, fy = 0, fz = 0;
-      for (int t0 = 0; t0 < cnt0; ++t0)
-        for (int t1 = 0; t1 < cnt1; ++t1)
-          for (int t2 = 0; t2 < cnt2; ++t2) {
-            const int off[3] = {stencil_offset(g, 0, t0), stencil_offset(g, 1, t1), stencil_offset(g, 2, t2)};
-            StencilEntry se;
-            stencil_entry(g, key, off, se);
-            if (se.cell < 0) continue;
-            const int jb = cell_start[se.cell], je = cell_start[se.cell + 1];
-            for (int j0 = jb; j0 < je; j0 += 32) {
-              const int nj = min(32, je - j0);
-              __syncwarp();
-              if (lane < nj) {
-                const double4 q = pos[j0 + lane];
-                double dx = q.x - ref.x, dy = q.y - ref.y, dz = q.z - ref.z;
-                if (!rint_path) {
-                  dx += se.sh[0];
-                  dy += se.sh[1];
-                  dz += se.sh[2];
-                }
-                stage[warp][lane] = make_float4((float)dx, (float)dy, (float)dz, (float)q.w);
-              } else {
-                stage[warp][lane] = make_float4(1e30f, 1e30f, 1e30f, 0.f);
-              }
-              __syncwarp();
-              if (!have) continue;
-              unsigned mask = 0u;
-#pragma unroll
-              for (int t = 0; t < 32; ++t) {
-                const float4 q = stage[warp][t];
-                float d0 = q.x - xi, d1 = q.y - yi, d2 = q.z - zi_;
-                if (rint_path) {
-                  d0 -= rintf(d0 / L0) * L0;
-                  d1 -= rintf(d1 / L1) * L1;
-                  d2 -= rintf(d2 / L2) * L2;
-                }
-                const float r2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2));
-                mask |= (r2 < c2 ? 1u : 0u) << t;
-              }
-              if (se.zero && i >= j0 && i < j0 + 32) mask &= ~(1u << (i - j0));
-              float ex = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
-              while (mask) {
-                const int t = __ffs(mask) - 1;
-                mask &= mask - 1u;
-                const float4 q = stage[warp][t];
-                float d0 = q.x - xi, d1 = q.y - yi, d2 = q.z - zi_;
-                if (rint_path) {
-                  d0 -= rintf(d0 / L0) * L0;
-                  d1 -= rintf(d1 / L1) * L1;
-                  d2 -= rintf(d2 / L2) * L2;
-                }
-                const float r2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2));
-                ++np;
-                float en, coef;
-                if (KIND == 0) {
-                  const int zj = (int)q.w;
-                  const float a = zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3];
-                  const float qq = 1.f - r2 * invc2;
-                  const float aq2 = a * qq * qq;
-                  en = aq2 * qq;
-                  coef = -6.f * aq2 * invc2;
-                } else {
-                  const float ir2 = __frcp_rn(r2);
-                  const float s2 = sigma2 * ir2;
-                  const float s6 = s2 * s2 * s2;
-                  en = eps4 * (s6 * s6 - s6) - shift;
-                  coef = eps24 * (s6 - 2.f * s6 * s6) * ir2;
-                }
-                const float gx = coef * d0, gy = coef * d1, gz = coef * d2;
-                fx += gx; fy += gy; fz += gz;
-                ex += en;
-                v0 += d0 * gx; v1 += d1 * gy; v2 += d2 * gz;
-                v3 += d0 * gy; v4 += d0 * gz; v5 += d1 * gz;
-              }
-              ke.add(ex);
-              kw[0].add(v0); kw[1].add(v1); kw[2].add(v2);
-              kw[3].add(v3); kw[4].add(v4); kw[5].add(v5);
-            }
-          }
-      if (have && prm.want_f) {
-        const int o = perm[i];
-        F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
-      }
+    for (int k = 0; k < 6; ++k) {
+      kw[k].add((double)cw[k]);
+      cw[k] = 0.f;
     }
+    ce = 0.f;
+    cn = 0;
+  };
+  warp_traverse_cell<MODE>(
+      g, cell, cell_start, pos, stage[warp], lane,
+      [&](int i, int, const double4& pi, const double4& pj, const StencilEntry&, const double* d, double r2d) {
+        if (i != cur) {
+          if (cur >= 0 && want_f) {
+            const int o = perm[cur];
+            F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
+          }
+          cur = i;
+          fx = fy = fz = 0.f;
+          if (KIND == 0) {
+            const int zi = min(max((int)pi.w, 0), prm.nz - 1);
+#pragma unroll
+            for (int z = 0; z < 4; ++z) arow[z] = z < prm.nz ? (float)prm.A[zi * prm.nz + z] : 0.f;
+          }
+        }
+        ++np;
+        const float d0 = (float)d[0], d1 = (float)d[1], d2 = (float)d[2];
+        const float r2 = (float)r2d;
+        float en, coef;
+        if (KIND == 0) {
+          const int zj = (int)pj.w;
+          const float a = zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3];
+          const float q = 1.f - r2 * invc2;
+          const float aq2 = a * q * q;
+          en = aq2 * q;
+          coef = -6.f * aq2 * invc2;
+        } else {
+          const float ir2 = __frcp_rn(r2);
+          const float s2 = sigma2 * ir2;
+          const float s6 = s2 * s2 * s2;
+          en = eps4 * (s6 * s6 - s6) - shift;
+          coef = eps24 * (s6 - 2.f * s6 * s6) * ir2;
+        }
+        const float gx = coef * d0, gy = coef * d1, gz = coef * d2;
+        fx += gx; fy += gy; fz += gz;
+        ce += en;
+        cw[0] += d0 * gx; cw[1] += d1 * gy; cw[2] += d2 * gz;
+        cw[3] += d0 * gy; cw[4] += d0 * gz; cw[5] += d1 * gz;
+        if (++cn == MIXED_CHUNK) fold();
+      });
+  if (cur >= 0 && want_f) {
+    const int o = perm[cur];
+    F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
   }
+  fold();
   double w[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) w[k] = kw[k].s - kw[k].c;
   write_cell_parts(cellpart, cell, lane, ke.s - ke.c, w, np, npairs);
-}
-
-// Deterministic reduction of per-cell partials → E and the 3×3 virial
-// (column-major, symmetric).  Kahan-compensated FP64.
-__global__ void k_reduce_parts(const double* __restrict__ parts, int nparts, int stride, double* __restrict__ E,
-                               double* __restrict__ W) {
-  __shared__ double sh[7][256];
-  Kahan acc[7];
-  for (int c = threadIdx.x; c < nparts; c += blockDim.x)
-#pragma unroll
-    for (int k = 0; k < 7; ++k) acc[k].add(parts[(size_t)stride * c + k]);
-#pragma unroll
-  for (int k = 0; k < 7; ++k) sh[k][threadIdx.x] = acc[k].s - acc[k].c;
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
-#pragma unroll
-      for (int k = 0; k < 7; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + s];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    if (E) E[0] = sh[0][0];
-    if (W) {
-      // components: xx, yy, zz, xy, xz, yz
-      W[0] = sh[1][0]; W[4] = sh[2][0]; W[8] = sh[3][0];
-      W[3] = W[1] = sh[4][0];
-      W[6] = W[2] = sh[5][0];
-      W[7] = W[5] = sh[6][0];
-    }
-  }
 }
 
 // Per-system reduction of a batch: block s sums the cells of system s.
@@ -357,10 +294,19 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   ws->stage_begin(1);
   if (ncells > 0) {
     dim3 grid(grid_for(ncells, PAIR_WARPS)), block(PAIR_WARPS * 32);
+    // the per-warp candidate lists make shared memory a residency limit:
+    // ask for the largest carveout
+    for (const void* k : {(const void*)k_pair64<0, 0>, (const void*)k_pair64<1, 0>, (const void*)k_pair64<0, 1>,
+                          (const void*)k_pair64<1, 1>, (const void*)k_pair32<0, 0>, (const void*)k_pair32<1, 0>,
+                          (const void*)k_pair32<0, 1>, (const void*)k_pair32<1, 1>})
+      PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     bool mixed = ws->opt.precision == PFW_PRECISION_MIXED;
-    if (mixed) {
-      if (m.kind == 0) k_pair32<0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
-      else k_pair32<1><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+    if (mixed && all_shift) {
+      if (m.kind == 0) k_pair32<0, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      else k_pair32<1, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+    } else if (mixed) {
+      if (m.kind == 0) k_pair32<0, 1><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      else k_pair32<1, 1><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
     } else if (all_shift) {
       if (m.kind == 0) k_pair64<0, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
       else k_pair64<1, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
@@ -377,7 +323,7 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   if (per_system) {
     if (P.nsys > 0) k_reduce_systems<<<P.nsys, 128, 0, st>>>(parts, dsys, 8, E_dev, W_dev);
   } else {
-    k_reduce_parts<<<1, 256, 0, st>>>(parts, ncells, 8, E, W);
+    reduce_pair_parts(ws, parts, ncells, 8, E, W);
   }
   ws->stage_end(2);
   ws->launches += 1;

@@ -100,7 +100,7 @@ struct pfw_ws {
       perm, inverse, pos, pos32, scan_tmp, minmax;
   // pair evaluation
   pfw::PairModel pair;
-  pfw::DevBuf cellpart, out_E, out_F, out_W, out_feat, counters;
+  pfw::DevBuf cellpart, out_E, out_F, out_W, out_feat, counters, red_partial;
   int64_t last_pairs = -1;
   // neighbour snapshot
   pfw::DevBuf nb_count, nb_offsets, nb_j, nb_S, nb_R;
@@ -133,6 +133,9 @@ void prepare_launch(pfw_ws* ws, bool wrap);    // device-only build, capturable
 void prepare_check(pfw_ws* ws);                // synchronise, raise on device flags
 void exclusive_scan_i32(pfw_ws* ws, const int32_t* in, int32_t* out, int64_t n);  // out has n+1 entries
 void exclusive_scan_i64(pfw_ws* ws, const int32_t* in, int64_t* out, int64_t n);
+// reduce.cu: deterministic partial sums → E[0] and W[9] (either may be null)
+void reduce_pair_parts(pfw_ws* ws, const double* parts, int nparts, int stride, double* E, double* W);
+void reduce_site_parts(pfw_ws* ws, const double* parts, int nparts, double* E, double* W);
 // pair.cu
 // per_system: E[s] and W[9s..] for every system of a batch
 void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system = false);

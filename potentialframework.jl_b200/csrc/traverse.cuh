@@ -24,7 +24,10 @@
 namespace pfw {
 
 constexpr int TRAVERSE_STAGE = 32;
-constexpr int LIST_K = 64;   // list capacity per lane
+#ifndef PFW_LIST_K
+#define PFW_LIST_K 64
+#endif
+constexpr int LIST_K = PFW_LIST_K;  // list capacity per lane (> TRAVERSE_STAGE)
 constexpr int LIST_NE = 32;  // stencil entries per block (one per lane)
 constexpr float PREFILTER_GUARD = 1.0f + 1.0f / 1024.0f;
 
