@@ -212,6 +212,69 @@ pfw_status pfw_batch_graph_launch(pfw_ws* ws, uint32_t request, double* E_dev, d
                                   double* W_dev, double* features_dev);
 pfw_status pfw_batch_graph_sync(pfw_ws* ws);
 
+/* ---- learned per-atom surrogate ----------------------------------------- */
+/* No GPU counterpart in the reference; the nearest CPU analogue is the
+ * invariant head ACEFeatureEnergy (ACE/feature_energy.jl:1-86).  A FEATURE
+ * MODEL (packed ACE tables restricted to low-order invariants: its nbasis
+ * invariants B = C·P, then its pair channels Q, nin = nbasis + nQ features
+ * per site) feeds an ensemble of MLPs per centre species,
+ * nin → hidden → hidden → 1 with SiLU, BF16 weights and FP32 arithmetic.
+ * Site energy = reference[z] + y_mean[z] + y_std[z]·mean over members;
+ * forces and virial follow from dE/dfeature through the ACE pullback.  A site
+ * falls back to the full ACE model (pfw_ace_model_load) when a standardised
+ * feature leaves [x_lo, x_hi] or the ensemble standard deviation of its
+ * energy exceeds tau (eV). */
+typedef struct pfw_mlp_params {
+  int32_t nz, members, nin, hidden;  /* members 1..4; nin, hidden multiples of 8 */
+  const uint16_t* W1;   /* [nz][members][hidden][nin]    BF16 bit patterns */
+  const float* b1;      /* [nz][members][hidden] */
+  const uint16_t* W2;   /* [nz][members][hidden][hidden] BF16 (row = output) */
+  const float* b2;      /* [nz][members][hidden] */
+  const uint16_t* w3;   /* [nz][members][hidden]         BF16 */
+  const float* b3;      /* [nz][members] */
+  const double* x_mean; /* [nz][nin] feature standardisation */
+  const double* x_std;
+  const float* x_lo;    /* [nz][nin] accepted standardised range, margin included */
+  const float* x_hi;
+  const double* y_mean; /* [nz] standardisation of (site energy - reference) */
+  const double* y_std;
+  double tau;           /* gate on the ensemble standard deviation (eV) */
+} pfw_mlp_params;
+
+#define PFW_MODEL_SURROGATE 2
+
+/* Load the feature model and (optionally, NULL) the MLP ensemble. */
+pfw_status pfw_surrogate_load(pfw_ws* ws, const pfw_ace_tables* features, const pfw_mlp_params* mlp);
+/* Per-site features of the current geometry (host, n × nin, original
+ * order): the training inputs. */
+pfw_status pfw_surrogate_features(pfw_ws* ws, double* features);
+/* Sites of the last surrogate evaluation and how many fell back to ACE. */
+pfw_status pfw_surrogate_stats(pfw_ws* ws, int64_t* fallback_sites, int64_t* sites);
+
+/* Ensemble training with hand-written forward/backward kernels: mean squared
+ * error on standardised site energies, Adam, one parameter vector per
+ * (species, member): [W1 hidden×nin | b1 | W2 hidden×hidden | b2 | w3 | b3]
+ * in FP32, nparams = hidden·nin + hidden² + 3·hidden + 1. */
+typedef struct pfw_mlp_shape {
+  int32_t nz, members, nin, hidden;
+} pfw_mlp_shape;
+typedef struct pfw_mlp_train_options {
+  int32_t epochs, batch;   /* batch: samples per member per step (multiple of 32) */
+  float lr, lr_final;      /* cosine decay from lr to lr_final */
+  uint64_t seed;           /* per-member sample orders */
+} pfw_mlp_train_options;
+/* Gradient of the mean squared error over the samples of each species for
+ * every (species, member) model: loss [nz·members], grad like params. */
+pfw_status pfw_mlp_param_grad(pfw_ws* ws, const pfw_mlp_shape* shape, const float* params, int64_t n,
+                              const float* X, const float* y, const int32_t* species, double* loss,
+                              float* grad);
+/* params: initial values in, trained values out.  X: n × nin standardised
+ * features, y: n standardised targets, species: n channels (host arrays).
+ * epoch_loss [epochs] (may be NULL): mean training loss over the models. */
+pfw_status pfw_mlp_train(pfw_ws* ws, const pfw_mlp_shape* shape, float* params, int64_t n, const float* X,
+                         const float* y, const int32_t* species, const pfw_mlp_train_options* options,
+                         float* epoch_loss);
+
 /* ---- device peak probe ------------------------------------------------- */
 /* Measured FP64 FMA throughput of the current device (TFLOP/s), used as the
  * FP64-pipe roofline denominator. */

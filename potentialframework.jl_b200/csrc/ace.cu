@@ -268,9 +268,8 @@ static void release_graph(AceDevice* a) {
   a->graph_key = GraphKey{};
 }
 
-void ace_free(pfw_ws* ws) {
-  if (!ws->ace) return;
-  AceDevice* a = ws->ace;
+static void free_device(AceDevice* a) {
+  if (!a) return;
   release_graph(a);
   DevBuf* bufs[] = {&a->r_len, &a->r_nodes, &a->r_coeff, &a->r_tr, &a->r_pow, &a->r_envk, &a->r_env,
                     &a->q_len, &a->q_nodes, &a->q_coeff, &a->q_tr, &a->q_pow, &a->q_envk, &a->q_env,
@@ -281,19 +280,40 @@ void ace_free(pfw_ws* ws) {
                     &a->batch_units, &a->batch_sys_units, &a->batch_out, &a->batch_feat};
   for (auto* b : bufs) b->release();
   delete a;
+}
+
+void ace_free(pfw_ws* ws) {
+  free_device(ws->ace);
   ws->ace = nullptr;
 }
 
-void ace_load(pfw_ws* ws, const pfw_ace_tables* t) {
+static void fill_model(pfw_ws* ws, AceDevice* a, const pfw_ace_tables* t);
+
+// Validated device copy of packed ACE tables (pack_model, ACE/adaptation.jl:78-98).
+static AceDevice* load_model(pfw_ws* ws, const pfw_ace_tables* t) {
   if (t->nz < 1 || t->nz > 16) throw Error(PFW_EINVAL, "ACE models support 1 to 16 species channels");
   if (t->lmax < 0 || t->lmax > ACE_LMAX) throw Error(PFW_EINVAL, "ACE lmax must be in 0..6");
   if (t->radial.nchannels < 1) throw Error(PFW_EINVAL, "empty radial basis");
   if (!(std::isfinite(t->cutoff) && t->cutoff > 0)) throw Error(PFW_EINVAL, "invalid ACE cutoff");
   if (t->ndensity < 1 || t->ndensity > 65534 || t->nproducts < 1 || t->nproducts > 65535)
     throw Error(PFW_EINVAL, "ACE basis size out of range (density <= 65534, products <= 65535)");
-  ace_free(ws);
   AceDevice* a = new AceDevice();
+  try {
+    fill_model(ws, a, t);
+  } catch (...) {
+    free_device(a);
+    throw;
+  }
+  return a;
+}
+
+void ace_load(pfw_ws* ws, const pfw_ace_tables* t) {
+  AceDevice* a = load_model(ws, t);
+  ace_free(ws);
   ws->ace = a;
+}
+
+static void fill_model(pfw_ws* ws, AceDevice* a, const pfw_ace_tables* t) {
   cudaStream_t st = ws->stream;
   const int nz = t->nz;
   a->nz = nz;
@@ -487,6 +507,7 @@ void ace_set_schedule(pfw_ws* ws, int chunk, int groups) {
 struct SiteLaunch {
   int nunits;
   const int* unit_begin;
+  const int* unit_sites;  // non-null: unit u is the single site unit_sites[u]
   int cap;
   const int* off;
   const double4* ed;
@@ -496,32 +517,33 @@ struct SiteLaunch {
   double* unit_feat;
   int want_grad;
   int* status;
+  SurParams sur;
 };
 
-template <int L, class T>
+template <int L, class T, bool SUR>
 static void launch_sites(const AceTables& p, const AceLayout& lay, const SiteLaunch& s, cudaStream_t st, int device) {
-  auto kern = k_ace_sites<L, T>;
+  auto kern = k_ace_sites<L, T, SUR>;
   PFW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total));
   int sms = 0, per_sm = 0;
   PFW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   PFW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ACE_GROUP * lay.G, lay.total));
   per_sm = std::max(per_sm, 1);
   const int blocks = std::max(1, std::min(sms * per_sm, (s.nunits + lay.G - 1) / lay.G));
-  kern<<<blocks, ACE_GROUP * lay.G, lay.total, st>>>(p, lay, s.nunits, s.unit_begin, s.cap, s.off, s.ed, s.pos, s.g,
-                                                     s.unit_out, s.unit_feat, s.want_grad, s.status);
+  kern<<<blocks, ACE_GROUP * lay.G, lay.total, st>>>(p, lay, s.sur, s.nunits, s.unit_begin, s.unit_sites, s.cap, s.off,
+                                                     s.ed, s.pos, s.g, s.unit_out, s.unit_feat, s.want_grad, s.status);
 }
 
-template <class T>
+template <class T, bool SUR = false>
 static void dispatch_sites(int lmax, const AceTables& p, const AceLayout& lay, const SiteLaunch& s, cudaStream_t st,
                            int device) {
   switch (lmax) {
-    case 0: launch_sites<0, T>(p, lay, s, st, device); break;
-    case 1: launch_sites<1, T>(p, lay, s, st, device); break;
-    case 2: launch_sites<2, T>(p, lay, s, st, device); break;
-    case 3: launch_sites<3, T>(p, lay, s, st, device); break;
-    case 4: launch_sites<4, T>(p, lay, s, st, device); break;
-    case 5: launch_sites<5, T>(p, lay, s, st, device); break;
-    default: launch_sites<6, T>(p, lay, s, st, device); break;
+    case 0: launch_sites<0, T, SUR>(p, lay, s, st, device); break;
+    case 1: launch_sites<1, T, SUR>(p, lay, s, st, device); break;
+    case 2: launch_sites<2, T, SUR>(p, lay, s, st, device); break;
+    case 3: launch_sites<3, T, SUR>(p, lay, s, st, device); break;
+    case 4: launch_sites<4, T, SUR>(p, lay, s, st, device); break;
+    case 5: launch_sites<5, T, SUR>(p, lay, s, st, device); break;
+    default: launch_sites<6, T, SUR>(p, lay, s, st, device); break;
   }
 }
 
@@ -606,9 +628,10 @@ static void sites_launch(pfw_ws* ws, AceDevice* a, uint32_t req, int nunits, con
   const int n = ws->prep.n;
   const bool want_grad = (req & (PFW_REQ_FORCES | PFW_REQ_VIRIAL)) != 0;
   const AceTables p = tables_of(a);
-  SiteLaunch s;
+  SiteLaunch s{};
   s.nunits = nunits;
   s.unit_begin = unit_begin;
+  s.unit_sites = nullptr;
   s.cap = a->cap;
   s.off = a->edge_off.as<int>();
   s.ed = a->edge_d.as<double4>();
@@ -868,6 +891,324 @@ double probe_fp64(pfw_ws* ws) {
   ws->launches += 2;
   const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
   return flops / (ms * 1e-3) / 1e12;
+}
+
+// ---------------------------------------------------------------------------
+// learned per-atom surrogate with gated ACE fallback
+// ---------------------------------------------------------------------------
+// The reference has no GPU surrogate; its closest analogue is the CPU
+// invariant head ACEFeatureEnergy (ACE/feature_energy.jl:1-86).  Here a
+// restricted ACE model (the low-order invariants and pair sums) produces 64
+// features per site inside the site kernel, an ensemble of BF16-weight MLPs
+// gives the site energy and dE/dfeature, and the ACE pullback turns that into
+// edge gradients.  Sites whose features leave the training range, or whose
+// ensemble disagrees by more than tau, are re-evaluated with the full ACE
+// model on the same environments.
+struct SurDevice {
+  AceDevice* fm = nullptr;  // the feature model (restricted ACE tables)
+  int nin = 0, H = 0, M = 0, nz = 0;
+  float tau = 0.f;
+  bool has_mlp = false;
+  DevBuf W1, W1T, W2, W2T, w3, b1, b2, b3, xm, xs, xlo, xhi, ym, ys, ccol_off, ccol_b, ccol_val;
+  DevBuf flags, fb_count, fb_list, fb_out, feat_all;
+  int64_t last_fallback = -1, last_sites = 0;
+};
+
+void sur_free(pfw_ws* ws) {
+  SurDevice* d = ws->sur;
+  if (!d) return;
+  free_device(d->fm);
+  DevBuf* bufs[] = {&d->W1, &d->W1T, &d->W2, &d->W2T, &d->w3, &d->b1, &d->b2, &d->b3, &d->xm, &d->xs, &d->xlo,
+                    &d->xhi, &d->ym, &d->ys, &d->ccol_off, &d->ccol_b, &d->ccol_val, &d->flags, &d->fb_count,
+                    &d->fb_list, &d->fb_out, &d->feat_all};
+  for (auto* b : bufs) b->release();
+  delete d;
+  ws->sur = nullptr;
+}
+
+void sur_load(pfw_ws* ws, const pfw_ace_tables* t, const pfw_mlp_params* mp) {
+  if (t->nbasis + t->pair.nchannels < 1) throw Error(PFW_EINVAL, "feature model has no features");
+  const int nin = t->nbasis + t->pair.nchannels;
+  if (mp) {
+    if (mp->nz != t->nz || mp->nin != nin) throw Error(PFW_ESHAPE, "MLP input shape does not match the feature model");
+    if (mp->members < 1 || mp->members > 4) throw Error(PFW_EINVAL, "ensemble of 1 to 4 members");
+    if (mp->hidden < 8 || mp->hidden > 256 || mp->hidden % 8 || nin % 8)
+      throw Error(PFW_EINVAL, "hidden width and input count must be multiples of 8 (hidden 8..256)");
+    if (!mp->W1 || !mp->b1 || !mp->W2 || !mp->b2 || !mp->w3 || !mp->b3 || !mp->x_mean || !mp->x_std ||
+        !mp->x_lo || !mp->x_hi || !mp->y_mean || !mp->y_std)
+      throw Error(PFW_EINVAL, "MLP parameter arrays are required");
+  }
+  AceDevice* fm = load_model(ws, t);
+  SurDevice* d = new SurDevice();
+  d->fm = fm;
+  try {
+    cudaStream_t st = ws->stream;
+    d->nin = nin;
+    d->nz = t->nz;
+    // coupling by product column: w_k = Σ_b C[b,k] dE/dB_b
+    std::vector<int> coff(t->nproducts + 1, 0);
+    for (int e = 0; e < t->ncoupling; ++e) coff[t->coupling_cols[e] + 1]++;
+    for (int k = 0; k < t->nproducts; ++k) coff[k + 1] += coff[k];
+    std::vector<int> cb(t->ncoupling);
+    std::vector<double> cv(t->ncoupling);
+    {
+      std::vector<int> fill(coff.begin(), coff.end() - 1);
+      for (int e = 0; e < t->ncoupling; ++e) {
+        const int q = fill[t->coupling_cols[e]]++;
+        cb[q] = t->coupling_rows[e];
+        cv[q] = t->coupling_vals[e];
+      }
+    }
+    upload(d->ccol_off, coff.data(), coff.size(), st);
+    upload(d->ccol_b, cb.data(), cb.size(), st);
+    upload(d->ccol_val, cv.data(), cv.size(), st);
+    if (mp) {
+      const int nz = mp->nz, M = mp->members, H = mp->hidden;
+      d->M = M;
+      d->H = H;
+      d->tau = (float)mp->tau;
+      const size_t n1 = (size_t)nz * M * H * nin, n2 = (size_t)nz * M * H * H;
+      std::vector<uint16_t> w1t(n1), w2t(n2);
+      for (int zm = 0; zm < nz * M; ++zm) {
+        for (int o = 0; o < H; ++o)
+          for (int i = 0; i < nin; ++i) w1t[((size_t)zm * nin + i) * H + o] = mp->W1[((size_t)zm * H + o) * nin + i];
+        for (int o = 0; o < H; ++o)
+          for (int i = 0; i < H; ++i) w2t[((size_t)zm * H + i) * H + o] = mp->W2[((size_t)zm * H + o) * H + i];
+      }
+      for (size_t k = 0; k < (size_t)nz * nin; ++k)
+        if (!(mp->x_std[k] > 0.0) || !std::isfinite(mp->x_mean[k]))
+          throw Error(PFW_EINVAL, "feature standardisation must be finite with positive scales");
+      upload(d->W1, mp->W1, n1, st);
+      upload(d->W1T, w1t.data(), n1, st);
+      upload(d->W2, mp->W2, n2, st);
+      upload(d->W2T, w2t.data(), n2, st);
+      upload(d->w3, mp->w3, (size_t)nz * M * H, st);
+      upload(d->b1, mp->b1, (size_t)nz * M * H, st);
+      upload(d->b2, mp->b2, (size_t)nz * M * H, st);
+      upload(d->b3, mp->b3, (size_t)nz * M, st);
+      upload(d->xm, mp->x_mean, (size_t)nz * nin, st);
+      upload(d->xs, mp->x_std, (size_t)nz * nin, st);
+      upload(d->xlo, mp->x_lo, (size_t)nz * nin, st);
+      upload(d->xhi, mp->x_hi, (size_t)nz * nin, st);
+      upload(d->ym, mp->y_mean, nz, st);
+      upload(d->ys, mp->y_std, nz, st);
+      d->has_mlp = true;
+    }
+    PFW_CUDA(cudaStreamSynchronize(st));
+  } catch (...) {
+    free_device(d->fm);
+    delete d;
+    throw;
+  }
+  sur_free(ws);
+  ws->sur = d;
+}
+
+// Per-site features in original order, own species block: out[o*nin + i].
+__global__ void k_site_features(int n, int nz, int nB, int nQ, const double* __restrict__ unit_feat,
+                                const double4* __restrict__ pos, const int* __restrict__ perm,
+                                double* __restrict__ out) {
+  const int nin = nB + nQ, nfeat = nz * nin;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n * nin) return;
+  const int s = k / nin, i = k - s * nin;
+  const int iz = min(max((int)pos[s].w, 0), nz - 1);
+  const double* f = unit_feat + (size_t)nfeat * s;
+  out[(size_t)perm[s] * nin + i] = i < nB ? f[iz * nB + i] : f[nz * nB + iz * nQ + (i - nB)];
+}
+
+static AceLayout choose_sur_layout(const AceTables& p, int device, int nin, int M, int H) {
+  int optin = 0;
+  PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  const int cand[][2] = {{32, 4}, {32, 3}, {16, 4}, {32, 2}, {16, 2}, {16, 1}, {8, 1}};
+  for (auto& c : cand) {
+    AceLayout lay;
+    lay.make(p, c[0], c[1], 1, nin, M, H);
+    if (lay.total <= (size_t)optin) return lay;
+  }
+  throw Error(PFW_EINVAL, "surrogate feature model too large for the site kernel's shared memory");
+}
+
+static void sur_prepare(pfw_ws* ws, SurDevice* d) {
+  AceDevice* a = d->fm;
+  cudaStream_t st = ws->stream;
+  ws->prep.valid = false;
+  prepare(ws, a->cutoff);
+  a->status.ensure(sizeof(int) * 4);
+  PFW_CUDA(cudaMemsetAsync(a->status.ptr, 0, sizeof(int) * 4, st));
+  build_edges(ws, a);
+  const int n = ws->prep.n;
+  a->n = n;
+  int* ub = static_cast<int*>(a->unit_begin.ensure(sizeof(int) * (n + 1)));
+  a->unit_out.ensure(sizeof(double) * 10 * std::max(n, 1));
+  k_iota<<<grid_for(n + 1, 256), 256, 0, st>>>(n, ub);
+  ws->launches += 1;
+}
+
+void sur_features(pfw_ws* ws, double* out_dev) {
+  SurDevice* d = ws->sur;
+  if (!d) throw Error(PFW_ESTATE, "no surrogate feature model loaded");
+  if (ws->max_species >= d->nz) throw Error(PFW_EINVAL, "feature model has no element channel for a species");
+  AceDevice* a = d->fm;
+  sur_prepare(ws, d);
+  const int n = ws->prep.n;
+  const AceTables p = tables_of(a);
+  AceLayout lay = choose_layout(p, ws->opt.device, 0, 0, 1);
+  const int nfeat = a->nz * (a->nB + a->nQ);
+  double* uf = static_cast<double*>(d->feat_all.ensure(sizeof(double) * (size_t)nfeat * std::max(n, 1)));
+  sites_launch(ws, a, PFW_REQ_ENERGY, n, a->unit_begin.as<int>(), a->unit_out.as<double>(), uf, lay, nullptr);
+  const int nin = a->nB + a->nQ;
+  if (n > 0) {
+    k_site_features<<<grid_for((int64_t)n * nin, 256), 256, 0, ws->stream>>>(
+        n, a->nz, a->nB, a->nQ, uf, ws->pos.as<double4>(), ws->perm.as<int>(), out_dev);
+    ws->launches += 1;
+  }
+  ws->stage_end(2);
+  ace_check(ws, a);
+}
+
+__global__ void k_flag_list(int n, const int* __restrict__ flags, const int* __restrict__ pos_excl,
+                            int* __restrict__ list) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n && flags[s]) list[pos_excl[s]] = s;
+}
+
+__global__ void k_scatter_sites(int count, const int* __restrict__ list, const double* __restrict__ fb_out,
+                                double* __restrict__ site_out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count * 10) return;
+  const int u = k / 10, c = k - u * 10;
+  site_out[10 * (size_t)list[u] + c] = fb_out[10 * (size_t)u + c];
+}
+
+void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev) {
+  SurDevice* d = ws->sur;
+  AceDevice* full = ws->ace;
+  if (!d || !d->has_mlp) throw Error(PFW_ESTATE, "no surrogate (feature model and MLP) loaded");
+  if (!full) throw Error(PFW_ESTATE, "the surrogate falls back to the ACE model: load it first");
+  if (full->cutoff != d->fm->cutoff || full->nz != d->nz)
+    throw Error(PFW_EINVAL, "surrogate feature model and ACE model differ in cutoff or species");
+  if (ws->max_species >= d->nz) throw Error(PFW_EINVAL, "feature model has no element channel for a species");
+  if (ws->opt.precision != PFW_PRECISION_FP64) throw Error(PFW_EINVAL, "the surrogate path runs in the FP64 workspace");
+  AceDevice* a = d->fm;
+  cudaStream_t st = ws->stream;
+  ws->stage_begin(3);
+  ws->stage_begin(0);
+  sur_prepare(ws, d);
+  ws->stage_end(0);
+  ws->stage_end(3);
+  const int n = ws->prep.n;
+  const bool want_grad = (req & (PFW_REQ_FORCES | PFW_REQ_VIRIAL)) != 0;
+  int* flags = static_cast<int*>(d->flags.ensure(sizeof(int) * std::max(n, 1)));
+  // surrogate pass over every site
+  const AceTables p = tables_of(a);
+  const AceLayout lay = choose_sur_layout(p, ws->opt.device, d->nin, d->M, d->H);
+  SiteLaunch s{};
+  s.nunits = n;
+  s.unit_begin = a->unit_begin.as<int>();
+  s.cap = a->cap;
+  s.off = a->edge_off.as<int>();
+  s.ed = a->edge_d.as<double4>();
+  s.pos = ws->pos.as<double4>();
+  s.g = a->edge_g.as<double>();
+  s.unit_out = a->unit_out.as<double>();
+  s.want_grad = want_grad;
+  s.status = a->status.as<int>();
+  SurParams& sp = s.sur;
+  sp.nin = d->nin;
+  sp.H = d->H;
+  sp.M = d->M;
+  sp.W1 = d->W1.as<unsigned short>();
+  sp.W1T = d->W1T.as<unsigned short>();
+  sp.W2 = d->W2.as<unsigned short>();
+  sp.W2T = d->W2T.as<unsigned short>();
+  sp.w3 = d->w3.as<unsigned short>();
+  sp.b1 = d->b1.as<float>();
+  sp.b2 = d->b2.as<float>();
+  sp.b3 = d->b3.as<float>();
+  sp.x_mean = d->xm.as<double>();
+  sp.x_std = d->xs.as<double>();
+  sp.x_lo = d->xlo.as<float>();
+  sp.x_hi = d->xhi.as<float>();
+  sp.y_mean = d->ym.as<double>();
+  sp.y_std = d->ys.as<double>();
+  sp.tau = d->tau;
+  sp.ccol_off = d->ccol_off.as<int>();
+  sp.ccol_b = d->ccol_b.as<int>();
+  sp.ccol_val = d->ccol_val.as<double>();
+  sp.flags = flags;
+  ws->stage_begin(1);
+  if (n > 0) {
+    dispatch_sites<double, true>(a->lmax, p, lay, s, st, ws->opt.device);
+    ws->launches += 1;
+  }
+  // fallback: the flagged sites with the full model on the same environments
+  int* pos_excl = static_cast<int*>(d->fb_count.ensure(sizeof(int) * (n + 1)));
+  exclusive_scan_i32(ws, flags, pos_excl, n);
+  int count = 0;
+  PFW_CUDA(cudaMemcpyAsync(&count, pos_excl + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PFW_CUDA(cudaStreamSynchronize(st));
+  d->last_fallback = count;
+  d->last_sites = n;
+  if (count > 0) {
+    int* list = static_cast<int*>(d->fb_list.ensure(sizeof(int) * count));
+    double* fb_out = static_cast<double*>(d->fb_out.ensure(sizeof(double) * 10 * count));
+    k_flag_list<<<grid_for(n, 256), 256, 0, st>>>(n, flags, pos_excl, list);
+    const AceTables pf = tables_of(full);
+    const AceLayout lf = choose_layout(pf, ws->opt.device, full->sched_chunk, full->sched_groups, 0);
+    SiteLaunch f = s;
+    f.sur = SurParams{};
+    f.nunits = count;
+    f.unit_begin = nullptr;
+    f.unit_sites = list;
+    f.unit_out = fb_out;
+    dispatch_sites<double, false>(full->lmax, pf, lf, f, st, ws->opt.device);
+    k_scatter_sites<<<grid_for((int64_t)count * 10, 256), 256, 0, st>>>(count, list, fb_out, a->unit_out.as<double>());
+    ws->launches += 3;
+  }
+  ws->stage_end(1);
+  ws->stage_begin(2);
+  if (F_dev && n > 0) {
+    if (want_grad) {
+      k_ace_gather<<<grid_for(n, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(),
+                                                     a->edge_g.as<double>(), ws->perm.as<int>(), F_dev);
+      ws->launches += 1;
+    } else {
+      PFW_CUDA(cudaMemsetAsync(F_dev, 0, sizeof(double) * 3 * n, st));
+    }
+  }
+  double* Esite = static_cast<double*>(a->site_E_orig.ensure(sizeof(double) * std::max(n, 1)));
+  if (n > 0) {
+    k_site_energies<<<grid_for(n, 256), 256, 0, st>>>(n, a->unit_out.as<double>(), ws->perm.as<int>(), Esite);
+    ws->launches += 1;
+  }
+  double* E = E_dev ? E_dev : static_cast<double*>(ws->out_E.ensure(sizeof(double)));
+  double* W = W_dev ? W_dev : static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
+  reduce_site_parts(ws, a->unit_out.as<double>(), n, E, W);
+  ws->stage_end(2);
+  a->evaluated = true;
+  d->last_sites = n;
+  ace_check(ws, a);
+}
+
+void sur_stats(pfw_ws* ws, int64_t* fallback, int64_t* sites) {
+  SurDevice* d = ws->sur;
+  if (!d) throw Error(PFW_ESTATE, "no surrogate loaded");
+  if (fallback) *fallback = d->last_fallback;
+  if (sites) *sites = d->last_sites;
+}
+
+int sur_feature_width(pfw_ws* ws) {
+  if (!ws->sur) throw Error(PFW_ESTATE, "no surrogate feature model loaded");
+  return ws->sur->nin;
+}
+
+void sur_site_energies(pfw_ws* ws, double* host) {
+  SurDevice* d = ws->sur;
+  if (!d || !d->fm->evaluated) throw Error(PFW_ESTATE, "no surrogate evaluation to report");
+  PFW_CUDA(cudaMemcpyAsync(host, d->fm->site_E_orig.ptr, sizeof(double) * d->fm->n, cudaMemcpyDeviceToHost,
+                           ws->stream));
+  PFW_CUDA(cudaStreamSynchronize(ws->stream));
 }
 
 }  // namespace pfw

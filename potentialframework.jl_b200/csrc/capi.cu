@@ -109,6 +109,14 @@ void upload_batch(pfw_ws* ws, int32_t nsys, const int64_t* offsets, const double
   ws->last_pairs = -1;
 }
 
+void dispatch_evaluate(pfw_ws* ws, int32_t model, uint32_t request, double* E, double* F, double* W) {
+  if (model == PFW_MODEL_PAIR) pfw::pair_evaluate(ws, request, E, F, W);
+  else if (model == PFW_MODEL_ACE) pfw::ace_evaluate(ws, request, E, F, W);
+  else if (model == PFW_MODEL_SURROGATE) pfw::sur_evaluate(ws, request, E, F, W);
+  else throw Error(PFW_EINVAL, "unknown model selector");
+  ws->last_model = model;
+}
+
 // Batch evaluation on device outputs (no host synchronisation for pairs).
 void evaluate_batch_device(pfw_ws* ws, int32_t model, uint32_t request, double* E, double* F, double* W,
                            double* feat) {
@@ -166,6 +174,7 @@ void pfw_ws_destroy(pfw_ws* ws) {
   cudaSetDevice(ws->opt.device);
   if (ws->stream) cudaStreamSynchronize(ws->stream);
   pfw::ace_free(ws);
+  pfw::sur_free(ws);
   pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
                          &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
                          &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
@@ -234,9 +243,7 @@ pfw_status pfw_evaluate_device(pfw_ws* ws, int32_t model, uint32_t request, doub
                                double* W_dev) {
   return guarded(ws, [&] {
     if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
-    if (model == PFW_MODEL_PAIR) pfw::pair_evaluate(ws, request, E_dev, F_dev, W_dev);
-    else if (model == PFW_MODEL_ACE) pfw::ace_evaluate(ws, request, E_dev, F_dev, W_dev);
-    else throw Error(PFW_EINVAL, "unknown model selector");
+    dispatch_evaluate(ws, model, request, E_dev, F_dev, W_dev);
   });
 }
 
@@ -248,9 +255,7 @@ pfw_status pfw_evaluate(pfw_ws* ws, int32_t model, uint32_t request, double* E, 
     double* dW = static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
     double* dF = (request & PFW_REQ_FORCES) ? static_cast<double*>(ws->out_F.ensure(sizeof(double) * 3 * std::max(n, 1)))
                                             : nullptr;
-    if (model == PFW_MODEL_PAIR) pfw::pair_evaluate(ws, request, dE, dF, dW);
-    else if (model == PFW_MODEL_ACE) pfw::ace_evaluate(ws, request, dE, dF, dW);
-    else throw Error(PFW_EINVAL, "unknown model selector");
+    dispatch_evaluate(ws, model, request, dE, dF, dW);
     double hE = 0, hW[9];
     unsigned long long np = 0;
     PFW_CUDA(cudaMemcpyAsync(&hE, dE, sizeof(double), cudaMemcpyDeviceToHost, ws->stream));
@@ -354,7 +359,47 @@ pfw_status pfw_batch_graph_sync(pfw_ws* ws) {
 }
 
 pfw_status pfw_site_energies(pfw_ws* ws, double* energies) {
-  return guarded(ws, [&] { pfw::ace_site_energies(ws, energies); });
+  return guarded(ws, [&] {
+    if (ws->last_model == PFW_MODEL_SURROGATE) pfw::sur_site_energies(ws, energies);
+    else pfw::ace_site_energies(ws, energies);
+  });
+}
+
+pfw_status pfw_surrogate_load(pfw_ws* ws, const pfw_ace_tables* features, const pfw_mlp_params* mlp) {
+  return guarded(ws, [&] {
+    if (!features) throw Error(PFW_EINVAL, "feature model tables required");
+    pfw::sur_load(ws, features, mlp);
+  });
+}
+
+pfw_status pfw_surrogate_features(pfw_ws* ws, double* features) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    if (!features) throw Error(PFW_EINVAL, "null output");
+    int32_t nin = 0;
+    pfw::sur_stats(ws, nullptr, nullptr);  // raises without a feature model
+    nin = pfw::sur_feature_width(ws);
+    double* d = static_cast<double*>(ws->out_feat.ensure(sizeof(double) * std::max<int64_t>(1, (int64_t)ws->n * nin)));
+    pfw::sur_features(ws, d);
+    if (ws->n > 0)
+      PFW_CUDA(cudaMemcpyAsync(features, d, sizeof(double) * (size_t)ws->n * nin, cudaMemcpyDeviceToHost, ws->stream));
+    PFW_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+pfw_status pfw_surrogate_stats(pfw_ws* ws, int64_t* fallback_sites, int64_t* sites) {
+  return guarded(ws, [&] { pfw::sur_stats(ws, fallback_sites, sites); });
+}
+
+pfw_status pfw_mlp_param_grad(pfw_ws* ws, const pfw_mlp_shape* shape, const float* params, int64_t n, const float* X,
+                              const float* y, const int32_t* species, double* loss, float* grad) {
+  return guarded(ws, [&] { pfw::mlp_param_grad(ws, shape, params, n, X, y, species, loss, grad); });
+}
+
+pfw_status pfw_mlp_train(pfw_ws* ws, const pfw_mlp_shape* shape, float* params, int64_t n, const float* X,
+                         const float* y, const int32_t* species, const pfw_mlp_train_options* options,
+                         float* epoch_loss) {
+  return guarded(ws, [&] { pfw::mlp_train(ws, shape, params, n, X, y, species, options, epoch_loss); });
 }
 
 pfw_status pfw_last_pair_count(pfw_ws* ws, int64_t* npairs) {

@@ -81,6 +81,7 @@ struct PairModel {
 };
 
 struct AceDevice;  // ace.cu
+struct SurDevice;  // ace.cu (surrogate)
 
 }  // namespace pfw
 
@@ -107,6 +108,8 @@ struct pfw_ws {
   int64_t nb_total = -1;
   // ACE
   pfw::AceDevice* ace = nullptr;
+  pfw::SurDevice* sur = nullptr;
+  int32_t last_model = -1;  // model selector of the last evaluation
   // bookkeeping
   uint64_t launches = 0;
   cudaStream_t own_stream = nullptr;  // the workspace's stream (stream may be the caller's)
@@ -153,6 +156,19 @@ void ace_evaluate_batch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
 void ace_batch_graph(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev);
 void ace_batch_graph_sync(pfw_ws* ws);
 double probe_fp64(pfw_ws* ws);
+// ace.cu: surrogate
+void sur_load(pfw_ws* ws, const pfw_ace_tables* features, const pfw_mlp_params* mlp);
+void sur_free(pfw_ws* ws);
+void sur_features(pfw_ws* ws, double* out_dev);
+void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev);
+void sur_stats(pfw_ws* ws, int64_t* fallback, int64_t* sites);
+void sur_site_energies(pfw_ws* ws, double* host);
+int sur_feature_width(pfw_ws* ws);
+// mlp.cu: ensemble training (mean-squared site-energy loss, Adam)
+void mlp_param_grad(pfw_ws* ws, const pfw_mlp_shape* shape, const float* params, int64_t n, const float* X,
+                    const float* y, const int32_t* species, double* loss, float* grad);
+void mlp_train(pfw_ws* ws, const pfw_mlp_shape* shape, float* params, int64_t n, const float* X, const float* y,
+               const int32_t* species, const pfw_mlp_train_options* opt, float* epoch_loss);
 
 inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
 }  // namespace pfw

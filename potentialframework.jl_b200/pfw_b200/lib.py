@@ -19,7 +19,7 @@ LIBPATH = os.path.join(PKG, "lib", "libpfw_b200.so")
 OK, EINVAL, EDOMAIN, ESHAPE, ECAPACITY, ECUDA, ETIMEDOUT, ESTATE = range(8)
 REQ_E, REQ_F, REQ_V = 1, 2, 4
 FP64, MIXED = 0, 1
-MODEL_PAIR, MODEL_ACE = 0, 1
+MODEL_PAIR, MODEL_ACE, MODEL_SURROGATE = 0, 1, 2
 
 
 class pfw_options(C.Structure):
@@ -98,6 +98,13 @@ def load():
     L.pfw_evaluate_batch_device.argtypes = [vp, C.c_int32, C.c_uint32, vp, vp, vp, vp]
     L.pfw_batch_graph_launch.argtypes = [vp, C.c_uint32, vp, vp, vp, vp]
     L.pfw_batch_graph_sync.argtypes = [vp]
+    L.pfw_surrogate_load.argtypes = [vp, C.POINTER(pfw_ace_tables), vp]
+    L.pfw_surrogate_features.argtypes = [vp, dp]
+    L.pfw_surrogate_stats.argtypes = [vp, i64p, i64p]
+    L.pfw_mlp_param_grad.argtypes = [vp, vp, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_float), i32p, dp, C.POINTER(C.c_float)]
+    L.pfw_mlp_train.argtypes = [vp, vp, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_float),
+                                C.POINTER(C.c_float), i32p, vp, C.POINTER(C.c_float)]
     _lib = L
     return L
 
@@ -265,6 +272,60 @@ class Handle:
 
     def set_stream(self, stream_ptr):
         self.check(self.L.pfw_set_stream(self.ws, stream_ptr))
+
+    # --- learned surrogate ----------------------------------------------
+    def surrogate(self, feature_model, sur=None, tau=None):
+        """Load the feature model and (optionally) a trained surrogate.Surrogate."""
+        self._sur_tables = feature_model.tables()
+        self._sur_model = feature_model
+        self._sur_struct = sur.mlp_struct(tau) if sur is not None else None
+        arg = C.byref(self._sur_struct) if sur is not None else None
+        self.check(self.L.pfw_surrogate_load(self.ws, C.byref(self._sur_tables), arg))
+        self.sur_nin = feature_model.nbasis + feature_model.pair.nchannels
+
+    def surrogate_features(self):
+        out = np.zeros((self.n, self.sur_nin))
+        self.check(self.L.pfw_surrogate_features(self.ws, ptr(out, C.c_double)))
+        return out
+
+    def surrogate_stats(self):
+        a = np.zeros(2, np.int64)
+        self.check(self.L.pfw_surrogate_stats(self.ws, ptr(a[:1], C.c_int64), ptr(a[1:], C.c_int64)))
+        return int(a[0]), int(a[1])
+
+    def _mlp_shape(self, P, nin):
+        from .surrogate import HIDDEN, pfw_mlp_shape
+        nz, M, _ = P.shape
+        self._shape = pfw_mlp_shape(nz, M, nin, HIDDEN)
+        return self._shape
+
+    def mlp_param_grad(self, P, X, y, Z):
+        P = np.ascontiguousarray(P, np.float32)
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        Z = np.ascontiguousarray(Z, np.int32)
+        shape = self._mlp_shape(P, X.shape[1])
+        loss = np.zeros(P.shape[0] * P.shape[1])
+        grad = np.zeros_like(P)
+        self.check(self.L.pfw_mlp_param_grad(self.ws, C.byref(shape), ptr(P, C.c_float), len(y), ptr(X, C.c_float),
+                                             ptr(y, C.c_float), ptr(Z, C.c_int32), ptr(loss, C.c_double),
+                                             ptr(grad, C.c_float)))
+        return loss.reshape(P.shape[:2]), grad
+
+    def mlp_train(self, P, X, y, Z, *, epochs, batch, lr, lr_final, seed):
+        """Train in place (P: FP32 [nz, M, nparams]); returns the per-epoch mean loss."""
+        from .surrogate import pfw_mlp_train_options
+        assert P.dtype == np.float32 and P.flags.c_contiguous
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        Z = np.ascontiguousarray(Z, np.int32)
+        shape = self._mlp_shape(P, X.shape[1])
+        opt = pfw_mlp_train_options(int(epochs), int(batch), float(lr), float(lr_final), int(seed))
+        hist = np.zeros(int(epochs), np.float32)
+        self.check(self.L.pfw_mlp_train(self.ws, C.byref(shape), ptr(P, C.c_float), len(y), ptr(X, C.c_float),
+                                        ptr(y, C.c_float), ptr(Z, C.c_int32), C.byref(opt),
+                                        ptr(hist, C.c_float)))
+        return hist
 
     def probe_fp64(self):
         v = np.zeros(1)

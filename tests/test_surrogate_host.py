@@ -1,0 +1,71 @@
+"""Host side of the learned surrogate: the restricted feature model reproduces
+the selected invariants and pair sums of the full ACE model exactly (CPU
+oracle), the numpy MLP reference that the GPU gradient check uses agrees with
+finite differences, and BF16 rounding is round-to-nearest-even."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pfw_b200 import ace_generate as G
+from pfw_b200 import surrogate as S
+from pfw_b200 import workloads as WL
+from pfw_b200.ace_model import read_resolved
+
+
+@pytest.fixture(scope="module")
+def models():
+    m = read_resolved(G.generate_b2_model())
+    feat, sel = S.restrict_model(m)
+    return m, feat, sel
+
+
+def test_feature_model_shape(models):
+    m, feat, sel = models
+    order = S.invariant_orders(m)
+    assert feat.nbasis + feat.pair.nchannels == S.NIN
+    assert all(order[b] in (1, 2) for b in sel)
+    assert sel == sorted(sel, key=lambda b: (order[b], b))
+    assert feat.lmax <= m.lmax and feat.ndensity < m.ndensity and feat.nproducts < m.nproducts
+
+
+def test_feature_model_reproduces_selected_invariants(models):
+    m, feat, sel = models
+    s = WL.b2(seed=1, nc=3)
+    rf = O.AceOracle(m).evaluate(s.X, s.H, s.pbc, s.species, request=1, features=True)["features"]
+    rr = O.AceOracle(feat).evaluate(s.X, s.H, s.pbc, s.species, request=1, features=True)["features"]
+    nz, nB, nQ, nb = m.nz, m.nbasis, m.pair.nchannels, feat.nbasis
+    for z in range(nz):
+        full = np.concatenate([rf[:, z * nB + np.array(sel)], rf[:, nz * nB + z * nQ:nz * nB + (z + 1) * nQ]], 1)
+        red = np.concatenate([rr[:, z * nb:(z + 1) * nb], rr[:, nz * nb + z * nQ:nz * nb + (z + 1) * nQ]], 1)
+        assert np.array_equal(full, red)
+
+
+def test_numpy_mlp_reference_gradients():
+    nin, H = 8, S.HIDDEN
+    P = S.init_params(1, 1, nin, H, seed=3)[0, 0].astype(np.float64)
+    P[H * nin:H * nin + H] = 0.1  # nonzero biases
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(5, nin))
+    t = rng.normal(size=5)
+    loss, g = S.mlp_param_grad_reference(P, x, t, nin, H)
+    for k in rng.choice(len(P), 12, replace=False):
+        e = np.zeros_like(P)
+        e[k] = 1e-6
+        fd = (S.mlp_param_grad_reference(P + e, x, t, nin, H)[0] - S.mlp_param_grad_reference(P - e, x, t, nin, H)[0]) / 2e-6
+        assert abs(fd - g[k]) <= 1e-6 + 1e-5 * abs(g[k])
+    y, dydx = S.mlp_forward(P, x, nin, H)
+    for i in range(nin):
+        e = np.zeros(nin)
+        e[i] = 1e-6
+        fd = (S.mlp_forward(P, x + e, nin, H)[0] - S.mlp_forward(P, x - e, nin, H)[0]) / 2e-6
+        assert np.allclose(fd, dydx[:, i], rtol=1e-5, atol=1e-7)
+
+
+def test_bf16_rounding():
+    vals = np.array([1.0, 1.00390625, 1.005859375, -2.5, 3.0e-3, 65504.0], np.float32)
+    b = S.to_bf16_bits(vals)
+    assert b[0] == 0x3F80
+    assert b[1] == 0x3F80  # 1 + 2^-8: tie, rounds to even
+    assert b[2] == 0x3F81  # 1 + 3·2^-9: above the tie
+    back = S.from_bf16_bits(b)
+    assert np.all(np.abs(back - vals) <= np.abs(vals) * 2.0 ** -8)
