@@ -90,6 +90,17 @@ class Workload:
             raise SystemExit(f"unknown workload {name}")
         self.n = len(self.sys)
 
+    def tune(self, h):
+        """ACE only: pick the site-kernel schedule by timing every one that fits (autotune.py)."""
+        if self.kind != "ace":
+            return
+        from pfw_b200 import autotune
+        s = self.sys
+        h.set_geometry(s.X, s.H, s.pbc, s.species)
+        path = os.path.join(tempfile.gettempdir(), "pfw_b200_bench_autotune.json")
+        c, g, ms = autotune.tune(h, self.ace, lambda: h.evaluate(1, 7), self.n, path=path)
+        self.config["schedule"] = dict(chunk=c, groups=g, tuned_ms={k: round(v, 3) for k, v in ms.items()})
+
     def bind(self, h):
         if self.kind == "pair":
             kind, params, c = self.pair
@@ -336,6 +347,7 @@ def run_b200(args):
     h = lib.Handle(lib.FP64, device=local)
     h.check(h.L.pfw_set_stream(h.ws, ctypes.c_void_p(stream.cuda_stream)))
     w.bind(h)
+    w.tune(h)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     if dist:
         dist.barrier()
@@ -417,12 +429,16 @@ def forms(args, dev, stream, flush, F_head):
         h = lib.Handle(lib.FP64, device=dev.index)
         h.check(h.L.pfw_set_stream(h.ws, ctypes.c_void_p(stream.cuda_stream)))
         w.bind(h)
+        w.tune(h)
         ms, stage, _ = time_device(h, w, dev, lib, steps, 3, flush, stream)
         ms = float(np.mean(ms))
         out[w.config["workload"] + "_fp64"] = dict(value=w.n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms,
                                                    kernel_ms=float(stage[:, 1].mean()))
+        if "schedule" in w.config:
+            out[w.config["workload"] + "_fp64"]["schedule"] = w.config["schedule"]
         h.close()
     out["ace_batch4096_fp64_graph"] = batch_form(dev, stream, flush)
+    out["surrogate_b2_80_1024000"] = surrogate_form(dev, stream, flush)
     for name in ("lj", "ace"):
         w = Workload(name)
         h64 = lib.Handle(lib.FP64, device=dev.index)
@@ -472,6 +488,14 @@ def batch_form(dev, stream, flush, nsys=4096, steps=20):
     ptrs = [ctypes.c_void_p(t.data_ptr()) for t in (E, F, W, X)]
     torch.cuda.synchronize()
 
+    from pfw_b200 import autotune
+
+    def eager_sync():
+        h.evaluate_batch_device(lib.MODEL_ACE, 7, *ptrs)
+
+    c, g, tuned = autotune.tune(h, model, eager_sync, n, nsys,
+                                path=os.path.join(tempfile.gettempdir(), "pfw_b200_bench_autotune.json"))
+
     def replay():
         h.batch_graph_launch(7, *ptrs)
 
@@ -513,9 +537,80 @@ def batch_form(dev, stream, flush, nsys=4096, steps=20):
     return dict(value=n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms, systems=nsys, atoms=n,
                 eager_ms_per_step=res["eager"]["ms"], eager_value=n / (res["eager"]["ms"] * 1e-3),
                 kernels_per_replay=res["graph"]["launches_per_step"], features_per_system=nfeat,
+                schedule=dict(chunk=c, groups=g, tuned_ms={k: round(v, 2) for k, v in tuned.items()}),
                 max_abs_err_vs_single_system=dict(energy=err_e, force=err_f, sample=32),
                 note="n log-uniform [8,256], triclinic lengths U[6,14] Å, angles U[70,110]°, hard core 1.6 Å, "
                      "n/V <= 0.11 Å^-3 (cells redrawn), species 50/50; synthetic ACE model; FP64")
+
+
+def surrogate_form(dev, stream, flush, steps=5):
+    """Learned surrogate of the synthetic ACE model: trained with the library's
+    MLP kernels on 208,000 B2 environments (13 lattices of 16,000 atoms,
+    displacement sigma evenly spread over [0.03, 0.25] Å, full-model site
+    energies as labels), evaluated on B2 2·80³ = 1,024,000 atoms (sigma
+    0.08 Å) against plain FP64 ACE on the same system."""
+    import torch
+
+    from pfw_b200 import ace_generate as G
+    from pfw_b200 import lib
+    from pfw_b200 import surrogate as S
+    from pfw_b200 import workloads as WL
+    from pfw_b200.ace_model import read_resolved
+    model = read_resolved(G.generate_b2_model())
+    feat, sel = S.restrict_model(model)
+    h = lib.Handle(lib.FP64, device=dev.index)
+    t0 = time.perf_counter()
+    X, E, Z = S.training_set(h, model, feat, n_lattices=13, nc=20, seed=11)
+    t1 = time.perf_counter()
+    sur = S.train(h, feat, sel, X, E, Z, epochs=40, batch=512, lr=2e-3, lr_final=2e-5, seed=7)
+    t2 = time.perf_counter()
+    h.close()
+    sysb = WL.b2(seed=12, nc=80, sigma=0.08)
+    n = len(sysb)
+    h = lib.Handle(lib.FP64, device=dev.index)
+    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+    h.ace(model)
+    h.surrogate(feat, sur)
+    Xd = torch.from_numpy(sysb.X).to(dev)
+    Sd = torch.from_numpy(sysb.species).to(dev)
+    Ed = torch.zeros(1, dtype=torch.float64, device=dev)
+    Fd = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    Wd = torch.zeros(9, dtype=torch.float64, device=dev)
+    ptrs = [ctypes.c_void_p(t.data_ptr()) for t in (Ed, Fd, Wd)]
+    res = {}
+    for label, sel_model in (("surrogate", lib.MODEL_SURROGATE), ("ace", lib.MODEL_ACE)):
+        h.set_geometry_device(n, ctypes.c_void_p(Xd.data_ptr()), sysb.H, sysb.pbc, ctypes.c_void_p(Sd.data_ptr()))
+        for _ in range(2):
+            h.evaluate_device(sel_model, 7, *ptrs)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            h.set_geometry_device(n, ctypes.c_void_p(Xd.data_ptr()), sysb.H, sysb.pbc, ctypes.c_void_p(Sd.data_ptr()))
+            h.evaluate_device(sel_model, 7, *ptrs)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        res[label] = dict(ms=float(np.mean(ms)), E=float(Ed.item()), F=Fd.cpu().numpy().copy())
+        if label == "surrogate":
+            res["fallback"] = h.surrogate_stats()
+    h.close()
+    dF = res["surrogate"]["F"] - res["ace"]["F"]
+    fb, ns = res["fallback"]
+    ms_s, ms_a = res["surrogate"]["ms"], res["ace"]["ms"]
+    return dict(value=n / (ms_s * 1e-3), unit="atoms/s", ms_per_step=ms_s, atoms=n,
+                plain_ace_value=n / (ms_a * 1e-3), plain_ace_ms_per_step=ms_a, speedup_vs_plain_ace=ms_a / ms_s,
+                force_rmse_vs_ace=float(np.sqrt(np.mean(dF ** 2))), force_max_err_vs_ace=float(np.abs(dF).max()),
+                energy_err_per_atom_vs_ace=abs(res["surrogate"]["E"] - res["ace"]["E"]) / n,
+                fallback_sites=fb, fallback_fraction=fb / max(ns, 1),
+                training=dict(environments=int(len(E)), epochs=40, members=S.MEMBERS, features=S.NIN,
+                              hidden=S.HIDDEN, final_loss=sur.history[-1], label_s=t1 - t0, train_s=t2 - t1,
+                              tau_eV=sur.tau),
+                note="MLP 64->64->64->1 SiLU, BF16 weights, FP32 arithmetic, ensemble of 4 per species; "
+                     "features: the 8 order-1 and first 48 order-2 invariants plus 8 pair radial sums; "
+                     "gate: standardised training range +-5 % or ensemble std > tau; FP64 features and pullback")
 
 
 def main():

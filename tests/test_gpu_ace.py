@@ -116,3 +116,19 @@ def test_mixed_precision_form(b2model):
     rmse = float(np.sqrt(np.mean((F32 - F64) ** 2)))
     assert rmse <= 1e-3, rmse
     assert abs(E32 - E64) <= 1e-5 * abs(E64)
+
+
+def test_autotune_picks_fastest_and_caches(b2model, tmp_path):
+    from pfw_b200 import autotune
+    s = WL.b2(nc=6, seed=7)
+    h = lib.Handle(lib.FP64)
+    h.ace(b2model)
+    h.set_geometry(s.X, s.H, s.pbc, s.species)
+    path = str(tmp_path / "tune.json")
+    c, g, ms = autotune.tune(h, b2model, lambda: h.evaluate(lib.MODEL_ACE, 7), len(s.species), path=path, reps=2)
+    assert f"{c}x{g}" == min(ms, key=ms.get) and len(ms) >= 3
+    E1, F1, W1 = h.evaluate(lib.MODEL_ACE, 7)
+    r = O.AceOracle(b2model).evaluate(s.X, s.H, s.pbc, s.species)
+    assert close(F1, r["forces"]) and abs(E1 - r["energy"]) <= 1e-10 * abs(r["energy"])
+    c2, g2, ms2 = autotune.tune(h, b2model, lambda: None, len(s.species), path=path)
+    assert (c2, g2) == (c, g) and ms2 == ms
