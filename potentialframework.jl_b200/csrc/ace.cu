@@ -520,7 +520,7 @@ struct SiteLaunch {
   SurParams sur;
 };
 
-template <int L, class T, bool SUR>
+template <int L, class T, int SUR>
 static void launch_sites(const AceTables& p, const AceLayout& lay, const SiteLaunch& s, cudaStream_t st, int device) {
   auto kern = k_ace_sites<L, T, SUR>;
   PFW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total));
@@ -533,7 +533,7 @@ static void launch_sites(const AceTables& p, const AceLayout& lay, const SiteLau
                                                      s.ed, s.pos, s.g, s.unit_out, s.unit_feat, s.want_grad, s.status);
 }
 
-template <class T, bool SUR = false>
+template <class T, int SUR = 0>
 static void dispatch_sites(int lmax, const AceTables& p, const AceLayout& lay, const SiteLaunch& s, cudaStream_t st,
                            int device) {
   switch (lmax) {
@@ -909,8 +909,8 @@ struct SurDevice {
   int nin = 0, H = 0, M = 0, nz = 0;
   float tau = 0.f;
   bool has_mlp = false;
-  DevBuf W1, W1T, W2, W2T, w3, b1, b2, b3, xm, xs, xlo, xhi, ym, ys, ccol_off, ccol_b, ccol_val;
-  DevBuf flags, fb_count, fb_list, fb_out, feat_all;
+  DevBuf W1, W2, w3, b1, b2, b3, xm, xs, xlo, xhi, ym, ys, ccol_off, ccol_b, ccol_val;
+  DevBuf flags, fb_count, fb_list, fb_out, site_A, site_feat, site_df, site_e, feat_out, zlist, zcount;
   int64_t last_fallback = -1, last_sites = 0;
 };
 
@@ -918,13 +918,17 @@ void sur_free(pfw_ws* ws) {
   SurDevice* d = ws->sur;
   if (!d) return;
   free_device(d->fm);
-  DevBuf* bufs[] = {&d->W1, &d->W1T, &d->W2, &d->W2T, &d->w3, &d->b1, &d->b2, &d->b3, &d->xm, &d->xs, &d->xlo,
-                    &d->xhi, &d->ym, &d->ys, &d->ccol_off, &d->ccol_b, &d->ccol_val, &d->flags, &d->fb_count,
-                    &d->fb_list, &d->fb_out, &d->feat_all};
+  DevBuf* bufs[] = {&d->W1, &d->W2, &d->w3, &d->b1, &d->b2, &d->b3, &d->xm, &d->xs, &d->xlo, &d->xhi, &d->ym,
+                    &d->ys, &d->ccol_off, &d->ccol_b, &d->ccol_val, &d->flags, &d->fb_count, &d->fb_list,
+                    &d->fb_out, &d->site_A, &d->site_feat, &d->site_df, &d->site_e, &d->feat_out, &d->zlist,
+                    &d->zcount};
   for (auto* b : bufs) b->release();
   delete d;
   ws->sur = nullptr;
 }
+
+constexpr int SUR_MAXW = 64;   // MLP kernel: nin, hidden <= 64
+constexpr int SUR_TILE = 64;   // sites per MLP tile
 
 void sur_load(pfw_ws* ws, const pfw_ace_tables* t, const pfw_mlp_params* mp) {
   if (t->nbasis + t->pair.nchannels < 1) throw Error(PFW_EINVAL, "feature model has no features");
@@ -932,11 +936,14 @@ void sur_load(pfw_ws* ws, const pfw_ace_tables* t, const pfw_mlp_params* mp) {
   if (mp) {
     if (mp->nz != t->nz || mp->nin != nin) throw Error(PFW_ESHAPE, "MLP input shape does not match the feature model");
     if (mp->members < 1 || mp->members > 4) throw Error(PFW_EINVAL, "ensemble of 1 to 4 members");
-    if (mp->hidden < 8 || mp->hidden > 256 || mp->hidden % 8 || nin % 8)
-      throw Error(PFW_EINVAL, "hidden width and input count must be multiples of 8 (hidden 8..256)");
+    if (mp->hidden < 1 || mp->hidden > SUR_MAXW || nin > SUR_MAXW)
+      throw Error(PFW_EINVAL, "the surrogate MLP supports up to 64 inputs and 64 hidden units");
     if (!mp->W1 || !mp->b1 || !mp->W2 || !mp->b2 || !mp->w3 || !mp->b3 || !mp->x_mean || !mp->x_std ||
         !mp->x_lo || !mp->x_hi || !mp->y_mean || !mp->y_std)
       throw Error(PFW_EINVAL, "MLP parameter arrays are required");
+    for (size_t k = 0; k < (size_t)mp->nz * nin; ++k)
+      if (!(mp->x_std[k] > 0.0) || !std::isfinite(mp->x_mean[k]))
+        throw Error(PFW_EINVAL, "feature standardisation must be finite with positive scales");
   }
   AceDevice* fm = load_model(ws, t);
   SurDevice* d = new SurDevice();
@@ -967,21 +974,8 @@ void sur_load(pfw_ws* ws, const pfw_ace_tables* t, const pfw_mlp_params* mp) {
       d->M = M;
       d->H = H;
       d->tau = (float)mp->tau;
-      const size_t n1 = (size_t)nz * M * H * nin, n2 = (size_t)nz * M * H * H;
-      std::vector<uint16_t> w1t(n1), w2t(n2);
-      for (int zm = 0; zm < nz * M; ++zm) {
-        for (int o = 0; o < H; ++o)
-          for (int i = 0; i < nin; ++i) w1t[((size_t)zm * nin + i) * H + o] = mp->W1[((size_t)zm * H + o) * nin + i];
-        for (int o = 0; o < H; ++o)
-          for (int i = 0; i < H; ++i) w2t[((size_t)zm * H + i) * H + o] = mp->W2[((size_t)zm * H + o) * H + i];
-      }
-      for (size_t k = 0; k < (size_t)nz * nin; ++k)
-        if (!(mp->x_std[k] > 0.0) || !std::isfinite(mp->x_mean[k]))
-          throw Error(PFW_EINVAL, "feature standardisation must be finite with positive scales");
-      upload(d->W1, mp->W1, n1, st);
-      upload(d->W1T, w1t.data(), n1, st);
-      upload(d->W2, mp->W2, n2, st);
-      upload(d->W2T, w2t.data(), n2, st);
+      upload(d->W1, mp->W1, (size_t)nz * M * H * nin, st);
+      upload(d->W2, mp->W2, (size_t)nz * M * H * H, st);
       upload(d->w3, mp->w3, (size_t)nz * M * H, st);
       upload(d->b1, mp->b1, (size_t)nz * M * H, st);
       upload(d->b2, mp->b2, (size_t)nz * M * H, st);
@@ -1004,29 +998,223 @@ void sur_load(pfw_ws* ws, const pfw_ace_tables* t, const pfw_mlp_params* mp) {
   ws->sur = d;
 }
 
-// Per-site features in original order, own species block: out[o*nin + i].
-__global__ void k_site_features(int n, int nz, int nB, int nQ, const double* __restrict__ unit_feat,
-                                const double4* __restrict__ pos, const int* __restrict__ perm,
-                                double* __restrict__ out) {
-  const int nin = nB + nQ, nfeat = nz * nin;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n * nin) return;
-  const int s = k / nin, i = k - s * nin;
-  const int iz = min(max((int)pos[s].w, 0), nz - 1);
-  const double* f = unit_feat + (size_t)nfeat * s;
-  out[(size_t)perm[s] * nin + i] = i < nB ? f[iz * nB + i] : f[nz * nB + iz * nQ + (i - nB)];
-}
-
-static AceLayout choose_sur_layout(const AceTables& p, int device, int nin, int M, int H) {
+static AceLayout choose_sur_layout(const AceTables& p, int device, int pass) {
   int optin = 0;
   PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   const int cand[][2] = {{32, 4}, {32, 3}, {16, 4}, {32, 2}, {16, 2}, {16, 1}, {8, 1}};
   for (auto& c : cand) {
     AceLayout lay;
-    lay.make(p, c[0], c[1], 1, nin, M, H);
+    lay.make(p, c[0], c[1], 0, pass);
     if (lay.total <= (size_t)optin) return lay;
   }
   throw Error(PFW_EINVAL, "surrogate feature model too large for the site kernel's shared memory");
+}
+
+// Sites of each species (lists in any order; every site's result is
+// independent of its position in the list).
+__global__ void k_species_lists(int n, int nz, const double4* __restrict__ pos, int* __restrict__ count,
+                                int* __restrict__ list) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int z = min(max((int)pos[s].w, 0), nz - 1);
+  list[(size_t)z * n + atomicAdd(count + z, 1)] = s;
+}
+
+__device__ __forceinline__ float bf16f(unsigned short b) { return __uint_as_float((unsigned)b << 16); }
+
+// The MLP ensemble on a tile of 64 sites of one species: standardised
+// inputs, forward and backward passes of every member as 64×64 tiles in
+// shared memory (FP32, BF16-valued weights), the site energy without the
+// reference, dE/dfeature and the gate.  Thread (r, c) owns rows r + 16i and
+// columns c + 16j (i, j < 4) of every 64×64 product.
+__global__ void __launch_bounds__(256)
+    k_sur_mlp(SurParams sp, int n, const int* __restrict__ count, const int* __restrict__ list) {
+  extern __shared__ float smf[];
+  const int z = blockIdx.y, tile = blockIdx.x;
+  const int cnt = count[z];
+  const int l0 = tile * SUR_TILE;
+  if (l0 >= cnt) return;
+  const int rows = min(SUR_TILE, cnt - l0);
+  const int* L = list + (size_t)z * n + l0;
+  const int nin = sp.nin, H = sp.H, M = sp.M, ST = SUR_MAXW + 1;
+  float* X = smf;                 // [64][ST] standardised inputs
+  float* W1 = X + SUR_TILE * ST;  // [H][ST]
+  float* W2 = W1 + SUR_MAXW * ST; // [H][ST]
+  float* H1 = W2 + SUR_MAXW * ST;
+  float* S1 = H1 + SUR_TILE * ST;
+  float* H2 = S1 + SUR_TILE * ST;
+  float* S2 = H2 + SUR_TILE * ST;
+  float* D2 = S2 + SUR_TILE * ST;
+  float* D1 = D2 + SUR_TILE * ST;
+  float* ym = D1 + SUR_TILE * ST;  // [4][64]
+  float* vec = ym + 4 * SUR_TILE;  // b1, b2, w3 of a member: [3][64]
+  int* gate = reinterpret_cast<int*>(vec + 3 * SUR_MAXW);  // [64]
+  const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
+  for (int k = tid; k < SUR_TILE * SUR_MAXW; k += 256) {
+    const int r = k / SUR_MAXW, i = k - r * SUR_MAXW;
+    float x = 0.f;
+    if (r < rows && i < nin) {
+      const double raw = sp.site_feat[(size_t)L[r] * nin + i];
+      x = (float)((raw - sp.x_mean[z * nin + i]) / sp.x_std[z * nin + i]);
+    }
+    X[r * ST + i] = x;
+  }
+  if (tid < SUR_TILE) gate[tid] = 0;
+  __syncthreads();
+  for (int k = tid; k < rows * nin; k += 256) {
+    const int r = k / nin, i = k - r * nin;
+    const float x = X[r * ST + i];
+    if (!(x >= sp.x_lo[z * nin + i] && x <= sp.x_hi[z * nin + i])) gate[r] = 1;  // NaN-safe
+  }
+  float dx[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) dx[a][b] = 0.f;
+  for (int m = 0; m < M; ++m) {
+    const size_t zm = (size_t)z * M + m;
+    __syncthreads();
+    for (int k = tid; k < H * nin; k += 256) W1[(k / nin) * ST + k % nin] = bf16f(sp.W1[zm * H * nin + k]);
+    for (int k = tid; k < H * H; k += 256) W2[(k / H) * ST + k % H] = bf16f(sp.W2[zm * H * H + k]);
+    for (int k = tid; k < H; k += 256) {
+      vec[k] = sp.b1[zm * H + k];
+      vec[SUR_MAXW + k] = sp.b2[zm * H + k];
+      vec[2 * SUR_MAXW + k] = bf16f(sp.w3[zm * H + k]);
+    }
+    __syncthreads();
+    // layer 1: Z1 = X·W1ᵀ + b1
+    {
+      float acc[4][4] = {};
+      for (int k = 0; k < nin; ++k) {
+        float a[4], b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          a[q] = X[(tr + 16 * q) * ST + k];
+          b[q] = W1[(tc + 16 * q) * ST + k];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int r = tr + 16 * i, o = tc + 16 * j;
+          if (o < H) {
+            const float zz = acc[i][j] + vec[o];
+            const float sg = 1.f / (1.f + expf(-zz));
+            H1[r * ST + o] = zz * sg;
+            S1[r * ST + o] = sg * (1.f + zz * (1.f - sg));
+          }
+        }
+    }
+    __syncthreads();
+    // layer 2: Z2 = H1·W2ᵀ + b2
+    {
+      float acc[4][4] = {};
+      for (int k = 0; k < H; ++k) {
+        float a[4], b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          a[q] = H1[(tr + 16 * q) * ST + k];
+          b[q] = W2[(tc + 16 * q) * ST + k];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int r = tr + 16 * i, o = tc + 16 * j;
+          if (o < H) {
+            const float zz = acc[i][j] + vec[SUR_MAXW + o];
+            const float sg = 1.f / (1.f + expf(-zz));
+            H2[r * ST + o] = zz * sg;
+            S2[r * ST + o] = sg * (1.f + zz * (1.f - sg));
+            D2[r * ST + o] = vec[2 * SUR_MAXW + o] * S2[r * ST + o];
+          }
+        }
+    }
+    __syncthreads();
+    // output layer
+    if (tid < SUR_TILE) {
+      float y = sp.b3[zm];
+      for (int o = 0; o < H; ++o) y = fmaf(vec[2 * SUR_MAXW + o], H2[tid * ST + o], y);
+      ym[m * SUR_TILE + tid] = y;
+    }
+    // D1 = (D2·W2) ⊙ S1
+    {
+      float acc[4][4] = {};
+      for (int o = 0; o < H; ++o) {
+        float a[4], b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          a[q] = D2[(tr + 16 * q) * ST + o];
+          b[q] = W2[o * ST + tc + 16 * q];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int r = tr + 16 * i, c = tc + 16 * j;
+          if (c < H) D1[r * ST + c] = acc[i][j] * S1[r * ST + c];
+        }
+    }
+    __syncthreads();
+    // dX += D1·W1
+    for (int o = 0; o < H; ++o) {
+      float a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = D1[(tr + 16 * q) * ST + o];
+        b[q] = W1[o * ST + tc + 16 * q];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dx[i][j] = fmaf(a[i], b[j], dx[i][j]);
+    }
+  }
+  __syncthreads();
+  const double ysd = sp.y_std[z];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = tr + 16 * i;
+    if (r >= rows) continue;
+    const size_t s = L[r];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = tc + 16 * j;
+      if (c < nin) sp.site_df[s * nin + c] = ysd * (double)(dx[i][j] / (float)M) / sp.x_std[z * nin + c];
+    }
+  }
+  if (tid < rows) {
+    float mean = 0.f;
+    for (int m = 0; m < M; ++m) mean += ym[m * SUR_TILE + tid];
+    mean /= (float)M;
+    float var = 0.f;
+    for (int m = 0; m < M; ++m) var += (ym[m * SUR_TILE + tid] - mean) * (ym[m * SUR_TILE + tid] - mean);
+    var /= (float)M;
+    const int s = L[tid];
+    sp.site_e[s] = sp.y_mean[z] + ysd * (double)mean;
+    sp.flags[s] = (gate[tid] || !(ysd * (double)sqrtf(var) <= (double)sp.tau)) ? 1 : 0;
+  }
+}
+
+static size_t sur_mlp_smem() {
+  const int ST = SUR_MAXW + 1;
+  return sizeof(float) * ((size_t)SUR_TILE * ST * 7 + (size_t)SUR_MAXW * ST * 2 + 4 * SUR_TILE + 3 * SUR_MAXW) +
+         sizeof(int) * SUR_TILE;
 }
 
 static void sur_prepare(pfw_ws* ws, SurDevice* d) {
@@ -1045,26 +1233,81 @@ static void sur_prepare(pfw_ws* ws, SurDevice* d) {
   ws->launches += 1;
 }
 
+static SiteLaunch sur_launch(pfw_ws* ws, SurDevice* d, int n, bool want_grad) {
+  AceDevice* a = d->fm;
+  SiteLaunch s{};
+  s.nunits = n;
+  s.unit_begin = a->unit_begin.as<int>();
+  s.cap = a->cap;
+  s.off = a->edge_off.as<int>();
+  s.ed = a->edge_d.as<double4>();
+  s.pos = ws->pos.as<double4>();
+  s.g = a->edge_g.as<double>();
+  s.unit_out = a->unit_out.as<double>();
+  s.want_grad = want_grad;
+  s.status = a->status.as<int>();
+  SurParams& sp = s.sur;
+  sp.nin = d->nin;
+  sp.H = d->H;
+  sp.M = d->M;
+  sp.W1 = d->W1.as<unsigned short>();
+  sp.W2 = d->W2.as<unsigned short>();
+  sp.w3 = d->w3.as<unsigned short>();
+  sp.b1 = d->b1.as<float>();
+  sp.b2 = d->b2.as<float>();
+  sp.b3 = d->b3.as<float>();
+  sp.x_mean = d->xm.as<double>();
+  sp.x_std = d->xs.as<double>();
+  sp.x_lo = d->xlo.as<float>();
+  sp.x_hi = d->xhi.as<float>();
+  sp.y_mean = d->ym.as<double>();
+  sp.y_std = d->ys.as<double>();
+  sp.tau = d->tau;
+  sp.ccol_off = d->ccol_off.as<int>();
+  sp.ccol_b = d->ccol_b.as<int>();
+  sp.ccol_val = d->ccol_val.as<double>();
+  const size_t nn = std::max(n, 1);
+  sp.flags = static_cast<int*>(d->flags.ensure(sizeof(int) * nn));
+  sp.site_A = static_cast<double*>(d->site_A.ensure(sizeof(double) * nn * a->D));
+  sp.site_feat = static_cast<double*>(d->site_feat.ensure(sizeof(double) * nn * d->nin));
+  sp.site_df = static_cast<double*>(d->site_df.ensure(sizeof(double) * nn * d->nin));
+  sp.site_e = static_cast<double*>(d->site_e.ensure(sizeof(double) * nn));
+  return s;
+}
+
+// Feature pass: A-basis and own-species features of every site.
+static void sur_feature_pass(pfw_ws* ws, SurDevice* d, const SiteLaunch& s) {
+  AceDevice* a = d->fm;
+  const AceTables p = tables_of(a);
+  if (s.nunits > 0) {
+    dispatch_sites<double, 1>(a->lmax, p, choose_sur_layout(p, ws->opt.device, 1), s, ws->stream, ws->opt.device);
+    ws->launches += 1;
+  }
+}
+
+// Per-site features in original order: out[o*nin + i].
+__global__ void k_permute_rows(int n, int w, const double* __restrict__ in, const int* __restrict__ perm,
+                               double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n * w) return;
+  const int s = k / w, i = k - s * w;
+  out[(size_t)perm[s] * w + i] = in[k];
+}
+
 void sur_features(pfw_ws* ws, double* out_dev) {
   SurDevice* d = ws->sur;
   if (!d) throw Error(PFW_ESTATE, "no surrogate feature model loaded");
   if (ws->max_species >= d->nz) throw Error(PFW_EINVAL, "feature model has no element channel for a species");
-  AceDevice* a = d->fm;
   sur_prepare(ws, d);
   const int n = ws->prep.n;
-  const AceTables p = tables_of(a);
-  AceLayout lay = choose_layout(p, ws->opt.device, 0, 0, 1);
-  const int nfeat = a->nz * (a->nB + a->nQ);
-  double* uf = static_cast<double*>(d->feat_all.ensure(sizeof(double) * (size_t)nfeat * std::max(n, 1)));
-  sites_launch(ws, a, PFW_REQ_ENERGY, n, a->unit_begin.as<int>(), a->unit_out.as<double>(), uf, lay, nullptr);
-  const int nin = a->nB + a->nQ;
+  SiteLaunch s = sur_launch(ws, d, n, false);
+  sur_feature_pass(ws, d, s);
   if (n > 0) {
-    k_site_features<<<grid_for((int64_t)n * nin, 256), 256, 0, ws->stream>>>(
-        n, a->nz, a->nB, a->nQ, uf, ws->pos.as<double4>(), ws->perm.as<int>(), out_dev);
+    k_permute_rows<<<grid_for((int64_t)n * d->nin, 256), 256, 0, ws->stream>>>(n, d->nin, s.sur.site_feat,
+                                                                               ws->perm.as<int>(), out_dev);
     ws->launches += 1;
   }
-  ws->stage_end(2);
-  ace_check(ws, a);
+  ace_check(ws, d->fm);
 }
 
 __global__ void k_flag_list(int n, const int* __restrict__ flags, const int* __restrict__ pos_excl,
@@ -1099,50 +1342,30 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   ws->stage_end(3);
   const int n = ws->prep.n;
   const bool want_grad = (req & (PFW_REQ_FORCES | PFW_REQ_VIRIAL)) != 0;
-  int* flags = static_cast<int*>(d->flags.ensure(sizeof(int) * std::max(n, 1)));
-  // surrogate pass over every site
   const AceTables p = tables_of(a);
-  const AceLayout lay = choose_sur_layout(p, ws->opt.device, d->nin, d->M, d->H);
-  SiteLaunch s{};
-  s.nunits = n;
-  s.unit_begin = a->unit_begin.as<int>();
-  s.cap = a->cap;
-  s.off = a->edge_off.as<int>();
-  s.ed = a->edge_d.as<double4>();
-  s.pos = ws->pos.as<double4>();
-  s.g = a->edge_g.as<double>();
-  s.unit_out = a->unit_out.as<double>();
-  s.want_grad = want_grad;
-  s.status = a->status.as<int>();
-  SurParams& sp = s.sur;
-  sp.nin = d->nin;
-  sp.H = d->H;
-  sp.M = d->M;
-  sp.W1 = d->W1.as<unsigned short>();
-  sp.W1T = d->W1T.as<unsigned short>();
-  sp.W2 = d->W2.as<unsigned short>();
-  sp.W2T = d->W2T.as<unsigned short>();
-  sp.w3 = d->w3.as<unsigned short>();
-  sp.b1 = d->b1.as<float>();
-  sp.b2 = d->b2.as<float>();
-  sp.b3 = d->b3.as<float>();
-  sp.x_mean = d->xm.as<double>();
-  sp.x_std = d->xs.as<double>();
-  sp.x_lo = d->xlo.as<float>();
-  sp.x_hi = d->xhi.as<float>();
-  sp.y_mean = d->ym.as<double>();
-  sp.y_std = d->ys.as<double>();
-  sp.tau = d->tau;
-  sp.ccol_off = d->ccol_off.as<int>();
-  sp.ccol_b = d->ccol_b.as<int>();
-  sp.ccol_val = d->ccol_val.as<double>();
-  sp.flags = flags;
   ws->stage_begin(1);
+  SiteLaunch s = sur_launch(ws, d, n, false);
+  // 1. features and A-basis of every site
+  sur_feature_pass(ws, d, s);
+  // 2. the MLP ensemble per species, tiles of 64 sites
+  int* zc = static_cast<int*>(d->zcount.ensure(sizeof(int) * d->nz));
+  int* zl = static_cast<int*>(d->zlist.ensure(sizeof(int) * (size_t)std::max(n, 1) * d->nz));
+  PFW_CUDA(cudaMemsetAsync(zc, 0, sizeof(int) * d->nz, st));
   if (n > 0) {
-    dispatch_sites<double, true>(a->lmax, p, lay, s, st, ws->opt.device);
+    k_species_lists<<<grid_for(n, 256), 256, 0, st>>>(n, d->nz, ws->pos.as<double4>(), zc, zl);
+    const size_t smem = sur_mlp_smem();
+    PFW_CUDA(cudaFuncSetAttribute(k_sur_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_sur_mlp<<<dim3(grid_for(n, SUR_TILE), d->nz), 256, smem, st>>>(s.sur, n, zc, zl);
+    ws->launches += 2;
+  }
+  // 3. pullback with the per-site weights
+  s.want_grad = want_grad;
+  if (n > 0) {
+    dispatch_sites<double, 2>(a->lmax, p, choose_sur_layout(p, ws->opt.device, 2), s, st, ws->opt.device);
     ws->launches += 1;
   }
   // fallback: the flagged sites with the full model on the same environments
+  int* flags = s.sur.flags;
   int* pos_excl = static_cast<int*>(d->fb_count.ensure(sizeof(int) * (n + 1)));
   exclusive_scan_i32(ws, flags, pos_excl, n);
   int count = 0;
@@ -1162,7 +1385,7 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
     f.unit_begin = nullptr;
     f.unit_sites = list;
     f.unit_out = fb_out;
-    dispatch_sites<double, false>(full->lmax, pf, lf, f, st, ws->opt.device);
+    dispatch_sites<double, 0>(full->lmax, pf, lf, f, st, ws->opt.device);
     k_scatter_sites<<<grid_for((int64_t)count * 10, 256), 256, 0, st>>>(count, list, fb_out, a->unit_out.as<double>());
     ws->launches += 3;
   }
@@ -1187,7 +1410,6 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   reduce_site_parts(ws, a->unit_out.as<double>(), n, E, W);
   ws->stage_end(2);
   a->evaluated = true;
-  d->last_sites = n;
   ace_check(ws, a);
 }
 

@@ -50,14 +50,14 @@ struct AceTables {
 // Learned per-atom surrogate: an ensemble of M MLPs per centre species,
 // nin → H → H → 1 with SiLU, BF16 weights (FP32 arithmetic), on the
 // standardised low-order invariants of a restricted ACE model (its nB
-// invariants B = C·P, then its nQ pair sums).  Weight rows are stored both
-// ways ([o][i] and [i][o]) so the forward and backward passes read rows.
+// invariants B = C·P, then its nQ pair sums).  The site kernel runs twice
+// around the batched MLP (k_sur_mlp): pass 1 stores every site's A-basis and
+// features, pass 2 turns dE/dfeature into per-site product and pair weights
+// and runs the ACE pullback with them.
 struct SurParams {
   int nin, H, M;
   const unsigned short* W1;   // [nz][M][H][nin]  (BF16 bits)
-  const unsigned short* W1T;  // [nz][M][nin][H]
   const unsigned short* W2;   // [nz][M][H][H]
-  const unsigned short* W2T;  // [nz][M][H][H] transposed
   const unsigned short* w3;   // [nz][M][H]
   const float *b1, *b2;       // [nz][M][H]
   const float* b3;            // [nz][M]
@@ -69,6 +69,10 @@ struct SurParams {
   const int* ccol_b;
   const double* ccol_val;
   int* flags;                 // [n] per sorted site: 1 = outside the gate, evaluate with ACE
+  double* site_A;             // [n][D] A-basis of each site (feature pass → pullback pass)
+  double* site_feat;          // [n][nin] features of each site, own species block
+  double* site_df;            // [n][nin] dE/dfeature (MLP pass)
+  double* site_e;             // [n] MLP site energy without the reference energy
 };
 
 // shared-memory layout (byte offsets), computed identically on host and device
@@ -77,18 +81,17 @@ struct AceLayout {
   int RS, YS;  // odd row strides of the per-edge R and Y tables (bank-conflict padding)
   int feat;    // 1: per-unit fitting features are accumulated
   int nfeat;   // nz * (nB + nQ)
-  int sur;     // 1: surrogate scratch (MLP activations, per-site weights)
+  int sur;     // surrogate pass: 1 features, 2 pullback with per-site weights
   size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, tables_end;
   size_t group_bytes, total;
   // group-relative double offsets
-  int A, dA, Y, dY, R, dR, T1, T2, esc, F, QV, S, DF, WK, WQ, ints;
+  int A, dA, Y, dY, R, dR, T1, T2, esc, F, QV, WK, WQ, ints;
   __host__ __device__ static size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
-  __host__ __device__ void make(const AceTables& t, int ch, int g, int with_feat = 0, int sur_nin = 0, int sur_M = 0,
-                                int sur_H = 0) {
+  __host__ __device__ void make(const AceTables& t, int ch, int g, int with_feat = 0, int sur_pass = 0) {
     CH = ch;
     G = g;
-    sur = sur_nin > 0;
-    feat = with_feat || sur;
+    sur = sur_pass;
+    feat = with_feat || sur == 1;
     nfeat = t.nz * (t.nB + t.nQ);
     size_t o = 0;
     prods = o; o = align16(o + sizeof(ushort4) * t.P);
@@ -114,11 +117,8 @@ struct AceLayout {
     esc = d; d += CH * 10 + 4 * 10;  // per-edge scalars, then warp partials
     F = d; d += feat ? nfeat : 0;     // unit feature accumulator
     QV = d; d += feat ? CH * t.nQ : 0;  // pair radial values of the chunk
-    // surrogate: floats x[nin], 6 activation arrays [M*H], y[M], dx[M*nin], gate
-    S = d; d += sur ? (sur_nin + 6 * sur_M * sur_H + 4 + sur_M * sur_nin + 4 + 1) / 2 : 0;
-    DF = d; d += sur ? sur_nin : 0;  // dE/d(feature)
-    WK = d; d += sur ? t.P : 0;      // per-site product weights
-    WQ = d; d += sur ? t.nQ : 0;     // per-site pair weights
+    WK = d; d += sur == 2 ? t.P : 0;   // per-site product weights
+    WQ = d; d += sur == 2 ? t.nQ : 0;  // per-site pair weights
     ints = d; d += CH;               // 2 ints per edge
     group_bytes = align16(sizeof(double) * d);
     total = tables_end + group_bytes * G;
@@ -202,129 +202,7 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   }
 }
 
-__device__ __forceinline__ float bf16_lo(unsigned v) { return __uint_as_float(v << 16); }
-__device__ __forceinline__ float bf16_hi(unsigned v) { return __uint_as_float(v & 0xffff0000u); }
-
-// Σ_i row[i]·x[i] over n (a multiple of 8) BF16 weights, FP32 accumulation.
-__device__ __forceinline__ float bf16_dot(const unsigned short* __restrict__ row, const float* x, int n) {
-  const uint4* r = reinterpret_cast<const uint4*>(row);
-  float acc = 0.f;
-  for (int i = 0; i < n; i += 8) {
-    const uint4 v = __ldg(r + (i >> 3));
-    acc = fmaf(bf16_lo(v.x), x[i], acc);
-    acc = fmaf(bf16_hi(v.x), x[i + 1], acc);
-    acc = fmaf(bf16_lo(v.y), x[i + 2], acc);
-    acc = fmaf(bf16_hi(v.y), x[i + 3], acc);
-    acc = fmaf(bf16_lo(v.z), x[i + 4], acc);
-    acc = fmaf(bf16_hi(v.z), x[i + 5], acc);
-    acc = fmaf(bf16_lo(v.w), x[i + 6], acc);
-    acc = fmaf(bf16_hi(v.w), x[i + 7], acc);
-  }
-  return acc;
-}
-
-// One site of the surrogate on a group of 128 threads: standardised inputs
-// from the feature accumulator, ensemble forward and backward passes, the
-// site energy (added to e_acc on thread 0), the gate, and the per-site
-// weights dE/dB pushed through the coupling onto the products (wk) and
-// dE/dQ (wq).  Returns with wk, wq valid after the closing barrier.
-__device__ void sur_site_mlp(const AceTables& p, const SurParams& sp, const AceLayout& lay, double* gb, int g,
-                             int lt, int iz, int site, double& e_acc) {
-  const int nin = sp.nin, H = sp.H, M = sp.M, nB = p.nB, nQ = p.nQ;
-  const double* Facc = gb + lay.F;
-  float* xs = reinterpret_cast<float*>(gb + lay.S);
-  float* h1 = xs + nin;
-  float* s1 = h1 + M * H;
-  float* h2 = s1 + M * H;
-  float* s2 = h2 + M * H;
-  float* d2 = s2 + M * H;
-  float* d1 = d2 + M * H;
-  float* ym = d1 + M * H;
-  float* dxs = ym + 4;
-  int* gate = reinterpret_cast<int*>(dxs + M * nin);
-  double* df = gb + lay.DF;
-  double* wk = gb + lay.WK;
-  double* wq = gb + lay.WQ;
-  const size_t zi = (size_t)iz * nin;
-  if (lt == 0) *gate = 0;
-  group_sync(g);
-  for (int i = lt; i < nin; i += ACE_GROUP) {
-    const double raw = i < nB ? Facc[iz * nB + i] : Facc[p.nz * nB + iz * nQ + (i - nB)];
-    const float x = (float)((raw - sp.x_mean[zi + i]) / sp.x_std[zi + i]);
-    xs[i] = x;
-    if (!(x >= sp.x_lo[zi + i] && x <= sp.x_hi[zi + i])) *gate = 1;  // NaN-safe
-  }
-  group_sync(g);
-  const size_t zm = (size_t)iz * M;
-  for (int idx = lt; idx < M * H; idx += ACE_GROUP) {
-    const int m = idx / H, o = idx - m * H;
-    const float z = sp.b1[(zm + m) * H + o] + bf16_dot(sp.W1 + ((zm + m) * H + o) * nin, xs, nin);
-    const float sg = 1.f / (1.f + expf(-z));
-    h1[idx] = z * sg;
-    s1[idx] = sg * (1.f + z * (1.f - sg));
-  }
-  group_sync(g);
-  for (int idx = lt; idx < M * H; idx += ACE_GROUP) {
-    const int m = idx / H, o = idx - m * H;
-    const float z = sp.b2[(zm + m) * H + o] + bf16_dot(sp.W2 + ((zm + m) * H + o) * H, h1 + m * H, H);
-    const float sg = 1.f / (1.f + expf(-z));
-    h2[idx] = z * sg;
-    s2[idx] = sg * (1.f + z * (1.f - sg));
-  }
-  group_sync(g);
-  // output layer: one warp per member (M <= 4), then the backward seeds
-  const int wg = lt >> 5, lane = lt & 31;
-  if (wg < M) {
-    const unsigned short* w3 = sp.w3 + (zm + wg) * H;
-    float acc = 0.f;
-    for (int o = lane; o < H; o += 32) {
-      const float w = __uint_as_float((unsigned)w3[o] << 16);
-      acc = fmaf(w, h2[wg * H + o], acc);
-      d2[wg * H + o] = w * s2[wg * H + o];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) ym[wg] = acc + sp.b3[zm + wg];
-  }
-  group_sync(g);
-  for (int idx = lt; idx < M * H; idx += ACE_GROUP) {
-    const int m = idx / H, i = idx - m * H;
-    d1[idx] = s1[idx] * bf16_dot(sp.W2T + ((zm + m) * H + i) * H, d2 + m * H, H);
-  }
-  group_sync(g);
-  for (int idx = lt; idx < M * nin; idx += ACE_GROUP) {
-    const int m = idx / nin, i = idx - m * nin;
-    dxs[idx] = bf16_dot(sp.W1T + ((zm + m) * nin + i) * H, d1 + m * H, H);
-  }
-  group_sync(g);
-  const double ysd = sp.y_std[iz];
-  if (lt == 0) {
-    float mean = 0.f;
-    for (int m = 0; m < M; ++m) mean += ym[m];
-    mean /= (float)M;
-    float var = 0.f;
-    for (int m = 0; m < M; ++m) var += (ym[m] - mean) * (ym[m] - mean);
-    var /= (float)M;
-    e_acc += sp.y_mean[iz] + ysd * (double)mean;
-    if (!(ysd * (double)sqrtf(var) <= (double)sp.tau)) *gate = 1;
-  }
-  for (int i = lt; i < nin; i += ACE_GROUP) {
-    float acc = 0.f;
-    for (int m = 0; m < M; ++m) acc += dxs[m * nin + i];
-    df[i] = ysd * (double)(acc / (float)M) / sp.x_std[zi + i];
-  }
-  group_sync(g);
-  for (int k = lt; k < p.P; k += ACE_GROUP) {
-    double acc = 0.0;
-    for (int q = sp.ccol_off[k]; q < sp.ccol_off[k + 1]; ++q) acc += sp.ccol_val[q] * df[sp.ccol_b[q]];
-    wk[k] = acc;
-  }
-  for (int n = lt; n < nQ; n += ACE_GROUP) wq[n] = df[nB + n];
-  if (lt == 0) sp.flags[site] = *gate;
-  group_sync(g);
-}
-
-template <int L, class T, bool SUR = false>
+template <int L, class T, int SUR = 0>
 __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
     k_ace_sites(AceTables p, AceLayout lay, SurParams sp, int nunits, const int* __restrict__ unit_begin,
                 const int* __restrict__ unit_sites, int cap,
@@ -390,14 +268,17 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
     const int iz = min(max((int)pos[s].w, 0), p.nz - 1);
     const int eb = min(edge_off[s], cap), E = min(edge_off[s + 1], cap) - eb;
     if (lt == 0) e_acc += p.ref[iz];
-    if (SUR && s > s_begin) {  // features are per site
+    if (SUR == 1 && s > s_begin) {  // features are per site
       group_sync(g);
       for (int k = lt; k < lay.nfeat; k += ACE_GROUP) Facc[k] = 0.0;
     }
     group_sync(g);
-    for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? 1.0 : 0.0;
+    if (SUR == 2)  // the feature pass's A-basis
+      for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? 1.0 : sp.site_A[(size_t)s * D + a];
+    else
+      for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? 1.0 : 0.0;
     // ---- pass 1: A-basis ----
-    for (int c0 = 0; c0 < E; c0 += CH) {
+    for (int c0 = 0; c0 < (SUR == 2 ? 0 : E); c0 += CH) {
       const int nc = min(CH, E - c0);
       group_sync(g);
       ace_chunk_edges<L, T, false>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, e_acc, status);
@@ -439,7 +320,7 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         }
         dA[a] = acc;
       }
-    if (lay.feat)  // B = C·P of the centre's species block (fitting.jl:28)
+    if (lay.feat && SUR != 2)  // B = C·P of the centre's species block (fitting.jl:28)
       for (int b = lt; b < p.nB; b += ACE_GROUP) {
         double acc = 0.0;
         for (int q = p.crow_off[b]; q < p.crow_off[b + 1]; ++q) {
@@ -449,11 +330,30 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         Facc[iz * p.nB + b] += acc;
       }
     const double* wq = nullptr;
-    if constexpr (SUR) {
-      // ---- surrogate: MLP ensemble on the features, per-site weights ----
-      sur_site_mlp(p, sp, lay, gb, g, lt, iz, s, e_acc);
-      const double* wk = gb + lay.WK;
-      wq = gb + lay.WQ;
+    if constexpr (SUR == 1) {
+      // ---- surrogate feature pass: keep A and the own-species features ----
+      group_sync(g);
+      const int nB = p.nB, nQ = p.nQ, nin = nB + nQ;
+      for (int a = lt; a < D; a += ACE_GROUP) sp.site_A[(size_t)s * D + a] = A[a];
+      for (int i = lt; i < nin; i += ACE_GROUP)
+        sp.site_feat[(size_t)s * nin + i] = i < nB ? Facc[iz * nB + i] : Facc[p.nz * nB + iz * nQ + (i - nB)];
+    }
+    if constexpr (SUR == 2) {
+      // ---- surrogate pullback: dE/dB through the coupling onto the products,
+      //      dE/dQ onto the pair radials, then the ordinary adjoint ----
+      const int nB = p.nB, nin = nB + p.nQ;
+      const double* df = sp.site_df + (size_t)s * nin;
+      double* wk = gb + lay.WK;
+      double* wqs = gb + lay.WQ;
+      for (int k = lt; k < P; k += ACE_GROUP) {
+        double acc = 0.0;
+        for (int q = sp.ccol_off[k]; q < sp.ccol_off[k + 1]; ++q) acc += sp.ccol_val[q] * df[sp.ccol_b[q]];
+        wk[k] = acc;
+      }
+      for (int n = lt; n < p.nQ; n += ACE_GROUP) wqs[n] = df[nB + n];
+      if (lt == 0) e_acc += sp.site_e[s];
+      group_sync(g);
+      wq = wqs;
       if (want_grad)
         for (int a = lt; a < D; a += ACE_GROUP) {
           T acc = T(0);
