@@ -287,7 +287,7 @@ def cpu_baseline(w, seconds=12.0, max_reps=20):
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="lj", choices=["lj", "lj1m", "lj_shear", "smooth", "ace", "ace_tial"])
@@ -365,7 +365,7 @@ def run_b200(args):
     value = world * w.n / (ms * 1e-3)
     kern_ms = float(stage[:, 1].mean())
     geom_ms = float(stage[:, 0].mean())
-    e2e_s, E_ref, F_ref = e2e_time(h, w, lib, max(args.steps // 4, 5))
+    e2e_s, E_ref, F_ref = e2e_time(h, w, lib, min(max(args.steps // 4, 5), 200))
     if dist:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
