@@ -83,6 +83,16 @@ pfw_status pfw_set_geometry_device(pfw_ws* ws, int64_t n, const double* X_dev,
                                    const double* H, const uint8_t pbc[3],
                                    const int32_t* species_dev);
 
+/* Domain decomposition (no counterpart in the single-process reference,
+ * README.md:327): atoms [0, n_owned) of the current single-system geometry
+ * are this rank's own, the rest are ghost copies of other ranks' atoms.
+ * Forces are computed for every atom (exact for owned atoms whose
+ * neighbourhood the ghosts cover), but energy and virial count only the
+ * owned atoms' shares — half of every directed pair of an owned centre, the
+ * site terms of owned sites — so the ranks' energies and virials sum to the
+ * whole system's.  -1 (the default after every geometry upload) = all. */
+pfw_status pfw_set_owned(pfw_ws* ws, int64_t n_owned);
+
 /* ---- pair models ------------------------------------------------------ */
 /* SmoothPair(labels, amplitudes, cutoff): U_ab(r) = A_ab (1 - r²/c²)³
  * (PairPotentials/models.jl:28-44 and PreparedSmooth :138-176).

@@ -196,6 +196,18 @@ __global__ void k_site_energies(int n, const double* __restrict__ site_out, cons
   if (s < n) Esite[perm[s]] = site_out[10 * (size_t)s];
 }
 
+__global__ void k_mask_sites(int n, int n_owned, const int* __restrict__ perm, double* __restrict__ site_out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n * 10) return;
+  if (perm[k / 10] >= n_owned) site_out[k] = 0.0;
+}
+
+void mask_unowned_sites(pfw_ws* ws, double* site_out, int n) {
+  if (ws->n_owned < 0 || ws->n_owned >= n || n == 0) return;
+  k_mask_sites<<<grid_for((int64_t)n * 10, 256), 256, 0, ws->stream>>>(n, ws->n_owned, ws->perm.as<int>(), site_out);
+  ws->launches += 1;
+}
+
 __global__ void k_iota(int n, int* __restrict__ out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k <= n) out[k] = k;
@@ -700,6 +712,7 @@ void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
     k_site_energies<<<grid_for(n, 256), 256, 0, st>>>(n, a->unit_out.as<double>(), ws->perm.as<int>(), Esite);
     ws->launches += 1;
   }
+  mask_unowned_sites(ws, a->unit_out.as<double>(), n);
   reduce_site_parts(ws, a->unit_out.as<double>(), n, E, W);
   ws->stage_end(2);
   a->evaluated = true;
@@ -1407,6 +1420,7 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   }
   double* E = E_dev ? E_dev : static_cast<double*>(ws->out_E.ensure(sizeof(double)));
   double* W = W_dev ? W_dev : static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
+  mask_unowned_sites(ws, a->unit_out.as<double>(), n);
   reduce_site_parts(ws, a->unit_out.as<double>(), n, E, W);
   ws->stage_end(2);
   a->evaluated = true;

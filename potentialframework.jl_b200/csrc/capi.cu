@@ -49,6 +49,7 @@ void upload_geometry(pfw_ws* ws, int64_t n, const double* X, const double* H, co
   hs.natoms = (int32_t)n;
   ws->systems.assign(1, hs);
   ws->n = (int32_t)n;
+  ws->n_owned = -1;
   ws->geometry_version += 1;
   cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   ws->X.ensure(sizeof(double) * 3 * std::max<int64_t>(n, 1));
@@ -102,6 +103,7 @@ void upload_batch(pfw_ws* ws, int32_t nsys, const int64_t* offsets, const double
   }
   ws->systems.swap(systems);
   ws->n = (int32_t)n;
+  ws->n_owned = -1;
   ws->max_species = max_species;
   ws->geometry_version += 1;
   ws->prep.valid = false;
@@ -197,6 +199,14 @@ pfw_status pfw_set_geometry(pfw_ws* ws, int64_t n, const double* X, const double
 pfw_status pfw_set_geometry_device(pfw_ws* ws, int64_t n, const double* X_dev, const double* H,
                                    const uint8_t pbc[3], const int32_t* species_dev) {
   return guarded(ws, [&] { upload_geometry(ws, n, X_dev, H, pbc, species_dev, true); });
+}
+
+pfw_status pfw_set_owned(pfw_ws* ws, int64_t n_owned) {
+  return guarded(ws, [&] {
+    if (ws->systems.size() != 1) throw Error(PFW_ESTATE, "owned atoms apply to a single-system geometry");
+    if (n_owned < -1 || n_owned > ws->n) throw Error(PFW_EINVAL, "owned atom count out of range");
+    ws->n_owned = (int32_t)n_owned;
+  });
 }
 
 pfw_status pfw_pair_model_smooth(pfw_ws* ws, int32_t nz, const double* A, double cutoff) {

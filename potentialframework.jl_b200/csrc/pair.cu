@@ -12,6 +12,7 @@
 // scatter; E and W take half of every directed pair.  Per-cell partials (E, 6
 // virial components) are reduced deterministically (reduce.cu).
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 
 #include "pfw_internal.h"
@@ -27,6 +28,7 @@ struct PairParams {
   double invc2;
   double eps4, eps24, sigma2, shift;  // LJ
   int want_f, want_v, want_e;
+  int n_owned;  // atoms [0, n_owned) (original order) own their E/W shares; the rest are ghost copies
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -75,6 +77,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
   double acc_e = 0, w[6] = {0, 0, 0, 0, 0, 0};
   unsigned long long np = 0;
   int cur = -1;
+  bool own = true;
   double fx = 0, fy = 0, fz = 0;
   double arow[4] = {0, 0, 0, 0};
   const bool want_f = prm.want_f;
@@ -87,6 +90,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
             F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
           }
           cur = i;
+          own = perm[i] < prm.n_owned;
           fx = fy = fz = 0;
           if (KIND == 0) {
             const int zi = min(max((int)pi.w, 0), prm.nz - 1);
@@ -115,9 +119,11 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
         }
         const double gx = coef * d[0], gy = coef * d[1], gz = coef * d[2];
         fx += gx; fy += gy; fz += gz;
-        acc_e += en;
-        w[0] += d[0] * gx; w[1] += d[1] * gy; w[2] += d[2] * gz;
-        w[3] += d[0] * gy; w[4] += d[0] * gz; w[5] += d[1] * gz;
+        if (own) {
+          acc_e += en;
+          w[0] += d[0] * gx; w[1] += d[1] * gy; w[2] += d[2] * gz;
+          w[3] += d[0] * gy; w[4] += d[0] * gz; w[5] += d[1] * gz;
+        }
       });
   if (cur >= 0 && want_f) {
     const int o = perm[cur];
@@ -153,6 +159,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
   int cn = 0;
   unsigned long long np = 0;
   int cur = -1;
+  bool own = true;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   float arow[4] = {0.f, 0.f, 0.f, 0.f};
   const bool want_f = prm.want_f;
@@ -177,6 +184,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
             F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
           }
           cur = i;
+          own = perm[i] < prm.n_owned;
           fx = fy = fz = 0.f;
           if (KIND == 0) {
             const int zi = min(max((int)pi.w, 0), prm.nz - 1);
@@ -204,10 +212,12 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
         }
         const float gx = coef * d0, gy = coef * d1, gz = coef * d2;
         fx += gx; fy += gy; fz += gz;
-        ce += en;
-        cw[0] += d0 * gx; cw[1] += d1 * gy; cw[2] += d2 * gz;
-        cw[3] += d0 * gy; cw[4] += d0 * gz; cw[5] += d1 * gz;
-        if (++cn == MIXED_CHUNK) fold();
+        if (own) {
+          ce += en;
+          cw[0] += d0 * gx; cw[1] += d1 * gy; cw[2] += d2 * gz;
+          cw[3] += d0 * gy; cw[4] += d0 * gz; cw[5] += d1 * gz;
+          if (++cn == MIXED_CHUNK) fold();
+        }
       });
   if (cur >= 0 && want_f) {
     const int o = perm[cur];
@@ -277,6 +287,7 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   prm.want_f = (req & PFW_REQ_FORCES) != 0;
   prm.want_v = (req & PFW_REQ_VIRIAL) != 0;
   prm.want_e = (req & PFW_REQ_ENERGY) != 0;
+  prm.n_owned = ws->n_owned < 0 ? INT32_MAX : ws->n_owned;
   const int ncells = P.ncells;
   double* parts = static_cast<double*>(ws->cellpart.ensure(sizeof(double) * 8 * std::max(ncells, 1)));
   unsigned long long* np = static_cast<unsigned long long*>(ws->counters.ensure(64)) + 4;

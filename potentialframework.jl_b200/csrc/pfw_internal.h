@@ -94,6 +94,7 @@ struct pfw_ws {
   int32_t max_species = 0;  // largest species channel of host-uploaded geometry
   std::vector<pfw::HostSystem> systems;
   uint64_t geometry_version = 0;  // bumped when the systems (count, sizes, cells) change
+  int32_t n_owned = -1;           // atoms [0, n_owned) own E/W (domain decomposition); -1: all
   pfw::DevBuf X, species, atom_sys;  // X: 3n doubles
   // prepared geometry
   pfw::Prepared prep;
@@ -151,6 +152,8 @@ void ace_set_schedule(pfw_ws* ws, int chunk, int groups);
 void ace_free(pfw_ws* ws);
 void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev);
 void ace_site_energies(pfw_ws* ws, double* host);
+// zero the E/W partials of sites whose atom is a ghost copy (perm[s] >= n_owned)
+void mask_unowned_sites(pfw_ws* ws, double* site_out, int n);
 int ace_feature_count(pfw_ws* ws);
 void ace_evaluate_batch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev);
 void ace_batch_graph(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev);

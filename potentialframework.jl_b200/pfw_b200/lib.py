@@ -98,6 +98,7 @@ def load():
     L.pfw_evaluate_batch_device.argtypes = [vp, C.c_int32, C.c_uint32, vp, vp, vp, vp]
     L.pfw_batch_graph_launch.argtypes = [vp, C.c_uint32, vp, vp, vp, vp]
     L.pfw_batch_graph_sync.argtypes = [vp]
+    L.pfw_set_owned.argtypes = [vp, C.c_int64]
     L.pfw_surrogate_load.argtypes = [vp, C.POINTER(pfw_ace_tables), vp]
     L.pfw_surrogate_features.argtypes = [vp, dp]
     L.pfw_surrogate_stats.argtypes = [vp, i64p, i64p]
@@ -162,6 +163,9 @@ class Handle:
         self.check(self.L.pfw_set_geometry_device(self.ws, int(n), X_dev_ptr, ptr(Hf, C.c_double),
                                                   ptr(pb, C.c_uint8), species_dev_ptr))
         self.n = int(n)
+
+    def set_owned(self, n_owned):
+        self.check(self.L.pfw_set_owned(self.ws, int(n_owned)))
 
     def smooth(self, A, cutoff):
         A = np.ascontiguousarray(A, dtype=np.float64)
