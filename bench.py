@@ -570,6 +570,12 @@ def surrogate_form(dev, stream, flush, steps=5):
     h = lib.Handle(lib.FP64, device=dev.index)
     h.set_stream(ctypes.c_void_p(stream.cuda_stream))
     h.ace(model)
+    # the plain-ACE comparison runs with its tuned schedule (tuned on the 16,000-atom B2 box)
+    from pfw_b200 import autotune
+    c3 = WL.b2(seed=4, nc=20)
+    h.set_geometry(c3.X, c3.H, c3.pbc, c3.species)
+    chunk, groups, _ = autotune.tune(h, model, lambda: h.evaluate(lib.MODEL_ACE, 7), len(c3.species),
+                                     path=os.path.join(tempfile.gettempdir(), "pfw_b200_bench_autotune.json"))
     h.surrogate(feat, sur)
     Xd = torch.from_numpy(sysb.X).to(dev)
     Sd = torch.from_numpy(sysb.species).to(dev)
@@ -602,6 +608,7 @@ def surrogate_form(dev, stream, flush, steps=5):
     ms_s, ms_a = res["surrogate"]["ms"], res["ace"]["ms"]
     return dict(value=n / (ms_s * 1e-3), unit="atoms/s", ms_per_step=ms_s, atoms=n,
                 plain_ace_value=n / (ms_a * 1e-3), plain_ace_ms_per_step=ms_a, speedup_vs_plain_ace=ms_a / ms_s,
+                plain_ace_schedule=dict(chunk=chunk, groups=groups),
                 force_rmse_vs_ace=float(np.sqrt(np.mean(dF ** 2))), force_max_err_vs_ace=float(np.abs(dF).max()),
                 energy_err_per_atom_vs_ace=abs(res["surrogate"]["E"] - res["ace"]["E"]) / n,
                 fallback_sites=fb, fallback_fraction=fb / max(ns, 1),
