@@ -145,8 +145,8 @@ typedef struct pfw_ace_tables {
 /* Load an ACE model (copies every table to the device). */
 pfw_status pfw_ace_model_load(pfw_ws* ws, const pfw_ace_tables* tables);
 
-/* Schedule of the ACE site kernel: edges per chunk (8, 16 or 32) and site
- * groups of 128 threads per CTA (1..4); 0, 0 = automatic (largest working set
+/* Schedule of the ACE site kernel: edges per chunk (8 or 16) and site
+ * groups of 64 threads per CTA (1..8); 0, 0 = automatic (largest working set
  * that fits).  The autotuner (pfw_b200/autotune.py) times the candidates on
  * the caller's workload and caches the choice.  Returns PFW_EINVAL when the
  * schedule does not fit the model in shared memory. */

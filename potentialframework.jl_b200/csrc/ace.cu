@@ -11,7 +11,7 @@
 //                 from the ORIGINAL coordinates (environments.jl:97-102)
 //   k_edge_rev    index of the reverse edge (j→i, -S) of every edge
 //   k_ace_sites   persistent site kernel (ace_site.cuh) over work units (one
-//                 site, or up to 16 sites of one system of a batch)
+//                 site, or up to 8 sites of one system of a batch)
 //   k_ace_gather  F_k = Σ_{e∈out(k)} g_e - g_{rev(e)}  (reduce_site!,
 //                 NeighbourList/execution.jl:256-273, without a racing scatter)
 //   reduce_site_parts  E and the 3×3 virial from per-site partials (reduce.cu)
@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "ace_math.cuh"
@@ -491,10 +492,13 @@ static AceLayout choose_layout(const AceTables& p, int device, int chunk, int gr
     if (lay.total <= limit) return lay;
     if (!feat) throw Error(PFW_EINVAL, "ACE schedule does not fit in shared memory");
   }
-  const int cand[][2] = {{32, 2}, {16, 3}, {16, 2}, {32, 1}, {16, 1}, {8, 1}};
-  for (auto& c : cand) {
+  const int cand128[][2] = {{32, 2}, {16, 3}, {16, 2}, {32, 1}, {16, 1}, {8, 1}};
+  const int cand64[][2] = {{16, 6}, {16, 4}, {8, 8}, {16, 3}, {8, 4}, {16, 2}, {8, 2}, {8, 1}};
+  const int (*cand)[2] = ACE_GROUP == 128 ? cand128 : cand64;
+  const int ncand = ACE_GROUP == 128 ? 6 : 8;
+  for (int k = 0; k < ncand; ++k) {
     AceLayout lay;
-    lay.make(p, c[0], c[1], feat);
+    lay.make(p, cand[k][0], cand[k][1], feat);
     if (lay.total <= limit) return lay;
   }
   throw Error(PFW_EINVAL, "ACE model too large for the site kernel's shared memory");
@@ -508,8 +512,9 @@ void ace_set_schedule(pfw_ws* ws, int chunk, int groups) {
     release_graph(a);
     return;
   }
-  if (!(chunk == 8 || chunk == 16 || chunk == 32) || groups < 1 || groups > ACE_MAX_GROUPS)
-    throw Error(PFW_EINVAL, "ACE schedule: chunk must be 8, 16 or 32 and groups 1..4");
+  if (!(chunk == 8 || chunk == 16 || chunk == 32) || chunk > ACE_MAX_CHUNK || groups < 1 || groups > ACE_MAX_GROUPS)
+    throw Error(PFW_EINVAL, "ACE schedule: chunk 8, 16 or 32 (at most a quarter of a site group's threads) and "
+                            "groups 1.." + std::to_string(ACE_MAX_GROUPS));
   choose_layout(tables_of(a), ws->opt.device, chunk, groups, 0);  // validates the fit
   a->sched_chunk = chunk;
   a->sched_groups = groups;
@@ -727,7 +732,10 @@ int ace_feature_count(pfw_ws* ws) {
 
 // Sites per work unit of a batch: small enough that large systems spread over
 // many site groups, large enough that a unit's feature partials stay few.
-constexpr int BATCH_UNIT_SITES = 16;
+#ifndef PFW_BATCH_UNIT_SITES
+#define PFW_BATCH_UNIT_SITES 8
+#endif
+constexpr int BATCH_UNIT_SITES = PFW_BATCH_UNIT_SITES;
 
 // Work units of the current batch.  In sorted order the sites of system s
 // are [atom_begin_s, atom_begin_s + natoms_s) (its cells follow those of
@@ -1014,8 +1022,9 @@ void sur_load(pfw_ws* ws, const pfw_ace_tables* t, const pfw_mlp_params* mp) {
 static AceLayout choose_sur_layout(const AceTables& p, int device, int pass) {
   int optin = 0;
   PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-  const int cand[][2] = {{32, 4}, {32, 3}, {16, 4}, {32, 2}, {16, 2}, {16, 1}, {8, 1}};
+  const int cand[][2] = {{32, 4}, {32, 3}, {16, 8}, {16, 6}, {16, 4}, {32, 2}, {16, 2}, {16, 1}, {8, 1}};
   for (auto& c : cand) {
+    if (c[0] > ACE_MAX_CHUNK || c[1] > ACE_MAX_GROUPS) continue;
     AceLayout lay;
     lay.make(p, c[0], c[1], 0, pass);
     if (lay.total <= (size_t)optin) return lay;

@@ -22,8 +22,14 @@
 
 namespace pfw {
 
-constexpr int ACE_GROUP = 128;
-constexpr int ACE_MAX_GROUPS = 4;
+// Threads per site group and site groups per CTA (512 threads per CTA).
+#ifndef PFW_ACE_GROUP
+#define PFW_ACE_GROUP 64
+#endif
+constexpr int ACE_GROUP = PFW_ACE_GROUP;
+constexpr int ACE_MAX_GROUPS = 512 / ACE_GROUP;
+constexpr int ACE_MAX_CHUNK = ACE_GROUP / 4;  // four threads per edge of a chunk
+static_assert(ACE_GROUP == 64 || ACE_GROUP == 128, "site groups of 64 or 128 threads");
 
 struct AceTables {
   RadialDev R, Q;
@@ -404,7 +410,7 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
           T2[t * YS + m] = acc;
         }
         group_sync(g);
-        // 4 threads per edge (CH <= 32)
+        // 4 threads per edge (CH <= ACE_MAX_CHUNK)
         const int t = lt >> 2, q4 = lt & 3;
         T s1 = T(0), gx = T(0), gy = T(0), gz = T(0);
         if (t < nc) {
@@ -455,7 +461,12 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
 #pragma unroll
       for (int k = 0; k < 10; ++k) es.wred[wg * 10 + k] = vals[k];
     group_sync(g);
-    if (lt < 10) unit_out[10 * (size_t)unit + lt] = es.wred[lt] + es.wred[10 + lt] + es.wred[20 + lt] + es.wred[30 + lt];
+    if (lt < 10) {
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < ACE_GROUP / 32; ++w) v += es.wred[10 * w + lt];
+      unit_out[10 * (size_t)unit + lt] = v;
+    }
     if (lay.feat && unit_feat)
       for (int k = lt; k < lay.nfeat; k += ACE_GROUP) unit_feat[(size_t)lay.nfeat * unit + k] = Facc[k];
   }

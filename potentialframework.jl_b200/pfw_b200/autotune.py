@@ -19,7 +19,10 @@ import numpy as np
 
 from . import lib
 
-CANDIDATES = ((8, 1), (8, 2), (8, 4), (16, 1), (16, 2), (16, 3), (16, 4), (32, 1), (32, 2), (32, 3), (32, 4))
+# (edges per chunk, site groups per CTA); schedules the library rejects for
+# its site-group size or the model's shared memory are skipped
+CANDIDATES = ((8, 1), (8, 2), (8, 4), (8, 8), (16, 1), (16, 2), (16, 3), (16, 4), (16, 6), (16, 8), (32, 1),
+              (32, 2), (32, 3), (32, 4))
 
 
 def cache_path():
