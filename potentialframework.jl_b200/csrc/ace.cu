@@ -480,7 +480,7 @@ static AceTables tables_of(AceDevice* a) {
   return p;
 }
 
-// Largest working set that fits (or the tuned schedule): site groups of 128
+// Largest working set that fits (or the tuned schedule): site groups of ACE_GROUP
 // threads per CTA and edges per chunk.
 static AceLayout choose_layout(const AceTables& p, int device, int chunk, int groups, int feat) {
   int optin = 0;

@@ -3,7 +3,7 @@
 // One CTA per SM slot holds the model's product, adjoint-term and density
 // tables in shared memory (loaded once; the precontracted weights are read
 // through L1), and
-// runs G groups of 128 threads; each group evaluates one site at a time
+// runs G groups of ACE_GROUP (64) threads; each group evaluates one site at a time
 // (sites strided over the grid), with its own A/dA vectors and an edge-chunk
 // working set of CH edges:
 //
