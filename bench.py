@@ -437,6 +437,7 @@ def forms(args, dev, stream, flush, F_head):
         if "schedule" in w.config:
             out[w.config["workload"] + "_fp64"]["schedule"] = w.config["schedule"]
         h.close()
+    out["lj_fcc40_256000_skin1.0_md"] = skin_form(dev, stream, flush)
     out["ace_batch4096_fp64_graph"] = batch_form(dev, stream, flush)
     out["surrogate_b2_80_1024000"] = surrogate_form(dev, stream, flush)
     for name in ("lj", "ace"):
@@ -460,6 +461,50 @@ def forms(args, dev, stream, flush, F_head):
             note="FP32 arithmetic, FP64 wrap/shift and FP64 (Kahan) energy/virial accumulation; errors vs plain FP64")
         h32.close()
     return out
+
+
+def skin_form(dev, stream, flush, steps=50, skin=1.0):
+    """LJ FCC 40³ (256,000 atoms) along an MD-like trajectory (Gaussian steps of
+    0.002 Å per component between evaluations) with a 1 Å Verlet skin: the
+    list is built once and reused while no atom moved more than skin/2; the
+    timed steps include the displacement check and the list kernel."""
+    import torch
+
+    from pfw_b200 import lib
+    w = Workload("lj")
+    h = lib.Handle(lib.FP64, device=dev.index)
+    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+    w.bind(h)
+    h.pair_skin(skin)
+    X = torch.from_numpy(w.sys.X.copy()).to(dev)
+    Z = torch.from_numpy(w.sys.species).to(dev)
+    E = torch.zeros(1, dtype=torch.float64, device=dev)
+    F = torch.zeros((w.n, 3), dtype=torch.float64, device=dev)
+    Wv = torch.zeros(9, dtype=torch.float64, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(3)
+    ptrs = [ctypes.c_void_p(t.data_ptr()) for t in (E, F, Wv)]
+
+    def step():
+        h.set_geometry_device(w.n, ctypes.c_void_p(X.data_ptr()), w.sys.H, w.sys.pbc, ctypes.c_void_p(Z.data_ptr()))
+        h.evaluate_device(lib.MODEL_PAIR, 7, *ptrs)
+
+    step()
+    ms = []
+    for _ in range(steps):
+        X.add_(torch.randn(X.shape, generator=gen, device=dev, dtype=torch.float64), alpha=0.002)
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    builds, reuses = h.skin_stats()
+    h.close()
+    m = float(np.mean(ms))
+    return dict(value=w.n / (m * 1e-3), unit="atoms/s", ms_per_step=m, skin=skin, list_builds=builds,
+                list_reuses=reuses, note="Verlet skin reuse (pfw_pair_set_skin); positions move 0.002 Å/step")
 
 
 def batch_form(dev, stream, flush, nsys=4096, steps=20):

@@ -102,6 +102,19 @@ pfw_status pfw_pair_model_smooth(pfw_ws* ws, int32_t nz, const double* A, double
  * (PairPotentials/lennard_jones.jl:5-33). */
 pfw_status pfw_pair_model_lj(pfw_ws* ws, double epsilon, double sigma, double cutoff);
 
+/* Verlet skin reuse of the pair list, the reference's GPU skin path
+ * (gpu_skin!, gpu_displacements!, NeighbourList/gpu.jl:404-549): with
+ * skin > 0 (Å) the pair evaluation of a single system builds the directed
+ * snapshot within cutoff + skin once and reuses it while the atom count, cell
+ * and periodicity are unchanged and no atom moved more than skin/2 (original
+ * coordinates) since the build; 0 (the default) rebuilds on every call, as
+ * evaluate! does.  FP64 workspaces only.  Pairs within about one ulp of the
+ * cutoff may be selected differently from a rebuild (the displacement is
+ * X_j - X_i + H·S from the original coordinates). */
+pfw_status pfw_pair_set_skin(pfw_ws* ws, double skin);
+/* List builds and reuses since the workspace was created. */
+pfw_status pfw_pair_skin_stats(pfw_ws* ws, int64_t* builds, int64_t* reuses);
+
 /* ---- ACE models ------------------------------------------------------- */
 /* Packed resolved-ACE tables; the host builds them from the resolved TOML v1
  * schema (ACE/resolved.jl:103-142), mirroring pack_model (ACE/adaptation.jl:78-98).

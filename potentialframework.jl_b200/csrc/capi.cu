@@ -177,6 +177,7 @@ void pfw_ws_destroy(pfw_ws* ws) {
   if (ws->stream) cudaStreamSynchronize(ws->stream);
   pfw::ace_free(ws);
   pfw::sur_free(ws);
+  pfw::skin_free(ws);
   pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
                          &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
                          &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
@@ -207,6 +208,17 @@ pfw_status pfw_set_owned(pfw_ws* ws, int64_t n_owned) {
     if (n_owned < -1 || n_owned > ws->n) throw Error(PFW_EINVAL, "owned atom count out of range");
     ws->n_owned = (int32_t)n_owned;
   });
+}
+
+pfw_status pfw_pair_set_skin(pfw_ws* ws, double skin) {
+  return guarded(ws, [&] {
+    if (!(std::isfinite(skin) && skin >= 0.0)) throw Error(PFW_EINVAL, "skin must be finite and nonnegative (Å)");
+    ws->skin = skin;
+  });
+}
+
+pfw_status pfw_pair_skin_stats(pfw_ws* ws, int64_t* builds, int64_t* reuses) {
+  return guarded(ws, [&] { pfw::skin_stats(ws, builds, reuses); });
 }
 
 pfw_status pfw_pair_model_smooth(pfw_ws* ws, int32_t nz, const double* A, double cutoff) {

@@ -16,20 +16,12 @@
 #include <cmath>
 
 #include "pfw_internal.h"
+#include "pair_math.cuh"
 #include "traverse.cuh"
 
 namespace pfw {
 
 constexpr int PAIR_WARPS = 4;  // warps (home cells) per CTA
-
-struct PairParams {
-  int kind, nz;
-  double A[16];  // SmoothPair amplitudes (nz <= 4)
-  double invc2;
-  double eps4, eps24, sigma2, shift;  // LJ
-  int want_f, want_v, want_e;
-  int n_owned;  // atoms [0, n_owned) (original order) own their E/W shares; the rest are ghost copies
-};
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -100,23 +92,8 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
         }
         ++np;
         double en, coef;
-        if (KIND == 0) {
-          const int zj = (int)pj.w;
-          const double a = zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3];
-          const double q = 1.0 - r2 * prm.invc2;
-          const double aq2 = a * q * q;
-          en = aq2 * q;
-          coef = -6.0 * aq2 * prm.invc2;
-        } else {
-          // 1/r² by two Newton steps y ← y(2 - r²y) from an FP32 seed (≈1 ulp)
-          double ir2 = (double)__frcp_rn((float)r2);
-          ir2 = fma(ir2, fma(-r2, ir2, 1.0), ir2);
-          ir2 = fma(ir2, fma(-r2, ir2, 1.0), ir2);
-          const double s2 = prm.sigma2 * ir2;
-          const double s6 = s2 * s2 * s2;
-          en = prm.eps4 * (s6 * s6 - s6) - prm.shift;
-          coef = prm.eps24 * (s6 - 2.0 * s6 * s6) * ir2;
-        }
+        const int zj = (int)pj.w;
+        pair_term<KIND>(prm, zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3], r2, en, coef);
         const double gx = coef * d[0], gy = coef * d[1], gz = coef * d[2];
         fx += gx; fy += gy; fz += gz;
         if (own) {
@@ -261,17 +238,8 @@ __global__ void k_reduce_systems(const double* __restrict__ parts, const SysGeom
   }
 }
 
-void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system) {
+PairParams make_pair_params(const pfw_ws* ws, uint32_t req) {
   const PairModel& m = ws->pair;
-  if (m.kind < 0) throw Error(PFW_ESTATE, "no pair model loaded");
-  if (m.kind == 0 && ws->max_species >= m.nz)
-    throw Error(PFW_EINVAL, "potential has no parameters for species channel " + std::to_string(ws->max_species));
-  ws->prep.valid = false;  // evaluate! rebuilds topology on every call
-  ws->stage_begin(0);
-  prepare(ws, m.cutoff);
-  ws->stage_end(0);
-  const Prepared& P = ws->prep;
-  cudaStream_t st = ws->stream;
   PairParams prm{};
   prm.kind = m.kind;
   prm.nz = m.nz;
@@ -288,6 +256,22 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   prm.want_v = (req & PFW_REQ_VIRIAL) != 0;
   prm.want_e = (req & PFW_REQ_ENERGY) != 0;
   prm.n_owned = ws->n_owned < 0 ? INT32_MAX : ws->n_owned;
+  return prm;
+}
+
+void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system) {
+  const PairModel& m = ws->pair;
+  if (m.kind < 0) throw Error(PFW_ESTATE, "no pair model loaded");
+  if (m.kind == 0 && ws->max_species >= m.nz)
+    throw Error(PFW_EINVAL, "potential has no parameters for species channel " + std::to_string(ws->max_species));
+  if (!per_system && skin_pair_evaluate(ws, req, E_dev, F_dev, W_dev)) return;
+  ws->prep.valid = false;  // evaluate! rebuilds topology on every call
+  ws->stage_begin(0);
+  prepare(ws, m.cutoff);
+  ws->stage_end(0);
+  const Prepared& P = ws->prep;
+  cudaStream_t st = ws->stream;
+  const PairParams prm = make_pair_params(ws, req);
   const int ncells = P.ncells;
   double* parts = static_cast<double*>(ws->cellpart.ensure(sizeof(double) * 8 * std::max(ncells, 1)));
   unsigned long long* np = static_cast<unsigned long long*>(ws->counters.ensure(64)) + 4;

@@ -82,6 +82,7 @@ struct PairModel {
 
 struct AceDevice;  // ace.cu
 struct SurDevice;  // ace.cu (surrogate)
+struct SkinState;  // skin.cu
 
 }  // namespace pfw
 
@@ -95,6 +96,8 @@ struct pfw_ws {
   std::vector<pfw::HostSystem> systems;
   uint64_t geometry_version = 0;  // bumped when the systems (count, sizes, cells) change
   int32_t n_owned = -1;           // atoms [0, n_owned) own E/W (domain decomposition); -1: all
+  double skin = 0.0;              // pair neighbour-list skin (Å); 0: rebuild every call
+  pfw::SkinState* skin_state = nullptr;
   pfw::DevBuf X, species, atom_sys;  // X: 3n doubles
   // prepared geometry
   pfw::Prepared prep;
@@ -140,11 +143,16 @@ void exclusive_scan_i64(pfw_ws* ws, const int32_t* in, int64_t* out, int64_t n);
 // reduce.cu: deterministic partial sums → E[0] and W[9] (either may be null)
 void reduce_pair_parts(pfw_ws* ws, const double* parts, int nparts, int stride, double* E, double* W);
 void reduce_site_parts(pfw_ws* ws, const double* parts, int nparts, double* E, double* W);
+// skin.cu: pair evaluation from a cached c+skin list while no atom moved more
+// than skin/2 since it was built (returns false when the list path does not apply)
+bool skin_pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev);
+void skin_free(pfw_ws* ws);
+void skin_stats(pfw_ws* ws, int64_t* builds, int64_t* reuses);
 // pair.cu
 // per_system: E[s] and W[9s..] for every system of a batch
 void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system = false);
 // snapshot.cu
-int64_t neighbour_build(pfw_ws* ws, double cutoff);
+int64_t neighbour_build(pfw_ws* ws, double cutoff, bool with_R = true);
 void neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);
 // ace.cu
 void ace_load(pfw_ws* ws, const pfw_ace_tables* t);

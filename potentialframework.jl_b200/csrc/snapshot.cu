@@ -80,7 +80,7 @@ static bool all_shift_mode(const Prepared& P) {
   return true;
 }
 
-int64_t neighbour_build(pfw_ws* ws, double cutoff) {
+int64_t neighbour_build(pfw_ws* ws, double cutoff, bool with_R) {
   ws->prep.valid = false;
   prepare(ws, cutoff);
   const Prepared& P = ws->prep;
@@ -106,7 +106,8 @@ int64_t neighbour_build(pfw_ws* ws, double cutoff) {
   PFW_CUDA(cudaStreamSynchronize(st));
   int* jd = static_cast<int*>(ws->nb_j.ensure(sizeof(int) * std::max<int64_t>(total, 1)));
   int* Sd = static_cast<int*>(ws->nb_S.ensure(sizeof(int) * 3 * std::max<int64_t>(total, 1)));
-  double* Rd = static_cast<double*>(ws->nb_R.ensure(sizeof(double) * 3 * std::max<int64_t>(total, 1)));
+  double* Rd = with_R ? static_cast<double*>(ws->nb_R.ensure(sizeof(double) * 3 * std::max<int64_t>(total, 1)))
+                      : nullptr;
   if (P.ncells > 0 && total > 0) {
     if (shift)
       k_nb_fill<0><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(), ws->cell_start.as<int>(),

@@ -99,6 +99,8 @@ def load():
     L.pfw_batch_graph_launch.argtypes = [vp, C.c_uint32, vp, vp, vp, vp]
     L.pfw_batch_graph_sync.argtypes = [vp]
     L.pfw_set_owned.argtypes = [vp, C.c_int64]
+    L.pfw_pair_set_skin.argtypes = [vp, C.c_double]
+    L.pfw_pair_skin_stats.argtypes = [vp, i64p, i64p]
     L.pfw_surrogate_load.argtypes = [vp, C.POINTER(pfw_ace_tables), vp]
     L.pfw_surrogate_features.argtypes = [vp, dp]
     L.pfw_surrogate_stats.argtypes = [vp, i64p, i64p]
@@ -166,6 +168,14 @@ class Handle:
 
     def set_owned(self, n_owned):
         self.check(self.L.pfw_set_owned(self.ws, int(n_owned)))
+
+    def pair_skin(self, skin):
+        self.check(self.L.pfw_pair_set_skin(self.ws, float(skin)))
+
+    def skin_stats(self):
+        a = np.zeros(2, np.int64)
+        self.check(self.L.pfw_pair_skin_stats(self.ws, ptr(a[:1], C.c_int64), ptr(a[1:], C.c_int64)))
+        return int(a[0]), int(a[1])
 
     def smooth(self, A, cutoff):
         A = np.ascontiguousarray(A, dtype=np.float64)
