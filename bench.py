@@ -53,15 +53,19 @@ class Workload:
         self.name = name
         self.model_sel = 0
         self.kind = "pair"
-        if name in ("lj", "lj1m", "lj_shear"):
+        if name in ("lj", "lj1m", "lj_shear", "lj_skin"):
             nc = 64 if name == "lj1m" else 40
             self.sys = WL.lj_fcc(seed=2 if nc == 40 else 3, nc=nc, shear=0.2 if name == "lj_shear" else 0.0)
             self.params = dict(potential="lennard_jones", epsilon=WL.LJ_EPS, sigma=WL.LJ_SIGMA, cutoff=WL.LJ_CUTOFF)
             self.pair = ("lj", (WL.LJ_EPS, WL.LJ_SIGMA), WL.LJ_CUTOFF)
             self.flop_per_pair = 65.0
             self.kernel = "k_pair64<LJ>"
-            self.config = dict(workload=f"lj_fcc{nc}_{len(self.sys)}" + ("_shear0.2" if name == "lj_shear" else ""),
+            self.config = dict(workload=f"lj_fcc{nc}_{len(self.sys)}" + ("_shear0.2" if name == "lj_shear" else "")
+                               + ("_skin1.0" if name == "lj_skin" else ""),
                                lattice_a=5.26, displacement_sigma=0.1, **self.params)
+            if name == "lj_skin":
+                self.kernel = "k_pair_list<LJ>"
+                self.config["skin"] = 1.0
         elif name == "smooth":
             self.sys = WL.smooth_fcc(seed=1)
             self.pair = ("smooth", WL.SMOOTH_A, WL.SMOOTH_CUTOFF)
@@ -108,6 +112,8 @@ class Workload:
                 h.lj(params[0], params[1], c)
             else:
                 h.smooth(params, c)
+            if self.name == "lj_skin":
+                h.pair_skin(1.0)
         else:
             h.ace(self.ace)
 
@@ -290,7 +296,8 @@ def parse():
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="lj", choices=["lj", "lj1m", "lj_shear", "smooth", "ace", "ace_tial"])
+    p.add_argument("--workload", default="lj",
+                   choices=["lj", "lj1m", "lj_shear", "lj_skin", "smooth", "ace", "ace_tial"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-forms", action="store_true")
     return p.parse_args()

@@ -267,7 +267,10 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   if (!per_system && skin_pair_evaluate(ws, req, E_dev, F_dev, W_dev)) return;
   ws->prep.valid = false;  // evaluate! rebuilds topology on every call
   ws->stage_begin(0);
-  prepare(ws, m.cutoff);
+  // cell list without the mid-call synchronisation: its input flags are read
+  // once at the end (a bad input only makes clamped cells and NaN sums)
+  const bool wrapped = prepare_plan(ws, m.cutoff);
+  prepare_launch(ws, !wrapped);
   ws->stage_end(0);
   const Prepared& P = ws->prep;
   cudaStream_t st = ws->stream;
@@ -323,6 +326,8 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   ws->stage_end(2);
   ws->launches += 1;
   PFW_CUDA(cudaGetLastError());
+  prepare_check(ws);
+  ws->prep.valid = true;
 }
 
 }  // namespace pfw
