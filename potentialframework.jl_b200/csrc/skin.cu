@@ -10,7 +10,10 @@
 // build and, while it is at most s/2, evaluate only the listed pairs — every
 // pair within c now was within c + s then:
 //
+//   k_pack_list  at a build: (j, S) → one int2 per entry, S as three 10-bit
+//                offsets (|S| < 512, else the list path is not used)
 //   k_max_disp   largest squared displacement (atomicMax on the FP64 bits)
+//   k_pos4       positions and species as one double4 per atom
 //   k_pair_list  8 lanes per atom stride over its list: d = (X_j - X_i) + H·S
 //                with the exact-rounding intrinsics of the snapshot's R,
 //                r² < c² selects the pairs, pair_term as the cell-list kernel;
@@ -37,14 +40,14 @@ struct SkinState {
   double H[9] = {};
   uint8_t pbc[3] = {};
   int kind = -1;
-  DevBuf off, j, S, Xref, dmax;
+  DevBuf off, j, S, list, Xref, dmax, pos4;
   int64_t builds = 0, reuses = 0;
 };
 
 void skin_free(pfw_ws* ws) {
   SkinState* s = ws->skin_state;
   if (!s) return;
-  DevBuf* bufs[] = {&s->off, &s->j, &s->S, &s->Xref, &s->dmax};
+  DevBuf* bufs[] = {&s->off, &s->j, &s->S, &s->list, &s->Xref, &s->dmax, &s->pos4};
   for (auto* b : bufs) b->release();
   delete s;
   ws->skin_state = nullptr;
@@ -64,45 +67,80 @@ __global__ void k_max_disp(int n, const double* __restrict__ X, const double* __
 }
 
 constexpr int SKIN_LANES = 8;  // lanes per atom
+constexpr int SKIN_SBITS = 10;
+constexpr int SKIN_SBIAS = 1 << (SKIN_SBITS - 1);
+
+__global__ void k_pack_list(int64_t m, const int* __restrict__ j, const int* __restrict__ S, int2* __restrict__ out,
+                            int* __restrict__ overflow) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) {
+    unsigned packed = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int v = S[3 * q + a] + SKIN_SBIAS;
+      if (v < 0 || v >= 2 * SKIN_SBIAS) atomicOr(overflow, 1);
+      packed |= (unsigned)(v & (2 * SKIN_SBIAS - 1)) << (SKIN_SBITS * a);
+    }
+    out[q] = make_int2(j[q], (int)packed);
+  }
+}
+
+__global__ void k_pos4(int n, const double* __restrict__ X, const int* __restrict__ species,
+                       double4* __restrict__ pos4) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pos4[i] = make_double4(X[3 * i], X[3 * i + 1], X[3 * i + 2], (double)species[i]);
+}
 
 template <int KIND>
 __global__ void __launch_bounds__(256)
-    k_pair_list(int n, const int64_t* __restrict__ off, const int* __restrict__ jl, const int* __restrict__ Sl,
-                const double* __restrict__ X, const int* __restrict__ species, const double* __restrict__ Hz,
-                double c2, PairParams prm, double* __restrict__ F, double* __restrict__ parts,
-                unsigned long long* __restrict__ npairs) {
+    k_pair_list(int n, const int64_t* __restrict__ off, const int2* __restrict__ list,
+                const double4* __restrict__ pos4, const double* __restrict__ Hz, double c2, PairParams prm,
+                double* __restrict__ F, double* __restrict__ parts, unsigned long long* __restrict__ npairs) {
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) / SKIN_LANES;
   const int sub = threadIdx.x & (SKIN_LANES - 1);
   const unsigned grp = 0xffu << (threadIdx.x & 24);  // the 8 lanes of this atom
   if (i >= n) return;
-  const double xi = X[3 * i], yi = X[3 * i + 1], zi = X[3 * i + 2];
+  const double4 pi = pos4[i];
+  const double xi = pi.x, yi = pi.y, zi = pi.z;
   double arow[4] = {0, 0, 0, 0};
   if (KIND == 0) {
-    const int z = min(max(species[i], 0), prm.nz - 1);
+    const int z = min(max((int)pi.w, 0), prm.nz - 1);
 #pragma unroll
     for (int k = 0; k < 4; ++k) arow[k] = k < prm.nz ? prm.A[z * prm.nz + k] : 0.0;
   }
   double fx = 0, fy = 0, fz = 0, e = 0, w[6] = {0, 0, 0, 0, 0, 0};
   unsigned long long np = 0;
   const int64_t e1 = off[i + 1];
-  for (int64_t q = off[i] + sub; q < e1; q += SKIN_LANES) {
-    const int j = jl[q];
+  const unsigned msk = 2 * SKIN_SBIAS - 1;
+  auto visit = [&](const int2 ent, const double4 pj) {
+    const unsigned pk = (unsigned)ent.y;
     double sh[3];
-    xmatvec(Hz, (double)Sl[3 * q], (double)Sl[3 * q + 1], (double)Sl[3 * q + 2], sh);
-    const double d0 = xadd(xsub(X[3 * j], xi), sh[0]);
-    const double d1 = xadd(xsub(X[3 * j + 1], yi), sh[1]);
-    const double d2 = xadd(xsub(X[3 * j + 2], zi), sh[2]);
+    xmatvec(Hz, (double)((int)(pk & msk) - SKIN_SBIAS), (double)((int)((pk >> SKIN_SBITS) & msk) - SKIN_SBIAS),
+            (double)((int)((pk >> (2 * SKIN_SBITS)) & msk) - SKIN_SBIAS), sh);
+    const double d0 = xadd(xsub(pj.x, xi), sh[0]);
+    const double d1 = xadd(xsub(pj.y, yi), sh[1]);
+    const double d2 = xadd(xsub(pj.z, zi), sh[2]);
     const double r2 = xr2(d0, d1, d2);
-    if (!(r2 < c2)) continue;
+    if (!(r2 < c2)) return;
     ++np;
     double en, coef;
-    const int zj = KIND == 0 ? min(max(species[j], 0), 3) : 0;
+    const int zj = KIND == 0 ? min(max((int)pj.w, 0), 3) : 0;
     pair_term<KIND>(prm, arow[zj], r2, en, coef);
     const double gx = coef * d0, gy = coef * d1, gz = coef * d2;
     fx += gx; fy += gy; fz += gz;
     e += en;
     w[0] += d0 * gx; w[1] += d1 * gy; w[2] += d2 * gz;
     w[3] += d0 * gy; w[4] += d0 * gz; w[5] += d1 * gz;
+  };
+  // two entries per lane in flight: both list loads, then both position loads
+  for (int64_t q = off[i] + sub; q < e1; q += 2 * SKIN_LANES) {
+    const int64_t q2 = q + SKIN_LANES;
+    const bool second = q2 < e1;
+    const int2 ea = list[q];
+    const int2 eb = second ? list[q2] : ea;
+    const double4 pa = pos4[ea.x];
+    const double4 pb = pos4[eb.x];
+    visit(ea, pa);
+    if (second) visit(eb, pb);
   }
   // fixed-order reduction over the atom's 8 lanes
 #pragma unroll
@@ -161,6 +199,18 @@ bool skin_pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
     std::swap(sk.j, ws->nb_j);
     std::swap(sk.S, ws->nb_S);
     ws->nb_total = -1;  // the snapshot buffers now belong to the skin list
+    int2* lst = static_cast<int2*>(sk.list.ensure(sizeof(int2) * std::max<int64_t>(total, 1)));
+    int* ovf = static_cast<int*>(sk.dmax.ensure(sizeof(unsigned long long)));
+    PFW_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int), st));
+    if (total > 0) {
+      k_pack_list<<<(int)std::min<int64_t>(grid_for(total, 256), 4096), 256, 0, st>>>(total, sk.j.as<int>(),
+                                                                                        sk.S.as<int>(), lst, ovf);
+      ws->launches += 1;
+    }
+    int hov = 0;
+    PFW_CUDA(cudaMemcpyAsync(&hov, ovf, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PFW_CUDA(cudaStreamSynchronize(st));
+    if (hov) return false;  // image shifts too large to pack: evaluate by rebuilding
     double* xr = static_cast<double*>(sk.Xref.ensure(sizeof(double) * 3 * std::max(n, 1)));
     if (n > 0) PFW_CUDA(cudaMemcpyAsync(xr, ws->X.ptr, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, st));
     sk.cutoff = m.cutoff;
@@ -186,14 +236,16 @@ bool skin_pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
   double* F = F_dev ? F_dev : static_cast<double*>(ws->out_F.ensure(sizeof(double) * 3 * std::max(n, 1)));
   ws->stage_begin(1);
   if (n > 0) {
+    double4* p4 = static_cast<double4*>(sk.pos4.ensure(sizeof(double4) * n));
+    k_pos4<<<grid_for(n, 256), 256, 0, st>>>(n, ws->X.as<double>(), ws->species.as<int>(), p4);
     const int grid = grid_for((int64_t)n * SKIN_LANES, 256);
     if (m.kind == 0)
-      k_pair_list<0><<<grid, 256, 0, st>>>(n, sk.off.as<int64_t>(), sk.j.as<int>(), sk.S.as<int>(), ws->X.as<double>(),
-                                           ws->species.as<int>(), dHz, m.cutoff * m.cutoff, prm, F, parts, np);
+      k_pair_list<0><<<grid, 256, 0, st>>>(n, sk.off.as<int64_t>(), sk.list.as<int2>(), p4, dHz, m.cutoff * m.cutoff,
+                                           prm, F, parts, np);
     else
-      k_pair_list<1><<<grid, 256, 0, st>>>(n, sk.off.as<int64_t>(), sk.j.as<int>(), sk.S.as<int>(), ws->X.as<double>(),
-                                           ws->species.as<int>(), dHz, m.cutoff * m.cutoff, prm, F, parts, np);
-    ws->launches += 1;
+      k_pair_list<1><<<grid, 256, 0, st>>>(n, sk.off.as<int64_t>(), sk.list.as<int2>(), p4, dHz, m.cutoff * m.cutoff,
+                                           prm, F, parts, np);
+    ws->launches += 2;
   }
   ws->stage_end(1);
   double* E = E_dev ? E_dev : static_cast<double*>(ws->out_E.ensure(sizeof(double)));
