@@ -118,4 +118,49 @@ function NL.neighbour_list(sys::AtomsBase.AbstractSystem{3}, cutoff, w::CUDAWork
     NL.NeighbourSnapshot(idx, disp, shf)
 end
 
+"""set_skin!(w, skin) — Verlet skin reuse of the pair list (pfw_pair_set_skin,
+the reference's gpu_skin!, NeighbourList/gpu.jl:404-549); 0 rebuilds on every
+call as evaluate! does."""
+set_skin!(w::CUDAWorkspace, skin) =
+    check(w, ccall((:pfw_pair_set_skin, libpfw), Cint, (Ptr{Cvoid}, Float64), w.handle,
+                   Float64(ustrip(u"Å", skin isa Unitful.Length ? skin : skin * u"Å"))))
+
+"""evaluate_batch!(w, systems, p; request) — energies, forces and virials of
+many independent structures in one launch (pfw_set_batch + pfw_evaluate_batch),
+as a loop of evaluate! calls would return them."""
+function evaluate_batch!(w::CUDAWorkspace, systems::AbstractVector, p; request=PP.EnergyForcesVirial())
+    nsys = length(systems)
+    offsets = zeros(Int64, nsys + 1)
+    for (s, sys) in enumerate(systems)
+        offsets[s+1] = offsets[s] + length(sys)
+    end
+    n = offsets[end]
+    X = Matrix{Float64}(undef, 3, n); H = zeros(9 * nsys); pbc = zeros(UInt8, 3 * nsys)
+    ch = Vector{Int32}(undef, n)
+    labels = p isa PP.SmoothPair ? p.labels : nothing
+    for (s, sys) in enumerate(systems)
+        for i = 1:length(sys), a = 1:3
+            X[a, offsets[s]+i] = ustrip(u"Å", AtomsBase.position(sys, i)[a])
+        end
+        cv = AtomsBase.cell_vectors(sys)
+        for j = 1:3, a = 1:3
+            H[9(s-1)+3(j-1)+a] = ustrip(u"Å", cv[j][a])
+        end
+        pbc[3(s-1)+1:3s] .= UInt8.(collect(AtomsBase.periodicity(sys)))
+        ch[offsets[s]+1:offsets[s+1]] .= isnothing(labels) ? zeros(Int32, length(sys)) : channels_for(sys, labels)
+    end
+    check(w, ccall((:pfw_set_batch, libpfw), Cint,
+                   (Ptr{Cvoid}, Int32, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}, Ptr{UInt8}, Ptr{Int32}),
+                   w.handle, nsys, offsets, X, H, pbc, ch))
+    bind_model!(w, p)
+    E = zeros(nsys); F = zeros(3, n); W = zeros(9, nsys)
+    check(w, ccall((:pfw_evaluate_batch, libpfw), Cint,
+                   (Ptr{Cvoid}, Int32, UInt32, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                   w.handle, 0, request_bits(request), E, F, W, C_NULL))
+    map(1:nsys) do s
+        (; energy=E[s] * u"eV", forces=F[:, offsets[s]+1:offsets[s+1]] * u"eV/Å",
+           virial=reshape(W[:, s], 3, 3) * u"eV")
+    end
+end
+
 end # module
