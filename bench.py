@@ -214,17 +214,17 @@ def device_step_fn(h, w, dev, lib):
     return step
 
 
-def time_device(h, w, dev, lib, steps, warmup, flush, stream):
-    """Per-step CUDA events on the launch stream; returns (ms list, stage array, launches)."""
+def time_device(h, w, dev, lib, steps, warmup, flush, stream, stage_steps=10):
+    """Per-step CUDA events on the launch stream; returns (ms list, stage array,
+    launches).  The timed steps run without diagnostics (repeated pair
+    evaluations of one structure replay a CUDA graph); a few extra steps with
+    the library's stage events give the per-stage breakdown (kernel times)."""
     import torch
     step = device_step_fn(h, w, dev, lib)
     for _ in range(max(warmup, 3)):
         step()
-    h.check(h.L.pfw_set_diagnostics(h.ws, 1))
-    ms_buf = np.zeros(4)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    stage = []
     torch.cuda.synchronize()
     l0 = h.launches
     for k in range(steps):
@@ -232,10 +232,16 @@ def time_device(h, w, dev, lib, steps, warmup, flush, stream):
         starts[k].record(stream)
         step()
         ends[k].record(stream)
-        h.L.pfw_stage_times(h.ws, ms_buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 4)
-        stage.append(ms_buf.copy())
     torch.cuda.synchronize()
     launches = h.launches - l0
+    h.check(h.L.pfw_set_diagnostics(h.ws, 1))
+    ms_buf = np.zeros(4)
+    stage = []
+    for _ in range(stage_steps):
+        flush.zero_()
+        step()
+        h.L.pfw_stage_times(h.ws, ms_buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 4)
+        stage.append(ms_buf.copy())
     h.check(h.L.pfw_set_diagnostics(h.ws, 0))
     return [a.elapsed_time(b) for a, b in zip(starts, ends)], np.array(stage), launches
 

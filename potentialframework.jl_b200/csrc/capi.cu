@@ -178,6 +178,7 @@ void pfw_ws_destroy(pfw_ws* ws) {
   pfw::ace_free(ws);
   pfw::sur_free(ws);
   pfw::skin_free(ws);
+  pfw::pair_graph_free(ws);
   pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
                          &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
                          &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
@@ -231,6 +232,7 @@ pfw_status pfw_pair_model_smooth(pfw_ws* ws, int32_t nz, const double* A, double
         if (!std::isfinite(A[a * nz + b]) || A[a * nz + b] != A[b * nz + a])
           throw Error(PFW_EINVAL, "amplitude table must be finite and symmetric");
     ws->pair.kind = 0;
+    ws->model_version += 1;
     ws->pair.nz = nz;
     ws->pair.A.assign(A, A + nz * nz);
     ws->pair.cutoff = cutoff;
@@ -243,6 +245,7 @@ pfw_status pfw_pair_model_lj(pfw_ws* ws, double epsilon, double sigma, double cu
           cutoff > 0))
       throw Error(PFW_EINVAL, "LJ parameters must be positive and finite");
     ws->pair.kind = 1;
+    ws->model_version += 1;
     ws->pair.nz = 1;
     ws->pair.eps = epsilon;
     ws->pair.sigma = sigma;

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cmath>
+#include <cstring>
 
 #include "pfw_internal.h"
 #include "pair_math.cuh"
@@ -259,17 +260,13 @@ PairParams make_pair_params(const pfw_ws* ws, uint32_t req) {
   return prm;
 }
 
-void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system) {
+// Device work of one pair evaluation on a planned cell list: cell-list build,
+// output clears, the pair kernel and the reductions (no allocation once the
+// buffers are sized, no host synchronisation: capturable).
+static void pair_launch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system,
+                        bool wrapped) {
   const PairModel& m = ws->pair;
-  if (m.kind < 0) throw Error(PFW_ESTATE, "no pair model loaded");
-  if (m.kind == 0 && ws->max_species >= m.nz)
-    throw Error(PFW_EINVAL, "potential has no parameters for species channel " + std::to_string(ws->max_species));
-  if (!per_system && skin_pair_evaluate(ws, req, E_dev, F_dev, W_dev)) return;
-  ws->prep.valid = false;  // evaluate! rebuilds topology on every call
   ws->stage_begin(0);
-  // cell list without the mid-call synchronisation: its input flags are read
-  // once at the end (a bad input only makes clamped cells and NaN sums)
-  const bool wrapped = prepare_plan(ws, m.cutoff);
   prepare_launch(ws, !wrapped);
   ws->stage_end(0);
   const Prepared& P = ws->prep;
@@ -292,12 +289,6 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   ws->stage_begin(1);
   if (ncells > 0) {
     dim3 grid(grid_for(ncells, PAIR_WARPS)), block(PAIR_WARPS * 32);
-    // the per-warp candidate lists make shared memory a residency limit:
-    // ask for the largest carveout
-    for (const void* k : {(const void*)k_pair64<0, 0>, (const void*)k_pair64<1, 0>, (const void*)k_pair64<0, 1>,
-                          (const void*)k_pair64<1, 1>, (const void*)k_pair32<0, 0>, (const void*)k_pair32<1, 0>,
-                          (const void*)k_pair32<0, 1>, (const void*)k_pair32<1, 1>})
-      PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     bool mixed = ws->opt.precision == PFW_PRECISION_MIXED;
     if (mixed && all_shift) {
       if (m.kind == 0) k_pair32<0, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
@@ -326,6 +317,98 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   ws->stage_end(2);
   ws->launches += 1;
   PFW_CUDA(cudaGetLastError());
+}
+
+// A captured pair evaluation and what it was captured for.
+struct PairGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<SysGeom> sys;
+  const void *E = nullptr, *F = nullptr, *W = nullptr;
+  uint32_t req = 0;
+  uint64_t model_version = 0, alloc_epoch = 0, kernels = 0;
+  int32_t n_owned = 0;
+  int precision = 0;
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  bool matches(const pfw_ws* ws, const void* e, const void* f, const void* w, uint32_t r) const {
+    const auto& ps = ws->prep.sys;
+    return exec && E == e && F == f && W == w && req == r && model_version == ws->model_version &&
+           alloc_epoch == g_alloc_epoch.load() && n_owned == ws->n_owned && precision == ws->opt.precision &&
+           sys.size() == ps.size() && std::memcmp(sys.data(), ps.data(), sizeof(SysGeom) * ps.size()) == 0;
+  }
+};
+
+void pair_graph_free(pfw_ws* ws) {
+  if (!ws->pair_graph) return;
+  ws->pair_graph->release();
+  delete ws->pair_graph;
+  ws->pair_graph = nullptr;
+}
+
+void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system) {
+  const PairModel& m = ws->pair;
+  if (m.kind < 0) throw Error(PFW_ESTATE, "no pair model loaded");
+  if (m.kind == 0 && ws->max_species >= m.nz)
+    throw Error(PFW_EINVAL, "potential has no parameters for species channel " + std::to_string(ws->max_species));
+  if (!per_system && skin_pair_evaluate(ws, req, E_dev, F_dev, W_dev)) return;
+  ws->prep.valid = false;  // evaluate! rebuilds topology on every call
+  // the per-warp candidate lists make shared memory a residency limit: ask
+  // for the largest carveout
+  for (const void* k : {(const void*)k_pair64<0, 0>, (const void*)k_pair64<1, 0>, (const void*)k_pair64<0, 1>,
+                        (const void*)k_pair64<1, 1>, (const void*)k_pair32<0, 0>, (const void*)k_pair32<1, 0>,
+                        (const void*)k_pair32<0, 1>, (const void*)k_pair32<1, 1>})
+    PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  // cell list without a mid-call synchronisation: its input flags are read
+  // once at the end (a bad input only makes clamped cells and NaN sums)
+  const bool wrapped = prepare_plan(ws, m.cutoff);
+  // Repeated calls on the same structure (cells, grid, atom count, outputs,
+  // model) replay one CUDA graph of the whole device sequence: the same work,
+  // without the per-kernel launch gaps.  A new structure runs eagerly once
+  // (sizing every buffer) and captures the graph for the calls after it.
+  const bool graphable = !per_system && !wrapped && !ws->diag;
+  if (graphable) {
+    if (!ws->pair_graph) ws->pair_graph = new PairGraph();
+    PairGraph& pg = *ws->pair_graph;
+    if (pg.matches(ws, E_dev, F_dev, W_dev, req)) {
+      PFW_CUDA(cudaGraphLaunch(pg.exec, ws->stream));
+      ws->launches += pg.kernels;
+    } else {
+      pg.release();
+      pair_launch(ws, req, E_dev, F_dev, W_dev, false, wrapped);
+      const uint64_t l0 = ws->launches;
+      cudaStream_t st = ws->stream;
+      PFW_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        pair_launch(ws, req, E_dev, F_dev, W_dev, false, wrapped);
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        ws->launches = l0;
+        throw;
+      }
+      PFW_CUDA(cudaStreamEndCapture(st, &pg.graph));
+      PFW_CUDA(cudaGraphInstantiate(&pg.exec, pg.graph, 0));
+      pg.kernels = ws->launches - l0;
+      ws->launches = l0;
+      pg.sys = ws->prep.sys;
+      pg.E = E_dev;
+      pg.F = F_dev;
+      pg.W = W_dev;
+      pg.req = req;
+      pg.model_version = ws->model_version;
+      pg.alloc_epoch = g_alloc_epoch.load();
+      pg.n_owned = ws->n_owned;
+      pg.precision = ws->opt.precision;
+    }
+  } else {
+    pair_launch(ws, req, E_dev, F_dev, W_dev, per_system, wrapped);
+  }
   prepare_check(ws);
   ws->prep.valid = true;
 }

@@ -83,6 +83,7 @@ struct PairModel {
 struct AceDevice;  // ace.cu
 struct SurDevice;  // ace.cu (surrogate)
 struct SkinState;  // skin.cu
+struct PairGraph;  // pair.cu
 
 }  // namespace pfw
 
@@ -98,6 +99,8 @@ struct pfw_ws {
   int32_t n_owned = -1;           // atoms [0, n_owned) own E/W (domain decomposition); -1: all
   double skin = 0.0;              // pair neighbour-list skin (Å); 0: rebuild every call
   pfw::SkinState* skin_state = nullptr;
+  pfw::PairGraph* pair_graph = nullptr;  // captured single-system pair evaluation
+  uint64_t model_version = 0;            // bumped by every pair-model change
   pfw::DevBuf X, species, atom_sys;  // X: 3n doubles
   // prepared geometry
   pfw::Prepared prep;
@@ -151,6 +154,7 @@ void skin_stats(pfw_ws* ws, int64_t* builds, int64_t* reuses);
 // pair.cu
 // per_system: E[s] and W[9s..] for every system of a batch
 void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system = false);
+void pair_graph_free(pfw_ws* ws);
 // snapshot.cu
 int64_t neighbour_build(pfw_ws* ws, double cutoff, bool with_R = true);
 void neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);
