@@ -143,8 +143,11 @@ struct EdgeScalars {
 };
 
 // Per-edge set-up of one chunk, four threads per edge (lt = 4t + q):
-// q = 0 the R-family transform/interval/envelope, q = 1 the pair radials,
-// and harmonics split by azimuthal order m ≡ q (mod 4).
+// q = 0 the R-family transform/interval/envelope (shared with the edge's
+// other three threads by shuffles), q = 1 the pair radials, harmonics split
+// by azimuthal order m ≡ q (mod 4), and the R channels n ≡ q (mod 4)
+// (values, and derivatives when Grad) — so no separate radial phase and
+// barrier follow.
 template <int L, class T, bool Grad>
 __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbase, const AceLayout& lay,
                                                 const EdgeScalars<T>& es, const double4* __restrict__ edge_d, int e0,
@@ -158,13 +161,14 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   const T dx = (T)d.x, dy = (T)d.y, dz = (T)d.z;
   const T r0 = sqrt(dx * dx + dy * dy + dz * dz);
   const T r = r0 > T(0) ? r0 : T(1);
+  EdgeRadial<T> er{};
   if (q == 0) {
     if (!(r0 > T(0))) atomicOr(status, 2);
     es.r[t] = r;
     es.dx[t] = dx;
     es.dy[t] = dy;
     es.dz[t] = dz;
-    const EdgeRadial<T> er = edge_radial<T>(p.R, pidx, r);
+    er = edge_radial<T>(p.R, pidx, r);
     es.k0[t] = er.k0;
     es.pidx[t] = pidx;
     es.u[t] = er.u;
@@ -205,6 +209,32 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
         dYt[3 * idx + 2] = j.gz;
       }
     });
+  }
+  // the edge's radial set-up from its first thread (the four threads of an
+  // edge are consecutive lanes of one warp, all inside or all outside nc)
+  const int lane = lt & 31;
+  const unsigned quad = 0xFu << (lane & 28);
+  const int src = lane & 28;
+  er.k0 = __shfl_sync(quad, er.k0, src);
+  er.u = __shfl_sync(quad, er.u, src);
+  er.e = __shfl_sync(quad, er.e, src);
+  if constexpr (Grad) {
+    er.de = __shfl_sync(quad, er.de, src);
+    er.du = __shfl_sync(quad, er.du, src);
+  }
+  double* Rt = gbase + lay.R + t * lay.RS;
+  double* dRt = gbase + lay.dR + t * lay.RS;
+  for (int n = q; n < p.nR; n += 4) {
+    const double* c = channel_coeff(p.R, pidx, er.k0, n);
+    if constexpr (Grad) {
+      T v, dv;
+      channel_ed<T>(c, er, v, dv);
+      Rt[n] = v;
+      dRt[n] = dv;
+    } else {
+      const T u = er.u;
+      Rt[n] = er.e * ((((T)c[3] * u + (T)c[2]) * u + (T)c[1]) * u + (T)c[0]);
+    }
   }
 }
 
@@ -295,13 +325,6 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
           for (int t = 0; t < nc; ++t) acc += QVc[t * p.nQ + n];
           Facc[p.nz * p.nB + iz * p.nQ + n] += acc;
         }
-      for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
-        const int t = idx / nR, n = idx - t * nR;
-        const double* c = channel_coeff(p.R, es.pidx[t], es.k0[t], n);
-        const T u = (T)es.u[t];
-        Rc[t * RS + n] = (T)es.e[t] * ((((T)c[3] * u + (T)c[2]) * u + (T)c[1]) * u + (T)c[0]);
-      }
-      group_sync(g);
       for (int a = lt; a < D; a += ACE_GROUP) {
         const int2 nm = s_dens[a];
         T acc = (T)A[a];
@@ -377,19 +400,6 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         group_sync(g);
         double dummy = 0.0;
         ace_chunk_edges<L, T, true>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, dummy, status, wq);
-        group_sync(g);
-        for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
-          const int t = idx / nR, n = idx - t * nR;
-          EdgeRadial<T> er;
-          er.u = (T)es.u[t];
-          er.e = (T)es.e[t];
-          er.de = (T)es.de[t];
-          er.du = (T)es.du[t];
-          T v, dv;
-          channel_ed<T>(channel_coeff(p.R, es.pidx[t], es.k0[t], n), er, v, dv);
-          Rc[t * RS + n] = v;
-          dRc[t * RS + n] = dv;
-        }
         group_sync(g);
         for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
           const int t = idx / nR, n = idx - t * nR;
