@@ -231,10 +231,12 @@ pfw_status pfw_pair_model_smooth(pfw_ws* ws, int32_t nz, const double* A, double
       for (int b = 0; b < nz; ++b)
         if (!std::isfinite(A[a * nz + b]) || A[a * nz + b] != A[b * nz + a])
           throw Error(PFW_EINVAL, "amplitude table must be finite and symmetric");
+    const std::vector<double> amp(A, A + nz * nz);
+    if (!(ws->pair.kind == 0 && ws->pair.nz == nz && ws->pair.A == amp && ws->pair.cutoff == cutoff))
+      ws->model_version += 1;  // an unchanged model keeps captured evaluations valid
     ws->pair.kind = 0;
-    ws->model_version += 1;
     ws->pair.nz = nz;
-    ws->pair.A.assign(A, A + nz * nz);
+    ws->pair.A = amp;
     ws->pair.cutoff = cutoff;
   });
 }
@@ -244,8 +246,9 @@ pfw_status pfw_pair_model_lj(pfw_ws* ws, double epsilon, double sigma, double cu
     if (!(std::isfinite(epsilon) && std::isfinite(sigma) && std::isfinite(cutoff) && epsilon > 0 && sigma > 0 &&
           cutoff > 0))
       throw Error(PFW_EINVAL, "LJ parameters must be positive and finite");
+    if (!(ws->pair.kind == 1 && ws->pair.eps == epsilon && ws->pair.sigma == sigma && ws->pair.cutoff == cutoff))
+      ws->model_version += 1;
     ws->pair.kind = 1;
-    ws->model_version += 1;
     ws->pair.nz = 1;
     ws->pair.eps = epsilon;
     ws->pair.sigma = sigma;

@@ -116,9 +116,13 @@ class Workspace:
 
     `width` is accepted for API compatibility (the GPU kernels have no SIMD
     lane width); `precision` is "Float64" (plain path) or "mixed"
-    (FP32 arithmetic, FP64 wrap, Kahan FP64 energy/virial)."""
+    (FP32 arithmetic, FP64 wrap, Kahan FP64 energy/virial).  `skin` > 0
+    keeps a pair list of all images within cutoff + skin between calls on
+    the same structure and rebuilds it only once an atom has moved more than
+    skin/2 (the GPU skin list of NeighbourList/gpu.jl:404-549); pairs within
+    about one ulp of the cutoff may then differ from a rebuild."""
 
-    def __init__(self, width=4, precision="Float64", bruteforce_threshold=32, device=0):
+    def __init__(self, width=4, precision="Float64", bruteforce_threshold=32, device=0, skin=0.0):
         if width not in (1, 2, 4, 8, 16):
             raise ArgumentError(_lib.EINVAL, "width must be 1, 2, 4, 8 or 16")
         if precision in ("Float64", np.float64, float):
@@ -132,6 +136,10 @@ class Workspace:
         self.width = width
         self.precision = precision
         self.handle = _lib.Handle(prec, bruteforce_threshold, device)
+        if not (np.isfinite(skin) and skin >= 0):
+            raise ArgumentError(_lib.EINVAL, "skin must be finite and nonnegative")
+        if skin:
+            self.handle.pair_skin(skin)
         self._model_key = None
 
     # geometry/model binding -------------------------------------------
