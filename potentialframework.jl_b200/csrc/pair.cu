@@ -310,12 +310,14 @@ static void pair_launch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
   double* W = W_dev ? W_dev : static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
   ws->stage_begin(2);
   if (per_system) {
-    if (P.nsys > 0) k_reduce_systems<<<P.nsys, 128, 0, st>>>(parts, dsys, 8, E_dev, W_dev);
+    if (P.nsys > 0) {
+      k_reduce_systems<<<P.nsys, 128, 0, st>>>(parts, dsys, 8, E_dev, W_dev);
+      ws->launches += 1;
+    }
   } else {
-    reduce_pair_parts(ws, parts, ncells, 8, E, W);
+    reduce_pair_parts(ws, parts, ncells, 8, E, W);  // counts its own launches
   }
   ws->stage_end(2);
-  ws->launches += 1;
   PFW_CUDA(cudaGetLastError());
 }
 
