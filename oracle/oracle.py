@@ -39,6 +39,7 @@ def lib():
         L.pfo_ace_model_destroy.argtypes = [C.c_void_p]
         L.pfo_ace_evaluate.argtypes = [C.c_void_p, C.c_int64, dp, dp, u8p, i32p, C.c_int32, C.c_uint32, C.c_int32,
                                        dp, dp, dp, dp, dp]
+        L.pfo_ace_set_scales.argtypes = [C.c_void_p, dp, dp]
         L.pfo_radial_ed.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, dp, dp]
         L.pfo_angular_ed.argtypes = [C.c_int32, dp, dp, dp]
         _lib = L
@@ -116,12 +117,22 @@ def neighbour_list(X, H, pbc, cutoff, *, brute_threshold=32):
 class AceOracle:
     """Restated ACE CPU executor on a PackedACE model."""
 
-    def __init__(self, packed):
+    def __init__(self, packed, radial_scale=None, pair_scale=None):
+        """radial_scale [nR, nz, nz] / pair_scale [nQ, nz, nz]: the trainable
+        scales ps.radial.scale / ps.pair.scale (ACE/serial.jl:12-17), applied
+        to the radial values at run time as the reference does."""
         self.packed = packed
         self._t = packed.tables()
         self.handle = lib().pfo_ace_model_create(C.byref(self._t))
         if not self.handle:
             raise OracleError(1, lib().pfo_last_error().decode())
+        if radial_scale is not None or pair_scale is not None:
+            nz = packed.nz
+            rs = None if radial_scale is None else np.asarray(radial_scale, np.float64).reshape(
+                packed.radial.nchannels, nz, nz).ravel(order="F").copy()
+            qs = None if pair_scale is None else np.asarray(pair_scale, np.float64).reshape(
+                packed.pair.nchannels, nz, nz).ravel(order="F").copy()
+            _check(lib().pfo_ace_set_scales(self.handle, _p(rs, C.c_double), _p(qs, C.c_double)))
 
     def __del__(self):
         if getattr(self, "handle", None) and _lib is not None:

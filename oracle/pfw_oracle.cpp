@@ -609,6 +609,9 @@ struct AceModel {
   double cutoff;
   std::vector<double> weights;  // [nz][P] = Cᵀ·WB
   std::vector<double> F;        // BlockAngular normalisation [(lmax+1)^2]
+  // trainable radial scales ps.radial.scale / ps.pair.scale, Julia layout
+  // (n, iz, jz) column-major; empty = the unit scales (serial.jl:12-17)
+  std::vector<double> rscale, qscale;
 };
 
 static Family copy_family(const pfw_radial_family& f, int nz) {
@@ -846,6 +849,19 @@ static SiteResult evaluate_site(const AceModel& m, int iz, const std::vector<Sit
     int pidx = iz * m.nz + zs[j];
     radial_ed(m.R, pidx, r, &R[(size_t)j * nR], &dR[(size_t)j * nR]);
     radial_ed(m.Q, pidx, r, &Qv[(size_t)j * nQ], &dQ[(size_t)j * nQ]);
+    // radial_scale (serial.jl:17; gpu.jl:74-91,229-238): scale · R applied at run time
+    if (!m.rscale.empty())
+      for (int n = 0; n < nR; ++n) {
+        const double sc = m.rscale[n + (size_t)nR * (iz + (size_t)m.nz * zs[j])];
+        R[(size_t)j * nR + n] *= sc;
+        dR[(size_t)j * nR + n] *= sc;
+      }
+    if (!m.qscale.empty())
+      for (int n = 0; n < nQ; ++n) {
+        const double sc = m.qscale[n + (size_t)nQ * (iz + (size_t)m.nz * zs[j])];
+        Qv[(size_t)j * nQ + n] *= sc;
+        dQ[(size_t)j * nQ + n] *= sc;
+      }
     if (!m.pair_allowed[zs[j]])
       for (int n = 0; n < nQ; ++n) Qv[(size_t)j * nQ + n] = dQ[(size_t)j * nQ + n] = 0;
     angular_ed(m.lmax, m.F, d, &Y[(size_t)j * nY], &dY[(size_t)j * nY * 3]);
@@ -1111,6 +1127,21 @@ int pfo_ace_evaluate(void* model, int64_t n, const double* X, const double* H, c
   if (F) std::copy(force.begin(), force.end(), F);
   if (W) std::copy(vir, vir + 9, W);
   if (site_energy) std::copy(es.begin(), es.end(), site_energy);
+  return 0;
+  PFO_CATCH
+}
+
+// Trainable radial scales of trainable_parameters (serial.jl:12-16): radial
+// [nR][nz][nz] and pair [nQ][nz][nz] in Julia column-major (n, iz, jz) order;
+// a null pointer restores the unit scales.
+int pfo_ace_set_scales(void* model, const double* radial_scale, const double* pair_scale) {
+  PFO_TRY
+  AceModel& m = *(AceModel*)model;
+  const size_t zz = (size_t)m.nz * m.nz;
+  if (radial_scale) m.rscale.assign(radial_scale, radial_scale + zz * m.R.nch);
+  else m.rscale.clear();
+  if (pair_scale) m.qscale.assign(pair_scale, pair_scale + zz * m.Q.nch);
+  else m.qscale.clear();
   return 0;
   PFO_CATCH
 }

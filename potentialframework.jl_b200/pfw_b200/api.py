@@ -14,8 +14,9 @@ Same names, argument meaning and error behaviour as PotentialFrameWork.jl:
   potential_energy / forces / virial / energy_forces / energy_forces_virial and the
   in-place forces_ / energy_forces_ / energy_forces_virial_ (which ADD into the
   destination)                      PairPotentials/calculators.jl:54-94
-  ACECalculator(model), load_resolved(path)
-                                    ACE/calculators.jl, ACE/resolved.jl:98-102
+  ACECalculator(model | path), load_resolved(path), save_calculator(path, calc),
+  trainable_parameters(model, ps)   ACE/calculators.jl, ACE/resolved.jl:98-102,
+                                    ACE/persistence.jl:101-167, ACE/serial.jl:12-16
 
 Systems are numeric (Å): any object with X (n,3), H (3,3, columns = cell
 vectors), pbc (3 flags) and species (channel ints or label strings).  Unit
@@ -25,8 +26,12 @@ on the GPU through libpfw_b200.so; there is no CPU path.
 """
 from __future__ import annotations
 
+import copy
+import os
+
 import numpy as np
 
+from . import checkpoint as _checkpoint
 from . import lib as _lib
 from .ace_model import PackedACE
 from .ace_model import load_resolved as _load_resolved
@@ -163,9 +168,10 @@ class Workspace:
             self.handle.lj(p.epsilon, p.sigma, p.radius)
         elif isinstance(p, ACECalculator):
             species = self._species(sys, p.model.atomic_numbers)
-            if self._model_key is not p:
-                self.handle.ace(p.model)
-                self._model_key = p
+            dev = p.device_model()
+            if self._model_key is not dev:
+                self.handle.ace(dev)
+                self._model_key = dev
         else:
             raise ArgumentError(_lib.EINVAL, "pair evaluation requires SmoothPair or lennard_jones")
         self.handle.set_geometry(sys.X, sys.H, sys.pbc, species)
@@ -217,6 +223,8 @@ def with_parameters(p, parameters):
         if set(parameters) != {"epsilon", "sigma"}:
             raise ArgumentError(_lib.EINVAL, "LJ parameters require epsilon and sigma; cutoff is fixed")
         return LennardJones(parameters["epsilon"], parameters["sigma"], p.radius)
+    if isinstance(p, ACECalculator):
+        return ACECalculator(p.model, parameters, p.state)
     raise ArgumentError(_lib.EINVAL, f"{type(p).__name__} does not implement with_parameters")
 
 
@@ -285,14 +293,45 @@ def neighbours(lst: NeighbourSnapshot, i):
 
 # ---- ACE ------------------------------------------------------------------
 class ACECalculator:
-    """GPU ACE calculator over a packed resolved model (ACE/calculators.jl)."""
+    """GPU ACE calculator (ACE/calculators.jl:1-40, persistence.jl:101-124).
 
-    def __init__(self, model, parameters=None):
-        if isinstance(model, str):
-            model = _load_resolved(model)
+    ACECalculator(model, parameters=None, state=None) over a packed resolved
+    model, or ACECalculator(path) for a checkpoint written by save_calculator
+    or a resolved TOML export (the file's content decides).  `parameters`
+    ({"WB": (nbasis, nz), "Wpair": (nQ, nz)} and optionally
+    {"radial": {"scale": (nR, nz, nz)}, "pair": {"scale": (nQ, nz, nz)}}) is
+    authoritative; replace it with set_parameters.  Execution keywords of the
+    reference (width, slots, angular_backend, ...) configure CPU scratch and
+    are accepted and ignored; nothing of the execution state is saved."""
+
+    def __init__(self, model, parameters=None, state=None, **execution):
+        if isinstance(model, (str, os.PathLike)):
+            model, ps0, st0 = _checkpoint.load(model)
+            parameters = ps0 if parameters is None else parameters
+            state = st0 if state is None else state
         if not isinstance(model, PackedACE):
             raise ArgumentError(_lib.EINVAL, "ACECalculator needs a resolved ACE model")
         self.model = model
+        self.parameters = copy.deepcopy(model.default_parameters() if parameters is None else parameters)
+        self.state = copy.deepcopy({} if state is None else state)
+        self._device = model.with_parameters(self.parameters)
+
+    def device_model(self):
+        """Packed tables for the installed parameters (mask and scales applied)."""
+        return self._device
+
+    def get_parameters(self):
+        return copy.deepcopy(self.parameters)
+
+    def set_parameters(self, ps):
+        """AC.set_parameters! (calculators.jl:38-42): same readout shapes or
+        DimensionMismatch; the calculator keeps its own copy."""
+        cur = self.parameters
+        if np.shape(ps["WB"]) != np.shape(cur["WB"]) or np.shape(ps["Wpair"]) != np.shape(cur["Wpair"]):
+            raise DimensionMismatch(_lib.ESHAPE, "ACE readout shapes")
+        self._device = self.model.with_parameters(ps)
+        self.parameters = copy.deepcopy(ps)
+        return self
 
     def cutoff(self):
         return self.model.cutoff
@@ -300,6 +339,16 @@ class ACECalculator:
 
 def load_resolved(path):
     return _load_resolved(path)
+
+
+def save_calculator(path, calc, parameters=None, state=None):
+    """save_calculator (ACE/persistence.jl:139-167)."""
+    return _checkpoint.save_calculator(path, calc, parameters, state)
+
+
+def trainable_parameters(model, ps):
+    """trainable_parameters (ACE/serial.jl:12-16)."""
+    return _checkpoint.trainable_parameters(model.model if isinstance(model, ACECalculator) else model, ps)
 
 
 # ---- AtomsCalculators methods (PairPotentials/calculators.jl:54-94) --------
@@ -364,7 +413,14 @@ def energy_forces_virial_(F, sys, p, neighbourlist=None, **kw):
 
 
 def calculate(props, sys, p, parameters=None, state=None, neighbourlist=None):
-    """AtomsCalculators.calculate (calculators.jl:96-143)."""
-    if parameters is not None:
+    """AtomsCalculators.calculate (PairPotentials/calculators.jl:100-143,
+    ACE/calculators.jl:113-129): the requested properties plus `state`
+    (the calculator's own state for ACE when none is given)."""
+    if isinstance(p, ACECalculator) and state is None:
+        state = p.state
+    if parameters is not None and not (isinstance(parameters, dict) and not parameters):
         p = with_parameters(p, parameters)
-    return evaluate_(_ws(neighbourlist), sys, p, request=props)
+    out = {} if isinstance(props, (tuple, list)) and len(props) == 0 else \
+        evaluate_(_ws(neighbourlist), sys, p, request=props)
+    out["state"] = state
+    return out

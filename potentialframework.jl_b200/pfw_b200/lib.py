@@ -16,7 +16,8 @@ from .ace_model import pfw_ace_tables
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIBPATH = os.path.join(PKG, "lib", "libpfw_b200.so")
 
-OK, EINVAL, EDOMAIN, ESHAPE, ECAPACITY, ECUDA, ETIMEDOUT, ESTATE = range(8)
+from .errors import (ECAPACITY, ECUDA, EDOMAIN, EINVAL, ESHAPE, ESTATE, ETIMEDOUT, OK,  # noqa: F401
+                     ArgumentError, DimensionMismatch, DomainError, PFWError)
 REQ_E, REQ_F, REQ_V = 1, 2, 4
 FP64, MIXED = 0, 1
 MODEL_PAIR, MODEL_ACE, MODEL_SURROGATE = 0, 1, 2
@@ -25,26 +26,6 @@ MODEL_PAIR, MODEL_ACE, MODEL_SURROGATE = 0, 1, 2
 class pfw_options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("bruteforce_threshold", C.c_int32), ("device", C.c_int32),
                 ("reserved", C.c_int32)]
-
-
-class PFWError(RuntimeError):
-    """Error status from the library; subclasses mirror the reference's exceptions."""
-
-    def __init__(self, code, msg):
-        super().__init__(msg)
-        self.code = code
-
-
-class ArgumentError(PFWError, ValueError):
-    pass
-
-
-class DomainError(PFWError, ArithmeticError):
-    pass
-
-
-class DimensionMismatch(PFWError, ValueError):
-    pass
 
 
 _ERRORS = {EINVAL: ArgumentError, EDOMAIN: DomainError, ESHAPE: DimensionMismatch}
