@@ -90,6 +90,22 @@ class Workload:
             self.config = dict(workload=f"ace_b2_20_{len(self.sys)}" + ("_tial" if name == "ace_tial" else ""),
                                model=label, cutoff=self.ace.cutoff, lattice_a=2.9, displacement_sigma=0.08,
                                densities=self.ace.ndensity, products=self.ace.nproducts, invariants=self.ace.nbasis)
+        elif name == "ace_may30":
+            from pfw_b200.ace_model import PackedACE
+            self.kind = "ace"
+            self.model_sel = 1
+            path = os.path.join(ROOT, "tests", "golden", "may30_model.npz")
+            if not os.path.exists(path):
+                raise FileNotFoundError("May30 model tables not generated (tests/golden/make_may30.py)")
+            self.ace = PackedACE.from_npz_dict(np.load(path), "model_")
+            fr = np.load(os.path.join(ROOT, "tests", "golden", "may30_frames.npz"))
+            self.sys = WL.supercell(WL.System(fr["f2_X"], fr["f2_H"], (1, 1, 1), fr["f2_species"]), 4)
+            self.kernel = "k_ace_sites"
+            self.config = dict(workload=f"ace_may30_omega240x64_{len(self.sys)}",
+                               model="May30 Ti-Al-V fit (solid harmonics l<=6, 114 radials on 1000 nodes, "
+                                     "PolyEnvelope1sR pairs, order 3)",
+                               cutoff=self.ace.cutoff, structure="omega-240 fixture replicated 4x4x4",
+                               densities=self.ace.ndensity, products=self.ace.nproducts, invariants=self.ace.nbasis)
         else:
             raise SystemExit(f"unknown workload {name}")
         self.n = len(self.sys)
@@ -303,7 +319,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="lj",
-                   choices=["lj", "lj1m", "lj_shear", "lj_skin", "smooth", "ace", "ace_tial"])
+                   choices=["lj", "lj1m", "lj_shear", "lj_skin", "smooth", "ace", "ace_tial", "ace_may30"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-forms", action="store_true")
     return p.parse_args()
@@ -435,10 +451,14 @@ def forms(args, dev, stream, flush, F_head):
     from pfw_b200 import lib
     out = {}
     steps = 10
-    for name in ("lj1m", "lj_shear", "smooth", "ace", "ace_tial"):
+    for name in ("lj1m", "lj_shear", "smooth", "ace", "ace_tial", "ace_may30"):
         if name == args.workload:
             continue
-        w = Workload(name)
+        try:
+            w = Workload(name)
+        except FileNotFoundError as e:
+            out[name] = dict(skipped=str(e))
+            continue
         h = lib.Handle(lib.FP64, device=dev.index)
         h.check(h.L.pfw_set_stream(h.ws, ctypes.c_void_p(stream.cuda_stream)))
         w.bind(h)

@@ -135,7 +135,7 @@ typedef struct pfw_radial_family {
 
 typedef struct pfw_ace_tables {
   int32_t nz;                   /* species channels */
-  int32_t lmax;                 /* real spherical harmonics, L2, l*l+l+m order */
+  int32_t lmax;                 /* harmonics degree (L2, l*l+l+m order), 0..6 */
   pfw_radial_family radial;     /* R channels */
   pfw_radial_family pair;       /* Q (pair) channels */
   int32_t ndensity;             /* D */
@@ -153,6 +153,8 @@ typedef struct pfw_ace_tables {
   const double* reference;      /* [nz] reference energies (0 when disabled) */
   const uint8_t* pair_allowed;  /* [nz] pair term enabled for neighbour species */
   double cutoff;                /* search cutoff = max rcut over channels (cpu.jl:316) */
+  int32_t angular_kind;         /* 0 real spherical Y_lm, 1 real solid r^l·Y_lm (BlockAngular
+                                   solid=true, ACE/angular_blocks.jl:25-48; the May30 models) */
 } pfw_ace_tables;
 
 /* Load an ACE model (copies every table to the device). */

@@ -42,6 +42,7 @@ def lib():
         L.pfo_ace_set_scales.argtypes = [C.c_void_p, dp, dp]
         L.pfo_radial_ed.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, dp, dp]
         L.pfo_angular_ed.argtypes = [C.c_int32, dp, dp, dp]
+        L.pfo_solid_ed.argtypes = [C.c_int32, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -168,10 +169,12 @@ class AceOracle:
         return v, d
 
 
-def angular_ed(lmax, d):
+def angular_ed(lmax, d, solid=False):
+    """BlockAngular values and Cartesian gradients; solid: r^l·Y_lm."""
     d = np.ascontiguousarray(d, dtype=np.float64)
     nY = (lmax + 1) ** 2
     Y = np.zeros(nY)
     dY = np.zeros((nY, 3))
-    _check(lib().pfo_angular_ed(lmax, _p(d, C.c_double), _p(Y, C.c_double), _p(dY, C.c_double)))
+    fn = lib().pfo_solid_ed if solid else lib().pfo_angular_ed
+    _check(fn(lmax, _p(d, C.c_double), _p(Y, C.c_double), _p(dY, C.c_double)))
     return Y, dY

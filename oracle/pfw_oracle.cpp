@@ -612,6 +612,7 @@ struct AceModel {
   // trainable radial scales ps.radial.scale / ps.pair.scale, Julia layout
   // (n, iz, jz) column-major; empty = the unit scales (serial.jl:12-17)
   std::vector<double> rscale, qscale;
+  bool solid = false;  // real solid harmonics r^l·Y_lm (angular_blocks.jl:47-48)
 };
 
 static Family copy_family(const pfw_radial_family& f, int nz) {
@@ -737,17 +738,23 @@ static std::vector<double> angular_normalisation(int L) {
   return F;
 }
 
-static void angular_ed(int L, const std::vector<double>& F, const double d[3], double* Y, double* dY) {
+// solid: the recurrences on the raw displacement with unit gradients, i.e. the
+// real solid harmonics r^l·Y_lm (BlockAngular solid=true, angular_blocks.jl:47-48).
+static void angular_ed(int L, const std::vector<double>& F, const double d[3], double* Y, double* dY,
+                       bool solid = false) {
   double radius = d[0] * d[0];
   radius = radius + d[1] * d[1];
   radius = radius + d[2] * d[2];
   radius = std::sqrt(radius);
   if (!(radius > 0)) throw Error(PFW_EDOMAIN, "physical zero directions are unsupported");
   double u[3] = {d[0] / radius, d[1] / radius, d[2] / radius};
+  if (solid)
+    for (int a = 0; a < 3; ++a) u[a] = d[a];
   Jet jx[3];
   for (int a = 0; a < 3; ++a) {
     jx[a].v = u[a];
-    for (int c = 0; c < 3; ++c) jx[a].g[c] = ((a == c ? 1.0 : 0.0) - u[a] * u[c]) / radius;
+    for (int c = 0; c < 3; ++c)
+      jx[a].g[c] = solid ? (a == c ? 1.0 : 0.0) : ((a == c ? 1.0 : 0.0) - u[a] * u[c]) / radius;
   }
   Jet x = jx[0], y = jx[1], z = jx[2];
   Jet r2 = jadd(jadd(jmul(x, x), jmul(y, y)), jmul(z, z));
@@ -790,6 +797,7 @@ static AceModel make_model(const pfw_ace_tables* t) {
   AceModel m;
   m.nz = t->nz;
   m.lmax = t->lmax;
+  m.solid = t->angular_kind == 1;
   m.nY = (t->lmax + 1) * (t->lmax + 1);
   m.R = copy_family(t->radial, t->nz);
   m.Q = copy_family(t->pair, t->nz);
@@ -864,7 +872,7 @@ static SiteResult evaluate_site(const AceModel& m, int iz, const std::vector<Sit
       }
     if (!m.pair_allowed[zs[j]])
       for (int n = 0; n < nQ; ++n) Qv[(size_t)j * nQ + n] = dQ[(size_t)j * nQ + n] = 0;
-    angular_ed(m.lmax, m.F, d, &Y[(size_t)j * nY], &dY[(size_t)j * nY * 3]);
+    angular_ed(m.lmax, m.F, d, &Y[(size_t)j * nY], &dY[(size_t)j * nY * 3], m.solid);
   }
   // project_rows! (cpu.jl:156-161): for (a,(r,m)), j
   std::vector<double> A(D, 0.0);
@@ -1158,6 +1166,13 @@ int pfo_angular_ed(int32_t lmax, const double* d, double* Y, double* dY) {
   PFO_TRY
   auto F = angular_normalisation(lmax);
   angular_ed(lmax, F, d, Y, dY);
+  return 0;
+  PFO_CATCH
+}
+int pfo_solid_ed(int32_t lmax, const double* d, double* Y, double* dY) {
+  PFO_TRY
+  auto F = angular_normalisation(lmax);
+  angular_ed(lmax, F, d, Y, dY, true);
   return 0;
   PFO_CATCH
 }

@@ -47,7 +47,7 @@ struct GraphKey {
 };
 
 struct AceDevice {
-  int nz = 0, lmax = 0, nY = 0, nR = 0, nQ = 0, D = 0, P = 0, T = 0, nB = 0, max_order = 0;
+  int nz = 0, lmax = 0, nY = 0, nR = 0, nQ = 0, D = 0, P = 0, T = 0, nB = 0, max_order = 0, solid = 0;
   double cutoff = 0;
   RadialDev R{}, Q{};
   DevBuf r_len, r_nodes, r_coeff, r_tr, r_pow, r_envk, r_env;
@@ -306,6 +306,8 @@ static void fill_model(pfw_ws* ws, AceDevice* a, const pfw_ace_tables* t);
 static AceDevice* load_model(pfw_ws* ws, const pfw_ace_tables* t) {
   if (t->nz < 1 || t->nz > 16) throw Error(PFW_EINVAL, "ACE models support 1 to 16 species channels");
   if (t->lmax < 0 || t->lmax > ACE_LMAX) throw Error(PFW_EINVAL, "ACE lmax must be in 0..6");
+  if (t->angular_kind != 0 && t->angular_kind != 1)
+    throw Error(PFW_EINVAL, "angular kind must be 0 (real spherical) or 1 (real solid)");
   if (t->radial.nchannels < 1) throw Error(PFW_EINVAL, "empty radial basis");
   if (!(std::isfinite(t->cutoff) && t->cutoff > 0)) throw Error(PFW_EINVAL, "invalid ACE cutoff");
   if (t->ndensity < 1 || t->ndensity > 65534 || t->nproducts < 1 || t->nproducts > 65535)
@@ -331,6 +333,7 @@ static void fill_model(pfw_ws* ws, AceDevice* a, const pfw_ace_tables* t) {
   const int nz = t->nz;
   a->nz = nz;
   a->lmax = t->lmax;
+  a->solid = t->angular_kind;
   a->nY = (t->lmax + 1) * (t->lmax + 1);
   a->nR = t->radial.nchannels;
   a->nQ = t->pair.nchannels;
@@ -477,6 +480,7 @@ static AceTables tables_of(AceDevice* a) {
   p.ref = a->ref.as<double>();
   p.pair_ok = a->pair_ok.as<int>();
   p.Fnorm = a->Fnorm.as<double>();
+  p.solid = a->solid;
   return p;
 }
 
@@ -486,21 +490,27 @@ static AceLayout choose_layout(const AceTables& p, int device, int chunk, int gr
   int optin = 0;
   PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   const size_t limit = (size_t)optin;
+  // tables staged in shared memory first; models whose adjoint terms (then
+  // products) do not fit read them from global memory instead
+  const int gtabs[] = {0, 1, 3};
   if (chunk > 0) {
-    AceLayout lay;
-    lay.make(p, chunk, groups, feat);
-    if (lay.total <= limit) return lay;
+    for (int gt : gtabs) {
+      AceLayout lay;
+      lay.make(p, chunk, groups, feat, 0, gt);
+      if (lay.total <= limit) return lay;
+    }
     if (!feat) throw Error(PFW_EINVAL, "ACE schedule does not fit in shared memory");
   }
   const int cand128[][2] = {{32, 2}, {16, 3}, {16, 2}, {32, 1}, {16, 1}, {8, 1}};
   const int cand64[][2] = {{16, 6}, {16, 4}, {8, 8}, {16, 3}, {8, 4}, {16, 2}, {8, 2}, {8, 1}};
   const int (*cand)[2] = ACE_GROUP == 128 ? cand128 : cand64;
   const int ncand = ACE_GROUP == 128 ? 6 : 8;
-  for (int k = 0; k < ncand; ++k) {
-    AceLayout lay;
-    lay.make(p, cand[k][0], cand[k][1], feat);
-    if (lay.total <= limit) return lay;
-  }
+  for (int k = 0; k < ncand; ++k)  // the largest working set that fits, tables staged where they fit
+    for (int gt : gtabs) {
+      AceLayout lay;
+      lay.make(p, cand[k][0], cand[k][1], feat, 0, gt);
+      if (lay.total <= limit) return lay;
+    }
   throw Error(PFW_EINVAL, "ACE model too large for the site kernel's shared memory");
 }
 
@@ -1025,9 +1035,11 @@ static AceLayout choose_sur_layout(const AceTables& p, int device, int pass) {
   const int cand[][2] = {{32, 4}, {32, 3}, {16, 8}, {16, 6}, {16, 4}, {32, 2}, {16, 2}, {16, 1}, {8, 1}};
   for (auto& c : cand) {
     if (c[0] > ACE_MAX_CHUNK || c[1] > ACE_MAX_GROUPS) continue;
-    AceLayout lay;
-    lay.make(p, c[0], c[1], 0, pass);
-    if (lay.total <= (size_t)optin) return lay;
+    for (int gt : {0, 1, 3}) {
+      AceLayout lay;
+      lay.make(p, c[0], c[1], 0, pass, gt);
+      if (lay.total <= (size_t)optin) return lay;
+    }
   }
   throw Error(PFW_EINVAL, "surrogate feature model too large for the site kernel's shared memory");
 }

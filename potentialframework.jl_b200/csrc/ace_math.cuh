@@ -175,15 +175,25 @@ constexpr int ACE_LMAX = 6;
 //   Q_mm = -(2m-1) Q_{m-1,m-1},  Q_{m+1,m} = (2m+1) z Q_mm,
 //   Q_lm = ((2l-1) z Q_{l-1,m} - (l+m-1) r² Q_{l-2,m}) / (l-m)
 // emit(index, Jet) receives Y_lm at l*l+l+m and, for m > 0, Y_l,-m at l*l+l-m.
+// solid: the same recurrences on the raw displacement (unit gradients), which
+// gives the real solid harmonics r^l·Y_lm (BlockAngular solid=true,
+// angular_blocks.jl:47-48).
 template <class T, bool Grad, int L, class Emit>
 __device__ __forceinline__ void harmonics_m(const double* __restrict__ F, T r, T dx, T dy, T dz, int m,
-                                            Emit&& emit) {
+                                            Emit&& emit, bool solid = false) {
   using J = Jet<T, Grad>;
   const T ir = T(1) / r;
-  const T ux = dx * ir, uy = dy * ir, uz = dz * ir;
-  const J x = {ux, Grad ? (T(1) - ux * ux) * ir : T(0), Grad ? (-ux * uy) * ir : T(0), Grad ? (-ux * uz) * ir : T(0)};
-  const J y = {uy, Grad ? (-uy * ux) * ir : T(0), Grad ? (T(1) - uy * uy) * ir : T(0), Grad ? (-uy * uz) * ir : T(0)};
-  const J z = {uz, Grad ? (-uz * ux) * ir : T(0), Grad ? (-uz * uy) * ir : T(0), Grad ? (T(1) - uz * uz) * ir : T(0)};
+  J x, y, z;
+  if (solid) {
+    x = {dx, Grad ? T(1) : T(0), T(0), T(0)};
+    y = {dy, T(0), Grad ? T(1) : T(0), T(0)};
+    z = {dz, T(0), T(0), Grad ? T(1) : T(0)};
+  } else {
+    const T ux = dx * ir, uy = dy * ir, uz = dz * ir;
+    x = {ux, Grad ? (T(1) - ux * ux) * ir : T(0), Grad ? (-ux * uy) * ir : T(0), Grad ? (-ux * uz) * ir : T(0)};
+    y = {uy, Grad ? (-uy * ux) * ir : T(0), Grad ? (T(1) - uy * uy) * ir : T(0), Grad ? (-uy * uz) * ir : T(0)};
+    z = {uz, Grad ? (-uz * ux) * ir : T(0), Grad ? (-uz * uy) * ir : T(0), Grad ? (T(1) - uz * uz) * ir : T(0)};
+  }
   const J r2 = jadd(jadd(jmul(x, x), jmul(y, y)), jmul(z, z));
   J cs = {T(1), T(0), T(0), T(0)}, sn = {T(0), T(0), T(0), T(0)};
   J q = {T(1), T(0), T(0), T(0)};  // Q_kk along the diagonal

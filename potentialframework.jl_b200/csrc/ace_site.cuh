@@ -2,7 +2,8 @@
 //
 // One CTA per SM slot holds the model's product, adjoint-term and density
 // tables in shared memory (loaded once; the precontracted weights are read
-// through L1), and
+// through L1; a model whose product or term tables do not fit leaves them in
+// global memory, read through L1), and
 // runs G groups of ACE_GROUP (64) threads; each group evaluates one site at a time
 // (sites strided over the grid), with its own A/dA vectors and an edge-chunk
 // working set of CH edges:
@@ -51,6 +52,7 @@ struct AceTables {
   const double* ref;              // [nz]
   const int* pair_ok;             // [nz]
   const double* Fnorm;            // [(L+1)^2]
+  int solid;                      // 1: real solid harmonics r^l·Y_lm
 };
 
 // Learned per-atom surrogate: an ensemble of M MLPs per centre species,
@@ -88,20 +90,24 @@ struct AceLayout {
   int feat;    // 1: per-unit fitting features are accumulated
   int nfeat;   // nz * (nB + nQ)
   int sur;     // surrogate pass: 1 features, 2 pullback with per-site weights
+  int gtab;    // tables read from global memory (L1-cached) instead of staged:
+               // bit 0 the adjoint terms, bit 1 the products (large models)
   size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, tables_end;
   size_t group_bytes, total;
   // group-relative double offsets
   int A, dA, Y, dY, R, dR, T1, T2, esc, F, QV, WK, WQ, ints;
   __host__ __device__ static size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
-  __host__ __device__ void make(const AceTables& t, int ch, int g, int with_feat = 0, int sur_pass = 0) {
+  __host__ __device__ void make(const AceTables& t, int ch, int g, int with_feat = 0, int sur_pass = 0,
+                                int global_tables = 0) {
     CH = ch;
     G = g;
     sur = sur_pass;
+    gtab = global_tables;
     feat = with_feat || sur == 1;
     nfeat = t.nz * (t.nB + t.nQ);
     size_t o = 0;
-    prods = o; o = align16(o + sizeof(ushort4) * t.P);
-    terms = o; o = align16(o + sizeof(ushort4) * t.T);
+    prods = o; o = align16(o + ((gtab & 2) ? 0 : sizeof(ushort4) * t.P));
+    terms = o; o = align16(o + ((gtab & 1) ? 0 : sizeof(ushort4) * t.T));
     term_off = o; o = align16(o + sizeof(int) * (t.D + 1));
     density = o; o = align16(o + sizeof(int2) * t.D);
     dn_off = o; o = align16(o + sizeof(int) * (t.nR + 1));
@@ -201,14 +207,17 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
     if ((m & 3) != q) continue;
-    harmonics_m<T, Grad, L>(p.Fnorm, r, dx, dy, dz, m, [&](int idx, const Jet<T, Grad>& j) {
-      Yt[idx] = j.v;
-      if constexpr (Grad) {
-        dYt[3 * idx] = j.gx;
-        dYt[3 * idx + 1] = j.gy;
-        dYt[3 * idx + 2] = j.gz;
-      }
-    });
+    harmonics_m<T, Grad, L>(
+        p.Fnorm, r, dx, dy, dz, m,
+        [&](int idx, const Jet<T, Grad>& j) {
+          Yt[idx] = j.v;
+          if constexpr (Grad) {
+            dYt[3 * idx] = j.gx;
+            dYt[3 * idx + 1] = j.gy;
+            dYt[3 * idx + 2] = j.gz;
+          }
+        },
+        p.solid != 0);
   }
   // the edge's radial set-up from its first thread (the four threads of an
   // edge are consecutive lanes of one warp, all inside or all outside nc)
@@ -247,16 +256,20 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
                 int want_grad, int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem[];
   // ---- stage the model tables once per CTA ----
-  ushort4* s_prods = reinterpret_cast<ushort4*>(smem + lay.prods);
-  ushort4* s_terms = reinterpret_cast<ushort4*>(smem + lay.terms);
+  ushort4* st_prods = reinterpret_cast<ushort4*>(smem + lay.prods);
+  ushort4* st_terms = reinterpret_cast<ushort4*>(smem + lay.terms);
+  const ushort4* s_prods = (lay.gtab & 2) ? p.prods : st_prods;
+  const ushort4* s_terms = (lay.gtab & 1) ? p.terms : st_terms;
   int* s_toff = reinterpret_cast<int*>(smem + lay.term_off);
   int2* s_dens = reinterpret_cast<int2*>(smem + lay.density);
   int* s_dnoff = reinterpret_cast<int*>(smem + lay.dn_off);
   int2* s_dn = reinterpret_cast<int2*>(smem + lay.dn);
   int* s_dmoff = reinterpret_cast<int*>(smem + lay.dm_off);
   int2* s_dm = reinterpret_cast<int2*>(smem + lay.dm);
-  for (int k = threadIdx.x; k < p.P; k += blockDim.x) s_prods[k] = p.prods[k];
-  for (int k = threadIdx.x; k < p.T; k += blockDim.x) s_terms[k] = p.terms[k];
+  if (!(lay.gtab & 2))
+    for (int k = threadIdx.x; k < p.P; k += blockDim.x) st_prods[k] = p.prods[k];
+  if (!(lay.gtab & 1))
+    for (int k = threadIdx.x; k < p.T; k += blockDim.x) st_terms[k] = p.terms[k];
   for (int k = threadIdx.x; k <= p.D; k += blockDim.x) s_toff[k] = p.term_off[k];
   for (int k = threadIdx.x; k < p.D; k += blockDim.x) {
     s_dens[k] = p.density[k];

@@ -59,6 +59,7 @@ class pfw_ace_tables(C.Structure):
         ("reference", C.POINTER(C.c_double)),
         ("pair_allowed", C.POINTER(C.c_uint8)),
         ("cutoff", C.c_double),
+        ("angular_kind", C.c_int32),
     ]
 
 
@@ -161,6 +162,7 @@ class PackedACE:
     pair_allowed: np.ndarray  # uint8 [nz]
     source_sha256: str = ""
     _keep: list = field(default_factory=list, repr=False)
+    angular_kind: int = 0  # 0 real spherical, 1 real solid r^l·Y_lm (angular_blocks.jl:25-48)
     # the resolved-schema model tree it was read from, without "parameters"
     # (written back by save_calculator); None when built from packed tables
     resolved: dict | None = field(default=None, repr=False)
@@ -220,6 +222,7 @@ class PackedACE:
         t.reference = _ptr(self.reference, C.c_double)
         t.pair_allowed = _ptr(self.pair_allowed, C.c_uint8)
         t.cutoff = self.cutoff
+        t.angular_kind = self.angular_kind
         return t
 
     def readout_mask(self) -> np.ndarray:
@@ -275,8 +278,8 @@ class PackedACE:
             "coefficient_precision": "Float64",
             "species_atomic_numbers": [int(v) for v in self.atomic_numbers],
             "reference_eV": [float(v) for v in self.reference],
-            "angular": {"kind": "real_spherical", "normalization": "L2", "ordering": "l*l+l+m+1",
-                        "lmax": int(self.lmax)},
+            "angular": {"kind": ("real_spherical", "real_solid")[self.angular_kind], "normalization": "L2",
+                        "ordering": "l*l+l+m+1", "lmax": int(self.lmax)},
             "radial": self.radial.to_dict(self.nz), "pair_radial": self.pair.to_dict(self.nz),
             "density_indices": [[int(a) + 1, int(b) + 1] for a, b in self.density],
             "products": [[int(i) + 1 for i in p] for p in self.products],
@@ -314,6 +317,7 @@ class PackedACE:
             f"{prefix}Wpair": self.Wpair,
             f"{prefix}reference": self.reference,
             f"{prefix}pair_allowed": self.pair_allowed,
+            f"{prefix}angular_kind": np.array(self.angular_kind),
         })
         return d
 
@@ -340,7 +344,8 @@ class PackedACE:
             nbasis=int(d[f"{prefix}nbasis"]), WB=np.ascontiguousarray(d[f"{prefix}WB"], dtype=np.float64),
             Wpair=np.ascontiguousarray(d[f"{prefix}Wpair"], dtype=np.float64),
             reference=np.ascontiguousarray(d[f"{prefix}reference"], dtype=np.float64),
-            pair_allowed=np.ascontiguousarray(d[f"{prefix}pair_allowed"], dtype=np.uint8))
+            pair_allowed=np.ascontiguousarray(d[f"{prefix}pair_allowed"], dtype=np.uint8),
+            angular_kind=int(d[f"{prefix}angular_kind"]) if f"{prefix}angular_kind" in d else 0)
 
     def save(self, path):
         np.savez_compressed(path, **self.to_npz_dict())
@@ -420,9 +425,13 @@ def read_resolved(D: dict) -> PackedACE:
     if len(set(z)) != nz or not all(v > 0 for v in z):
         raise argument_error("invalid species channels")
     ang = D["angular"]
-    if not (ang["kind"] == "real_spherical" and ang["normalization"] == "L2" and ang["ordering"] == "l*l+l+m+1"):
-        raise argument_error("unsupported angular convention (only real_spherical is packed for the device)")
+    if not (ang["kind"] in ("real_spherical", "real_solid") and ang["normalization"] == "L2"
+            and ang["ordering"] == "l*l+l+m+1"):
+        raise argument_error("unsupported angular convention")
+    angular_kind = 1 if ang["kind"] == "real_solid" else 0
     lmax = int(ang["lmax"])
+    if lmax < 0:
+        raise argument_error("invalid lmax")
     radial = _read_family(D["radial"], nz)
     pair = _read_family(D["pair_radial"], nz)
     density = [tuple(int(x) for x in v) for v in D["density_indices"]]
@@ -486,7 +495,7 @@ def read_resolved(D: dict) -> PackedACE:
         products=[[i - 1 for i in p] for p in products],
         coupling_rows=crow, coupling_cols=ccol, coupling_vals=uvals, nbasis=m,
         WB=np.ascontiguousarray(WB), Wpair=np.ascontiguousarray(Wpair), reference=ref.copy(),
-        pair_allowed=pair_allowed, source_sha256=str(D.get("source_sha256", "")),
+        pair_allowed=pair_allowed, source_sha256=str(D.get("source_sha256", "")), angular_kind=angular_kind,
         resolved={k: copy.deepcopy(v) for k, v in D.items() if k != "parameters"}, mask=mask,
         parameters0=parameters0)
 

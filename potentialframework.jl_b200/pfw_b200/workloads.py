@@ -88,6 +88,13 @@ def lj_1m(seed=3):
     return lj_fcc(seed=seed, nc=64)
 
 
+def supercell(s, nr):
+    """nr×nr×nr periodic copies of a system (cell vectors scaled by nr)."""
+    shifts = np.array([[a, b, c] for a in range(nr) for b in range(nr) for c in range(nr)], np.float64)
+    X = (s.X[None, :, :] + (shifts @ s.H.T)[:, None, :]).reshape(-1, 3)
+    return System(X, s.H * nr, s.pbc, np.tile(s.species, len(shifts)), name=f"{s.name}x{nr}")
+
+
 def b2(seed=4, nc=20, a=2.9, sigma=0.08):
     """B2 (CsCl): species 0 at corners, 1 at body centres."""
     rng = np.random.default_rng(seed)
