@@ -473,6 +473,7 @@ def forms(args, dev, stream, flush, F_head):
     out["lj_fcc40_256000_skin1.0_md"] = skin_form(dev, stream, flush)
     out["ace_batch4096_fp64_graph"] = batch_form(dev, stream, flush)
     out["surrogate_b2_80_1024000"] = surrogate_form(dev, stream, flush)
+    out["ace_design_rows_1024"] = design_form(dev, stream, flush)
     for name in ("lj", "ace"):
         w = Workload(name)
         h64 = lib.Handle(lib.FP64, device=dev.index)
@@ -619,6 +620,49 @@ def batch_form(dev, stream, flush, nsys=4096, steps=20):
                 max_abs_err_vs_single_system=dict(energy=err_e, force=err_f, sample=32),
                 note="n log-uniform [8,256], triclinic lengths U[6,14] Å, angles U[70,110]°, hard core 1.6 Å, "
                      "n/V <= 0.11 Å^-3 (cells redrawn), species 50/50; synthetic ACE model; FP64")
+
+
+def design_form(dev, stream, flush, nsys=1024, steps=5):
+    """Energy/force/virial design rows (design_matrix, ACE/fitting.jl:18-67)
+    of 1024 independent triclinic structures (n log-uniform on [8, 96]) with
+    the synthetic ACE model: one batched call writes the stacked rows into a
+    device buffer.  Reported as structures/s and rows/s, with the matrix's
+    bytes per second (every element is written once and, for force rows,
+    updated once per incoming edge)."""
+    import torch
+
+    from pfw_b200 import ace_generate as G
+    from pfw_b200 import lib
+    from pfw_b200 import workloads as WL
+    from pfw_b200.ace_model import read_resolved
+    model = read_resolved(G.generate_b2_model())
+    systems = WL.batched(seed=6, nsys=nsys, nmin=8, nmax=96)
+    h = lib.Handle(lib.FP64, device=dev.index)
+    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+    h.ace(model)
+    h.set_batch(systems)
+    rows, cols = h.design_shape()
+    A = torch.empty(rows * cols, dtype=torch.float64, device=dev)
+    base = torch.empty(nsys, dtype=torch.float64, device=dev)
+    ptr_a, ptr_b = ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(base.data_ptr())
+    for _ in range(2):
+        h.design_matrix_device(ptr_a, cols, rows, ptr_b)
+    torch.cuda.synchronize()
+    st = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    en = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        st[k].record(stream)
+        h.design_matrix_device(ptr_a, cols, rows, ptr_b)
+        en[k].record(stream)
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in zip(st, en)]))
+    h.close()
+    return dict(value=nsys / (ms * 1e-3), unit="structures/s", ms_per_step=ms, structures=nsys, atoms=h.n,
+                rows=rows, cols=cols, rows_per_s=rows / (ms * 1e-3),
+                matrix_gb_per_s=rows * cols * 8 / (ms * 1e-3) / 1e9,
+                note="synthetic ACE model (332 invariants, 8 pair channels, 2 species); FP64; cell lists, "
+                     "environments and the design kernel per call")
 
 
 def surrogate_form(dev, stream, flush, steps=5):

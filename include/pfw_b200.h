@@ -211,6 +211,22 @@ pfw_status pfw_set_batch_device(pfw_ws* ws, int32_t nsys, const int64_t* atom_of
  * evaluation; on_device != 0: X is device memory (queued, no sync).  A
  * captured batch graph stays valid. */
 pfw_status pfw_batch_update_positions(pfw_ws* ws, const double* X, int32_t on_device);
+/* Dense energy/force/virial design rows of the loaded ACE model for the
+ * current geometry or batch: replaces design_matrix(X, model, ps, env, H;
+ * fit_pair=true) (ACE/fitting.jl:18-67) for every structure at once, the
+ * assembly ACEfit stacks.  Rows of system s start at 10·s + 3·(atoms before
+ * s): the energy row, 3 force rows per atom (original order, component
+ * fastest), the 9 virial rows (column-major 3×3); columns (row-major, leading
+ * dimension ld ≥ cols) are vec(WB) (species block z at z·nbasis + b) then
+ * vec(Wpair) (nz·nbasis + z·nQ + q), so A·[vec(WB); vec(Wpair)] + baseline
+ * reproduces [E; F; W].  baseline[s] (optional, nsys) is the structure's sum
+ * of reference energies (the energy row's baseline; the other rows' are 0).
+ * Rows are deterministic.  PFW_ESHAPE when the buffer is too small. */
+pfw_status pfw_ace_design_shape(pfw_ws* ws, int64_t* rows, int64_t* cols);
+pfw_status pfw_ace_design_matrix(pfw_ws* ws, double* A, int64_t ld, int64_t rows_capacity, double* baseline);
+pfw_status pfw_ace_design_matrix_device(pfw_ws* ws, double* A_dev, int64_t ld, int64_t rows_capacity,
+                                        double* baseline_dev);
+
 /* Per-structure fitting features of the loaded ACE model: nz·(nB + nQ)
  * values per system, laid out [Σ_i B_i of species block z (nB each, z =
  * 0..nz-1), then Σ_{i,j} Q[j,:] of species block z (nQ each)] — the energy

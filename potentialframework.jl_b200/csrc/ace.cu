@@ -26,6 +26,7 @@
 #include <string>
 #include <vector>
 
+#include "ace_design.cuh"
 #include "ace_math.cuh"
 #include "ace_site.cuh"
 #include "pfw_internal.h"
@@ -59,6 +60,8 @@ struct AceDevice {
   DevBuf unit_begin, unit_out;  // single system: one unit per site
   // batch: units of at most BATCH_UNIT_SITES sites, never spanning two systems
   DevBuf batch_units, batch_sys_units, batch_out, batch_feat;
+  DevBuf design_G;      // design rows: product factor gradients, one row per site group
+  DevBuf design_order;  // design rows: systems largest first, then the work counter
   uint64_t batch_version = ~0ull;
   int batch_nunits = 0;
   std::vector<int> h_batch_units, h_batch_sys_units;
@@ -290,7 +293,8 @@ static void free_device(AceDevice* a) {
                     &a->weights, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm, &a->crow_off, &a->crow_k, &a->crow_val,
                     &a->edge_count, &a->edge_off, &a->edge_j, &a->edge_d, &a->edge_S, &a->edge_rev, &a->edge_g,
                     &a->site_out, &a->site_E_orig, &a->status, &a->unit_begin, &a->unit_out,
-                    &a->batch_units, &a->batch_sys_units, &a->batch_out, &a->batch_feat};
+                    &a->batch_units, &a->batch_sys_units, &a->batch_out, &a->batch_feat, &a->design_G,
+                    &a->design_order};
   for (auto* b : bufs) b->release();
   delete a;
 }
@@ -878,6 +882,99 @@ void ace_batch_graph_sync(pfw_ws* ws) {
     if (e.code == PFW_ECAPACITY) release_graph(a);  // the next launch re-plans
     throw;
   }
+}
+
+// ---------------------------------------------------------------------------
+// design rows (design_matrix_impl, ACE/fitting.jl:18-67)
+// ---------------------------------------------------------------------------
+// The adjoint terms are never read; products staged where they fit.
+static AceLayout choose_design_layout(const AceTables& p, int device) {
+  int optin = 0;
+  PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  const int cand[][2] = {{16, 4}, {8, 8}, {16, 2}, {8, 4}, {8, 2}, {8, 1}};
+  for (auto& c : cand) {
+    if (c[0] > ACE_MAX_CHUNK || c[1] > ACE_MAX_GROUPS) continue;
+    for (int gt : {1, 3}) {
+      AceLayout lay;
+      lay.make(p, c[0], c[1], 0, 0, gt, 1);
+      if (lay.total <= (size_t)optin) return lay;
+    }
+  }
+  throw Error(PFW_EINVAL, "ACE model too large for the design kernel's shared memory");
+}
+
+template <int L>
+static void launch_design(const AceTables& p, const AceLayout& lay, int nsys, const SysGeom* sysv, AceDevice* a,
+                          const pfw_ws* ws, double* A_dev, int64_t ld, double* base_dev) {
+  auto kern = k_ace_design<L>;
+  PFW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total));
+  int sms = 0, per_sm = 0;
+  PFW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws->opt.device));
+  PFW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, ACE_GROUP * lay.G, lay.total));
+  per_sm = std::max(per_sm, 1);
+  // column slices per system so that small batches still fill every group
+  const int slots = sms * per_sm * lay.G;
+  const int nslice = nsys >= slots ? 1 : std::max(1, std::min((slots + nsys - 1) / nsys, (p.nB + ACE_GROUP - 1) / ACE_GROUP));
+  const int blocks = std::max(1, std::min(sms * per_sm, (nsys * nslice + lay.G - 1) / lay.G));
+  // one row of product factor gradients per site group
+  double4* gs = static_cast<double4*>(a->design_G.ensure(sizeof(double4) * (size_t)blocks * lay.G * p.P));
+  // systems by decreasing atom count, handed out by a counter
+  std::vector<int> order(nsys);
+  for (int s = 0; s < nsys; ++s) order[s] = s;
+  const auto& ps = ws->prep.sys;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return ps[x].natoms > ps[y].natoms; });
+  int* dorder = static_cast<int*>(a->design_order.ensure(sizeof(int) * (nsys + 1)));
+  PFW_CUDA(cudaMemcpyAsync(dorder, order.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, ws->stream));
+  PFW_CUDA(cudaMemsetAsync(dorder + nsys, 0, sizeof(int), ws->stream));
+  kern<<<blocks, ACE_GROUP * lay.G, lay.total, ws->stream>>>(
+      p, lay, nsys, sysv, a->cap, a->edge_off.as<int>(), a->edge_j.as<int>(), a->edge_d.as<double4>(),
+      ws->pos.as<double4>(), ws->perm.as<int>(), gs, dorder, dorder + nsys, nslice, A_dev, ld, base_dev,
+      a->status.as<int>());
+}
+
+void ace_design_shape(pfw_ws* ws, int64_t* rows, int64_t* cols) {
+  AceDevice* a = ws->ace;
+  if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
+  if (rows) *rows = 10 * (int64_t)ws->systems.size() + 3 * (int64_t)ws->n;
+  if (cols) *cols = (int64_t)a->nz * (a->nB + a->nQ);
+}
+
+void ace_design_matrix(pfw_ws* ws, double* A_dev, int64_t ld, int64_t rows_capacity, double* base_dev) {
+  AceDevice* a = ws->ace;
+  if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
+  if (ws->max_species >= a->nz) throw Error(PFW_EINVAL, "ACE model has no element channel for a species");
+  if (a->nQ > 4 * ACE_GROUP) throw Error(PFW_EINVAL, "design rows support at most 256 pair channels");
+  int64_t rows = 0, cols = 0;
+  ace_design_shape(ws, &rows, &cols);
+  if (!A_dev) throw Error(PFW_EINVAL, "null design matrix");
+  if (ld < cols || rows_capacity < rows) throw Error(PFW_ESHAPE, "design matrix buffer too small");
+  cudaStream_t st = ws->stream;
+  ws->prep.valid = false;
+  prepare(ws, a->cutoff);
+  a->status.ensure(sizeof(int) * 4);
+  PFW_CUDA(cudaMemsetAsync(a->status.ptr, 0, sizeof(int) * 4, st));
+  build_edges(ws, a);
+  a->n = ws->prep.n;
+  const int nsys = (int)ws->prep.sys.size();
+  const AceTables p = tables_of(a);
+  const AceLayout lay = choose_design_layout(p, ws->opt.device);
+  // the rows arrive zeroed; the kernel only adds
+  PFW_CUDA(cudaMemset2DAsync(A_dev, sizeof(double) * ld, 0, sizeof(double) * cols, rows, st));
+  if (nsys > 0) {
+    const SysGeom* sysv = ws->sysgeom.as<SysGeom>();
+    switch (a->lmax) {
+      case 0: launch_design<0>(p, lay, nsys, sysv, a, ws, A_dev, ld, base_dev); break;
+      case 1: launch_design<1>(p, lay, nsys, sysv, a, ws, A_dev, ld, base_dev); break;
+      case 2: launch_design<2>(p, lay, nsys, sysv, a, ws, A_dev, ld, base_dev); break;
+      case 3: launch_design<3>(p, lay, nsys, sysv, a, ws, A_dev, ld, base_dev); break;
+      case 4: launch_design<4>(p, lay, nsys, sysv, a, ws, A_dev, ld, base_dev); break;
+      case 5: launch_design<5>(p, lay, nsys, sysv, a, ws, A_dev, ld, base_dev); break;
+      default: launch_design<6>(p, lay, nsys, sysv, a, ws, A_dev, ld, base_dev); break;
+    }
+    ws->launches += 1;
+  }
+  a->evaluated = false;
+  ace_check(ws, a);
 }
 
 void ace_site_energies(pfw_ws* ws, double* host) {

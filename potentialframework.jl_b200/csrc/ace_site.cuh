@@ -95,10 +95,10 @@ struct AceLayout {
   size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, tables_end;
   size_t group_bytes, total;
   // group-relative double offsets
-  int A, dA, Y, dY, R, dR, T1, T2, esc, F, QV, WK, WQ, ints;
+  int A, dA, Y, dY, R, dR, T1, T2, esc, F, QV, WK, WQ, DD, QD, ints;
   __host__ __device__ static size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
   __host__ __device__ void make(const AceTables& t, int ch, int g, int with_feat = 0, int sur_pass = 0,
-                                int global_tables = 0) {
+                                int global_tables = 0, int design = 0) {
     CH = ch;
     G = g;
     sur = sur_pass;
@@ -131,6 +131,8 @@ struct AceLayout {
     QV = d; d += feat ? CH * t.nQ : 0;  // pair radial values of the chunk
     WK = d; d += sur == 2 ? t.P : 0;   // per-site product weights
     WQ = d; d += sur == 2 ? t.nQ : 0;  // per-site pair weights
+    DD = d; d += design ? CH * (t.D + 1) * 3 : 0;  // design rows: ∂A_a/∂d of the chunk's edges (+ a zero row)
+    QD = d; d += design ? CH * t.nQ * 2 : 0;  // design rows: pair values and d/dr
     ints = d; d += CH;               // 2 ints per edge
     group_bytes = align16(sizeof(double) * d);
     total = tables_end + group_bytes * G;

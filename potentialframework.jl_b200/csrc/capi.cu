@@ -335,6 +335,41 @@ pfw_status pfw_ace_feature_count(pfw_ws* ws, int32_t* nfeat) {
   });
 }
 
+pfw_status pfw_ace_design_shape(pfw_ws* ws, int64_t* rows, int64_t* cols) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    pfw::ace_design_shape(ws, rows, cols);
+  });
+}
+
+pfw_status pfw_ace_design_matrix_device(pfw_ws* ws, double* A_dev, int64_t ld, int64_t rows_capacity,
+                                        double* baseline_dev) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    pfw::ace_design_matrix(ws, A_dev, ld, rows_capacity, baseline_dev);
+  });
+}
+
+pfw_status pfw_ace_design_matrix(pfw_ws* ws, double* A, int64_t ld, int64_t rows_capacity, double* baseline) {
+  return guarded(ws, [&] {
+    if (ws->systems.empty()) throw Error(PFW_ESTATE, "no geometry set");
+    if (!A) throw Error(PFW_EINVAL, "null design matrix");
+    int64_t rows = 0, cols = 0;
+    pfw::ace_design_shape(ws, &rows, &cols);
+    if (ld < cols || rows_capacity < rows) throw Error(PFW_ESHAPE, "design matrix buffer too small");
+    const size_t nsys = ws->systems.size();
+    double* dA = static_cast<double*>(ws->out_design.ensure(sizeof(double) * std::max<int64_t>(rows * cols, 1)));
+    double* dB = static_cast<double*>(ws->out_base.ensure(sizeof(double) * std::max<size_t>(nsys, 1)));
+    pfw::ace_design_matrix(ws, dA, cols, rows, dB);
+    if (rows > 0 && cols > 0)
+      PFW_CUDA(cudaMemcpy2DAsync(A, sizeof(double) * ld, dA, sizeof(double) * cols, sizeof(double) * cols, rows,
+                                 cudaMemcpyDeviceToHost, ws->stream));
+    if (baseline && nsys > 0)
+      PFW_CUDA(cudaMemcpyAsync(baseline, dB, sizeof(double) * nsys, cudaMemcpyDeviceToHost, ws->stream));
+    PFW_CUDA(cudaStreamSynchronize(ws->stream));
+  });
+}
+
 pfw_status pfw_evaluate_batch_device(pfw_ws* ws, int32_t model, uint32_t request, double* E_dev, double* F_dev,
                                      double* W_dev, double* features_dev) {
   return guarded(ws, [&] {

@@ -108,7 +108,7 @@ struct pfw_ws {
       perm, inverse, pos, pos32, scan_tmp, minmax;
   // pair evaluation
   pfw::PairModel pair;
-  pfw::DevBuf cellpart, out_E, out_F, out_W, out_feat, counters, red_partial;
+  pfw::DevBuf cellpart, out_E, out_F, out_W, out_feat, counters, red_partial, out_design, out_base;
   int64_t last_pairs = -1;
   // neighbour snapshot
   pfw::DevBuf nb_count, nb_offsets, nb_j, nb_S, nb_R;
@@ -167,6 +167,8 @@ void ace_site_energies(pfw_ws* ws, double* host);
 // zero the E/W partials of sites whose atom is a ghost copy (perm[s] >= n_owned)
 void mask_unowned_sites(pfw_ws* ws, double* site_out, int n);
 int ace_feature_count(pfw_ws* ws);
+void ace_design_shape(pfw_ws* ws, int64_t* rows, int64_t* cols);
+void ace_design_matrix(pfw_ws* ws, double* A_dev, int64_t ld, int64_t rows_capacity, double* base_dev);
 void ace_evaluate_batch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev);
 void ace_batch_graph(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev);
 void ace_batch_graph_sync(pfw_ws* ws);

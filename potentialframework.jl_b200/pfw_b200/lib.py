@@ -75,6 +75,9 @@ def load():
     L.pfw_set_batch_device.argtypes = [vp, C.c_int32, i64p, vp, dp, u8p, vp]
     L.pfw_batch_update_positions.argtypes = [vp, vp, C.c_int32]
     L.pfw_ace_feature_count.argtypes = [vp, i32p]
+    L.pfw_ace_design_shape.argtypes = [vp, i64p, i64p]
+    L.pfw_ace_design_matrix.argtypes = [vp, dp, C.c_int64, C.c_int64, dp]
+    L.pfw_ace_design_matrix_device.argtypes = [vp, vp, C.c_int64, C.c_int64, vp]
     L.pfw_evaluate_batch.argtypes = [vp, C.c_int32, C.c_uint32, dp, dp, dp, dp]
     L.pfw_evaluate_batch_device.argtypes = [vp, C.c_int32, C.c_uint32, vp, vp, vp, vp]
     L.pfw_batch_graph_launch.argtypes = [vp, C.c_uint32, vp, vp, vp, vp]
@@ -245,6 +248,24 @@ class Handle:
         v = np.zeros(1, np.int32)
         self.check(self.L.pfw_ace_feature_count(self.ws, ptr(v, C.c_int32)))
         return int(v[0])
+
+    def design_shape(self):
+        r = np.zeros(2, np.int64)
+        self.check(self.L.pfw_ace_design_shape(self.ws, ptr(r[:1], C.c_int64), ptr(r[1:], C.c_int64)))
+        return int(r[0]), int(r[1])
+
+    def design_matrix(self):
+        """Stacked design rows [rows × cols] of the current geometry or batch
+        and the per-system reference-energy baselines [nsys]."""
+        rows, cols = self.design_shape()
+        A = np.zeros((rows, cols))
+        nsys = (rows - 3 * self.n) // 10
+        base = np.zeros(max(nsys, 1))
+        self.check(self.L.pfw_ace_design_matrix(self.ws, ptr(A, C.c_double), cols, rows, ptr(base, C.c_double)))
+        return A, base[:nsys]
+
+    def design_matrix_device(self, A_ptr, ld, rows_capacity, base_ptr=None):
+        self.check(self.L.pfw_ace_design_matrix_device(self.ws, A_ptr, ld, rows_capacity, base_ptr))
 
     def evaluate_batch(self, model=MODEL_ACE, request=7, features=False):
         """Per-system E [nsys], F [N×3], W [nsys×3×3] and (ACE) fitting features [nsys×nfeat]."""
