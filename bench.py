@@ -737,7 +737,7 @@ def surrogate_form(dev, stream, flush, steps=5):
                 training=dict(environments=int(len(E)), epochs=40, members=S.MEMBERS, features=S.NIN,
                               hidden=S.HIDDEN, final_loss=sur.history[-1], label_s=t1 - t0, train_s=t2 - t1,
                               tau_eV=sur.tau),
-                note="MLP 64->64->64->1 SiLU, BF16 weights, FP32 arithmetic, ensemble of 4 per species; "
+                note="MLP 64->64->64->1 SiLU, BF16 weights, tcgen05 TF32 products with hi/lo activation split (FP32 accuracy), ensemble of 4 per species; "
                      "features: the 8 order-1 and first 48 order-2 invariants plus 8 pair radial sums; "
                      "gate: standardised training range +-5 % or ensemble std > tau; FP64 features and pullback")
 

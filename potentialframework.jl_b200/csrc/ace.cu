@@ -29,6 +29,7 @@
 #include "ace_design.cuh"
 #include "ace_math.cuh"
 #include "ace_site.cuh"
+#include "mlp_tc.cuh"
 #include "pfw_internal.h"
 #include "traverse.cuh"
 
@@ -699,6 +700,7 @@ static void ace_check(pfw_ws* ws, AceDevice* a) {
   if (hs[0] & 2) throw Error(PFW_EDOMAIN, "coincident physical atoms have undefined harmonics / pair envelope");
   if (hs[0] & 8) throw Error(PFW_ECAPACITY, "neighbour environments outgrew the planned capacity; re-plan");
   if (hs[0] & 4) throw Error(PFW_EINVAL, "internal: reverse edge not found");
+  if (hs[0] & 16) throw Error(PFW_ETIMEDOUT, "a tensor-core wait of the surrogate MLP ran out");
 }
 
 void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev) {
@@ -1056,7 +1058,6 @@ void sur_free(pfw_ws* ws) {
 }
 
 constexpr int SUR_MAXW = 64;   // MLP kernel: nin, hidden <= 64
-constexpr int SUR_TILE = 64;   // sites per MLP tile
 
 void sur_load(pfw_ws* ws, const pfw_ace_tables* t, const pfw_mlp_params* mp) {
   if (t->nbasis + t->pair.nchannels < 1) throw Error(PFW_EINVAL, "feature model has no features");
@@ -1149,203 +1150,6 @@ __global__ void k_species_lists(int n, int nz, const double4* __restrict__ pos, 
   if (s >= n) return;
   const int z = min(max((int)pos[s].w, 0), nz - 1);
   list[(size_t)z * n + atomicAdd(count + z, 1)] = s;
-}
-
-__device__ __forceinline__ float bf16f(unsigned short b) { return __uint_as_float((unsigned)b << 16); }
-
-// The MLP ensemble on a tile of 64 sites of one species: standardised
-// inputs, forward and backward passes of every member as 64×64 tiles in
-// shared memory (FP32, BF16-valued weights), the site energy without the
-// reference, dE/dfeature and the gate.  Thread (r, c) owns rows r + 16i and
-// columns c + 16j (i, j < 4) of every 64×64 product.
-__global__ void __launch_bounds__(256)
-    k_sur_mlp(SurParams sp, int n, const int* __restrict__ count, const int* __restrict__ list) {
-  extern __shared__ float smf[];
-  const int z = blockIdx.y, tile = blockIdx.x;
-  const int cnt = count[z];
-  const int l0 = tile * SUR_TILE;
-  if (l0 >= cnt) return;
-  const int rows = min(SUR_TILE, cnt - l0);
-  const int* L = list + (size_t)z * n + l0;
-  const int nin = sp.nin, H = sp.H, M = sp.M, ST = SUR_MAXW + 1;
-  float* X = smf;                 // [64][ST] standardised inputs
-  float* W1 = X + SUR_TILE * ST;  // [H][ST]
-  float* W2 = W1 + SUR_MAXW * ST; // [H][ST]
-  float* H1 = W2 + SUR_MAXW * ST;
-  float* S1 = H1 + SUR_TILE * ST;
-  float* H2 = S1 + SUR_TILE * ST;
-  float* S2 = H2 + SUR_TILE * ST;
-  float* D2 = S2 + SUR_TILE * ST;
-  float* D1 = D2 + SUR_TILE * ST;
-  float* ym = D1 + SUR_TILE * ST;  // [4][64]
-  float* vec = ym + 4 * SUR_TILE;  // b1, b2, w3 of a member: [3][64]
-  int* gate = reinterpret_cast<int*>(vec + 3 * SUR_MAXW);  // [64]
-  const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
-  for (int k = tid; k < SUR_TILE * SUR_MAXW; k += 256) {
-    const int r = k / SUR_MAXW, i = k - r * SUR_MAXW;
-    float x = 0.f;
-    if (r < rows && i < nin) {
-      const double raw = sp.site_feat[(size_t)L[r] * nin + i];
-      x = (float)((raw - sp.x_mean[z * nin + i]) / sp.x_std[z * nin + i]);
-    }
-    X[r * ST + i] = x;
-  }
-  if (tid < SUR_TILE) gate[tid] = 0;
-  __syncthreads();
-  for (int k = tid; k < rows * nin; k += 256) {
-    const int r = k / nin, i = k - r * nin;
-    const float x = X[r * ST + i];
-    if (!(x >= sp.x_lo[z * nin + i] && x <= sp.x_hi[z * nin + i])) gate[r] = 1;  // NaN-safe
-  }
-  float dx[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) dx[a][b] = 0.f;
-  for (int m = 0; m < M; ++m) {
-    const size_t zm = (size_t)z * M + m;
-    __syncthreads();
-    for (int k = tid; k < H * nin; k += 256) W1[(k / nin) * ST + k % nin] = bf16f(sp.W1[zm * H * nin + k]);
-    for (int k = tid; k < H * H; k += 256) W2[(k / H) * ST + k % H] = bf16f(sp.W2[zm * H * H + k]);
-    for (int k = tid; k < H; k += 256) {
-      vec[k] = sp.b1[zm * H + k];
-      vec[SUR_MAXW + k] = sp.b2[zm * H + k];
-      vec[2 * SUR_MAXW + k] = bf16f(sp.w3[zm * H + k]);
-    }
-    __syncthreads();
-    // layer 1: Z1 = X·W1ᵀ + b1
-    {
-      float acc[4][4] = {};
-      for (int k = 0; k < nin; ++k) {
-        float a[4], b[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          a[q] = X[(tr + 16 * q) * ST + k];
-          b[q] = W1[(tc + 16 * q) * ST + k];
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int r = tr + 16 * i, o = tc + 16 * j;
-          if (o < H) {
-            const float zz = acc[i][j] + vec[o];
-            const float sg = 1.f / (1.f + expf(-zz));
-            H1[r * ST + o] = zz * sg;
-            S1[r * ST + o] = sg * (1.f + zz * (1.f - sg));
-          }
-        }
-    }
-    __syncthreads();
-    // layer 2: Z2 = H1·W2ᵀ + b2
-    {
-      float acc[4][4] = {};
-      for (int k = 0; k < H; ++k) {
-        float a[4], b[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          a[q] = H1[(tr + 16 * q) * ST + k];
-          b[q] = W2[(tc + 16 * q) * ST + k];
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int r = tr + 16 * i, o = tc + 16 * j;
-          if (o < H) {
-            const float zz = acc[i][j] + vec[SUR_MAXW + o];
-            const float sg = 1.f / (1.f + expf(-zz));
-            H2[r * ST + o] = zz * sg;
-            S2[r * ST + o] = sg * (1.f + zz * (1.f - sg));
-            D2[r * ST + o] = vec[2 * SUR_MAXW + o] * S2[r * ST + o];
-          }
-        }
-    }
-    __syncthreads();
-    // output layer
-    if (tid < SUR_TILE) {
-      float y = sp.b3[zm];
-      for (int o = 0; o < H; ++o) y = fmaf(vec[2 * SUR_MAXW + o], H2[tid * ST + o], y);
-      ym[m * SUR_TILE + tid] = y;
-    }
-    // D1 = (D2·W2) ⊙ S1
-    {
-      float acc[4][4] = {};
-      for (int o = 0; o < H; ++o) {
-        float a[4], b[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          a[q] = D2[(tr + 16 * q) * ST + o];
-          b[q] = W2[o * ST + tc + 16 * q];
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int r = tr + 16 * i, c = tc + 16 * j;
-          if (c < H) D1[r * ST + c] = acc[i][j] * S1[r * ST + c];
-        }
-    }
-    __syncthreads();
-    // dX += D1·W1
-    for (int o = 0; o < H; ++o) {
-      float a[4], b[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a[q] = D1[(tr + 16 * q) * ST + o];
-        b[q] = W1[o * ST + tc + 16 * q];
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) dx[i][j] = fmaf(a[i], b[j], dx[i][j]);
-    }
-  }
-  __syncthreads();
-  const double ysd = sp.y_std[z];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = tr + 16 * i;
-    if (r >= rows) continue;
-    const size_t s = L[r];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int c = tc + 16 * j;
-      if (c < nin) sp.site_df[s * nin + c] = ysd * (double)(dx[i][j] / (float)M) / sp.x_std[z * nin + c];
-    }
-  }
-  if (tid < rows) {
-    float mean = 0.f;
-    for (int m = 0; m < M; ++m) mean += ym[m * SUR_TILE + tid];
-    mean /= (float)M;
-    float var = 0.f;
-    for (int m = 0; m < M; ++m) var += (ym[m * SUR_TILE + tid] - mean) * (ym[m * SUR_TILE + tid] - mean);
-    var /= (float)M;
-    const int s = L[tid];
-    sp.site_e[s] = sp.y_mean[z] + ysd * (double)mean;
-    sp.flags[s] = (gate[tid] || !(ysd * (double)sqrtf(var) <= (double)sp.tau)) ? 1 : 0;
-  }
-}
-
-static size_t sur_mlp_smem() {
-  const int ST = SUR_MAXW + 1;
-  return sizeof(float) * ((size_t)SUR_TILE * ST * 7 + (size_t)SUR_MAXW * ST * 2 + 4 * SUR_TILE + 3 * SUR_MAXW) +
-         sizeof(int) * SUR_TILE;
 }
 
 static void sur_prepare(pfw_ws* ws, SurDevice* d) {
@@ -1484,9 +1288,9 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   PFW_CUDA(cudaMemsetAsync(zc, 0, sizeof(int) * d->nz, st));
   if (n > 0) {
     k_species_lists<<<grid_for(n, 256), 256, 0, st>>>(n, d->nz, ws->pos.as<double4>(), zc, zl);
-    const size_t smem = sur_mlp_smem();
-    PFW_CUDA(cudaFuncSetAttribute(k_sur_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_sur_mlp<<<dim3(grid_for(n, SUR_TILE), d->nz), 256, smem, st>>>(s.sur, n, zc, zl);
+    const size_t smem = tc_mlp_smem();
+    PFW_CUDA(cudaFuncSetAttribute(k_sur_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_sur_mlp_tc<<<dim3(grid_for(n, TC_TILE), d->nz), 256, smem, st>>>(s.sur, n, zc, zl, a->status.as<int>());
     ws->launches += 2;
   }
   // 3. pullback with the per-site weights
