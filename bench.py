@@ -432,7 +432,7 @@ def run_b200(args):
                      h2d_bytes_per_step=28 * w.n, d2h_bytes_per_step=24 * w.n + 8 + 72,
                      api="pfw_set_geometry + pfw_evaluate (host buffers, pinned)"),
             gpu_launches=launches, clocks=clk)
-        if not args.no_forms:
+        if not args.no_forms and world == 1:  # single-GPU configurations; the other ranks would idle at a barrier
             line["forms"] = forms(args, dev, stream, flush, F_ref)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(w)
