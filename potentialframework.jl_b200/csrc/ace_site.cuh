@@ -29,7 +29,7 @@ namespace pfw {
 #endif
 constexpr int ACE_GROUP = PFW_ACE_GROUP;
 constexpr int ACE_MAX_GROUPS = 512 / ACE_GROUP;
-constexpr int ACE_MAX_CHUNK = ACE_GROUP / 4;  // four threads per edge of a chunk
+constexpr int ACE_MAX_CHUNK = ACE_GROUP / 4;  // at least four threads per edge of a chunk
 static_assert(ACE_GROUP == 64 || ACE_GROUP == 128, "site groups of 64 or 128 threads");
 
 struct AceTables {
@@ -150,10 +150,11 @@ struct EdgeScalars {
   int *k0, *pidx;
 };
 
-// Per-edge set-up of one chunk, four threads per edge (lt = 4t + q):
-// q = 0 the R-family transform/interval/envelope (shared with the edge's
-// other three threads by shuffles), q = 1 the pair radials, harmonics split
-// by azimuthal order m ≡ q (mod 4), and the R channels n ≡ q (mod 4)
+// Per-edge set-up of one chunk, ACE_GROUP / CH threads per edge (4 or 8;
+// lt = tpe·t + q): q = 0 the R-family transform/interval/envelope (shared
+// with the edge's other threads by shuffles), q = 1 the pair radials,
+// harmonics split by azimuthal order m ≡ q (mod tpe), and the R channels
+// n ≡ q (mod tpe)
 // (values, and derivatives when Grad) — so no separate radial phase and
 // barrier follow.
 template <int L, class T, bool Grad>
@@ -161,7 +162,9 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
                                                 const EdgeScalars<T>& es, const double4* __restrict__ edge_d, int e0,
                                                 int nc, int iz, int lt, double& e_acc, int* status,
                                                 const double* wq = nullptr) {
-  const int t = lt >> 2, q = lt & 3;
+  // ACE_GROUP / CH threads per edge: 4 for chunks of 16 edges, 8 for chunks of 8
+  const int tpe = ACE_GROUP / lay.CH, tsh = 31 - __clz(tpe);
+  const int t = lt >> tsh, q = lt & (tpe - 1);
   if (t >= nc) return;
   const double4 d = edge_d[e0 + t];
   const int zj = min(max((int)d.w, 0), p.nz - 1);
@@ -208,7 +211,7 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   double* dYt = gbase + lay.dY + t * lay.YS * 3;
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
-    if ((m & 3) != q) continue;
+    if ((m & (tpe - 1)) != q) continue;
     harmonics_m<T, Grad, L>(
         p.Fnorm, r, dx, dy, dz, m,
         [&](int idx, const Jet<T, Grad>& j) {
@@ -221,11 +224,11 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
         },
         p.solid != 0);
   }
-  // the edge's radial set-up from its first thread (the four threads of an
+  // the edge's radial set-up from its first thread (the tpe threads of an
   // edge are consecutive lanes of one warp, all inside or all outside nc)
   const int lane = lt & 31;
-  const unsigned quad = 0xFu << (lane & 28);
-  const int src = lane & 28;
+  const int src = lane & ~(tpe - 1);
+  const unsigned quad = ((1u << tpe) - 1u) << src;
   er.k0 = __shfl_sync(quad, er.k0, src);
   er.u = __shfl_sync(quad, er.u, src);
   er.e = __shfl_sync(quad, er.e, src);
@@ -235,7 +238,7 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   }
   double* Rt = gbase + lay.R + t * lay.RS;
   double* dRt = gbase + lay.dR + t * lay.RS;
-  for (int n = q; n < p.nR; n += 4) {
+  for (int n = q; n < p.nR; n += tpe) {
     const double* c = channel_coeff(p.R, pidx, er.k0, n);
     if constexpr (Grad) {
       T v, dv;
@@ -435,20 +438,20 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
           T2[t * YS + m] = acc;
         }
         group_sync(g);
-        // 4 threads per edge (CH <= ACE_MAX_CHUNK)
-        const int t = lt >> 2, q4 = lt & 3;
+        // ACE_GROUP / CH threads per edge (4 or 8)
+        const int tpe = ACE_GROUP / CH, tsh = 31 - __clz(tpe);
+        const int t = lt >> tsh, q4 = lt & (tpe - 1);
         T s1 = T(0), gx = T(0), gy = T(0), gz = T(0);
         if (t < nc) {
-          for (int n = q4; n < nR; n += 4) s1 += (T)dRc[t * RS + n] * (T)T1[t * RS + n];
-          for (int m = q4; m < nY; m += 4) {
+          for (int n = q4; n < nR; n += tpe) s1 += (T)dRc[t * RS + n] * (T)T1[t * RS + n];
+          for (int m = q4; m < nY; m += tpe) {
             const T t2 = (T)T2[t * YS + m];
             gx += (T)dYc[(t * YS + m) * 3] * t2;
             gy += (T)dYc[(t * YS + m) * 3 + 1] * t2;
             gz += (T)dYc[(t * YS + m) * 3 + 2] * t2;
           }
         }
-#pragma unroll
-        for (int o = 1; o < 4; o <<= 1) {
+        for (int o = 1; o < tpe; o <<= 1) {
           s1 += __shfl_xor_sync(0xffffffffu, s1, o);
           gx += __shfl_xor_sync(0xffffffffu, gx, o);
           gy += __shfl_xor_sync(0xffffffffu, gy, o);
