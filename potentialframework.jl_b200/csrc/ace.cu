@@ -262,6 +262,11 @@ static RadialDev upload_family(const pfw_radial_family& f, int nz, DevBuf& len, 
     const int kind = f.envelope_kind[k];
     if (kind < 1 || kind > 3) throw Error(PFW_EINVAL, "unsupported radial envelope");
     if (f.powers[2 * k] <= 0 || f.powers[2 * k + 1] < f.powers[2 * k]) throw Error(PFW_EINVAL, "invalid Agnesi transform");
+    // read_radial's node rule (ACE/resolved.jl:80-81): -1 = first < ... < last = 1
+    const double* nd = f.nodes + (size_t)k * f.nknots;
+    bool sorted = nd[0] == -1.0 && nd[f.lengths[k] - 1] == 1.0;
+    for (int i = 1; i < f.lengths[k]; ++i) sorted = sorted && nd[i] > nd[i - 1];
+    if (!sorted) throw Error(PFW_EINVAL, "spline nodes must increase from -1 to 1");
   }
   RadialDev d;
   d.nch = f.nchannels;

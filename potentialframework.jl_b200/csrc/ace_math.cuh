@@ -109,15 +109,18 @@ __device__ __forceinline__ EdgeRadial<T> edge_radial(const RadialDev& f, int pid
       o.de = (T(-pp) * ipow(ss, -pp - 1) * (T(1) - ss) - (ipow(ss, -pp) - T(1))) / rc;
     }
   }
-  // searchsortedlast(nodes, x) clamped to [1, K-1] (1-based)
+  // searchsortedlast(nodes, x) clamped to [1, K-1] (1-based).  The nodes run
+  // from -1 to 1 (checked at load); the interval of a uniform grid is the
+  // first guess and the node values themselves settle it, so the count of
+  // nodes <= x is exactly the bisection's, in one round of loads instead of
+  // log2(K) dependent ones.
   const double* nd = f.nodes + (size_t)f.nknots * pidx;
   const int K = f.lengths[pidx];
-  int lo = 0, hi = K;  // count of nodes <= x
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if ((T)nd[mid] <= x) lo = mid + 1;
-    else hi = mid;
-  }
+  const T gd = (x + T(1)) * (T)(0.5 * (K - 1));
+  int gi = gd >= T(0) ? (gd < (T)(K - 1) ? (int)gd : K - 1) : 0;  // NaN → 0
+  while (gi + 1 < K && (T)nd[gi + 1] <= x) ++gi;
+  while (gi >= 0 && (T)nd[gi] > x) --gi;
+  const int lo = gi + 1;  // count of nodes <= x
   int k = lo < 1 ? 1 : (lo > K - 1 ? K - 1 : lo);
   o.k0 = k - 1;
   const T step = (T)nd[k] - (T)nd[k - 1];

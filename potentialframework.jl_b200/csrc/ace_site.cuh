@@ -157,12 +157,51 @@ struct EdgeScalars {
 // n ≡ q (mod tpe)
 // (values, and derivatives when Grad) — so no separate radial phase and
 // barrier follow.
+// Channels n ≡ q (mod tpe) of one radial family for one edge, NB channels'
+// coefficients loaded before any is evaluated (independent loads in flight).
+// on(n, v, dv) receives each channel's value and d/dr (dv unused without Grad).
+template <class T, bool Grad, int NB, class On>
+__device__ __forceinline__ void edge_channels(const RadialDev& f, int pidx, const EdgeRadial<T>& er, int q, int tpe,
+                                              On&& on) {
+  const double* cb = channel_coeff(f, pidx, er.k0, 0);
+  for (int n0 = q; n0 < f.nch; n0 += NB * tpe) {
+    double2 lo[NB], hi[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const int n = n0 + j * tpe;
+      if (n < f.nch) {
+        const double2* cp = reinterpret_cast<const double2*>(cb + 4 * n);
+        lo[j] = __ldg(cp);
+        hi[j] = __ldg(cp + 1);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const int n = n0 + j * tpe;
+      if (n >= f.nch) break;
+      const T c0 = (T)lo[j].x, c1 = (T)lo[j].y, c2 = (T)hi[j].x, c3 = (T)hi[j].y, u = er.u;
+      const T v = ((c3 * u + c2) * u + c1) * u + c0;
+      if constexpr (Grad) {
+        const T dv = (T(3) * c3 * (u * u) + T(2) * c2 * u + c1);
+        on(n, er.e * v, er.de * v + er.e * dv * er.du);
+      } else {
+        on(n, er.e * v, T(0));
+      }
+    }
+  }
+}
+
+// Per-edge set-up of one chunk, ACE_GROUP / CH threads per edge (4 or 8;
+// lt = tpe·t + q): q = 0 the R-family transform/interval/envelope, q = 1 the
+// pair family's (both shared with the edge's other threads by shuffles),
+// harmonics split by azimuthal order m ≡ q (mod tpe), the R and pair
+// channels n ≡ q (mod tpe) (values, and derivatives when Grad); the pair
+// energy and Σ Wpair·dQ/dr are summed over the edge's threads.
 template <int L, class T, bool Grad>
 __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbase, const AceLayout& lay,
                                                 const EdgeScalars<T>& es, const double4* __restrict__ edge_d, int e0,
                                                 int nc, int iz, int lt, double& e_acc, int* status,
                                                 const double* wq = nullptr) {
-  // ACE_GROUP / CH threads per edge: 4 for chunks of 16 edges, 8 for chunks of 8
   const int tpe = ACE_GROUP / lay.CH, tsh = 31 - __clz(tpe);
   const int t = lt >> tsh, q = lt & (tpe - 1);
   if (t >= nc) return;
@@ -172,7 +211,8 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   const T dx = (T)d.x, dy = (T)d.y, dz = (T)d.z;
   const T r0 = sqrt(dx * dx + dy * dy + dz * dz);
   const T r = r0 > T(0) ? r0 : T(1);
-  EdgeRadial<T> er{};
+  const bool pair = p.nQ > 0 && p.pair_ok[zj];  // the same for all of the edge's threads
+  EdgeRadial<T> er{}, eq{};
   if (q == 0) {
     if (!(r0 > T(0))) atomicOr(status, 2);
     es.r[t] = r;
@@ -186,27 +226,61 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
     es.e[t] = er.e;
     es.de[t] = er.de;
     es.du[t] = er.du;
-  } else if (q == 1) {
+  } else if (q == 1 && pair) {
+    eq = edge_radial<T>(p.Q, pidx, r);
+    if (!eq.ok) atomicOr(status, 2);
+  }
+  // the radial set-ups from the edge's first two threads (the tpe threads of
+  // an edge are consecutive lanes of one warp, all inside or all outside nc)
+  const int lane = lt & 31;
+  const int src = lane & ~(tpe - 1);
+  const unsigned seg = ((1u << tpe) - 1u) << src;
+  er.k0 = __shfl_sync(seg, er.k0, src);
+  er.u = __shfl_sync(seg, er.u, src);
+  er.e = __shfl_sync(seg, er.e, src);
+  if constexpr (Grad) {
+    er.de = __shfl_sync(seg, er.de, src);
+    er.du = __shfl_sync(seg, er.du, src);
+  }
+  double* Rt = gbase + lay.R + t * lay.RS;
+  double* dRt = gbase + lay.dR + t * lay.RS;
+  edge_channels<T, Grad, 1>(p.R, pidx, er, q, tpe, [&](int n, T v, T dv) {
+    Rt[n] = v;
+    if constexpr (Grad) dRt[n] = dv;
+  });
+  if (p.nQ > 0) {
+    double* qv = (!Grad && lay.feat) ? gbase + lay.QV + t * p.nQ : nullptr;
     double qe = 0.0;
     T qd = T(0);
-    double* qv = (!Grad && lay.feat) ? gbase + lay.QV + t * p.nQ : nullptr;
-    if (p.nQ > 0 && p.pair_ok[zj]) {
-      const EdgeRadial<T> eq = edge_radial<T>(p.Q, pidx, r);
-      if (!eq.ok) atomicOr(status, 2);
-      const double* wp = wq ? wq : p.wpair + (size_t)iz * p.nQ;
-      for (int n = 0; n < p.nQ; ++n) {
-        T v, dv;
-        channel_ed<T>(channel_coeff(p.Q, pidx, eq.k0, n), eq, v, dv);
-        qe += (double)v * wp[n];
-        qd += (T)wp[n] * dv;
-        if (qv) qv[n] = v;
+    if (pair) {
+      eq.k0 = __shfl_sync(seg, eq.k0, src + 1);
+      eq.u = __shfl_sync(seg, eq.u, src + 1);
+      eq.e = __shfl_sync(seg, eq.e, src + 1);
+      if constexpr (Grad) {
+        eq.de = __shfl_sync(seg, eq.de, src + 1);
+        eq.du = __shfl_sync(seg, eq.du, src + 1);
       }
+      const double* wp = wq ? wq : p.wpair + (size_t)iz * p.nQ;
+      edge_channels<T, Grad, 1>(p.Q, pidx, eq, q, tpe, [&](int n, T v, T dv) {
+        qe += (double)v * wp[n];
+        if constexpr (Grad) qd += (T)wp[n] * dv;
+        if (qv) qv[n] = v;
+      });
     } else if (qv) {
-      for (int n = 0; n < p.nQ; ++n) qv[n] = 0.0;
+      for (int n = q; n < p.nQ; n += tpe) qv[n] = 0.0;
     }
-    if (!Grad) e_acc += qe;
-    es.dq[t] = qd;
+    for (int o = 1; o < tpe; o <<= 1) {
+      qe += __shfl_xor_sync(seg, qe, o);
+      qd += __shfl_xor_sync(seg, qd, o);
+    }
+    if (q == 0) {
+      if (!Grad) e_acc += qe;
+      es.dq[t] = qd;
+    }
+  } else if (q == 0) {
+    es.dq[t] = T(0);
   }
+  // harmonics last: the radial set-ups are dead by now
   double* Yt = gbase + lay.Y + t * lay.YS;
   double* dYt = gbase + lay.dY + t * lay.YS * 3;
 #pragma unroll
@@ -223,32 +297,6 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
           }
         },
         p.solid != 0);
-  }
-  // the edge's radial set-up from its first thread (the tpe threads of an
-  // edge are consecutive lanes of one warp, all inside or all outside nc)
-  const int lane = lt & 31;
-  const int src = lane & ~(tpe - 1);
-  const unsigned quad = ((1u << tpe) - 1u) << src;
-  er.k0 = __shfl_sync(quad, er.k0, src);
-  er.u = __shfl_sync(quad, er.u, src);
-  er.e = __shfl_sync(quad, er.e, src);
-  if constexpr (Grad) {
-    er.de = __shfl_sync(quad, er.de, src);
-    er.du = __shfl_sync(quad, er.du, src);
-  }
-  double* Rt = gbase + lay.R + t * lay.RS;
-  double* dRt = gbase + lay.dR + t * lay.RS;
-  for (int n = q; n < p.nR; n += tpe) {
-    const double* c = channel_coeff(p.R, pidx, er.k0, n);
-    if constexpr (Grad) {
-      T v, dv;
-      channel_ed<T>(c, er, v, dv);
-      Rt[n] = v;
-      dRt[n] = dv;
-    } else {
-      const T u = er.u;
-      Rt[n] = er.e * ((((T)c[3] * u + (T)c[2]) * u + (T)c[1]) * u + (T)c[0]);
-    }
   }
 }
 
