@@ -50,13 +50,33 @@ struct EdgeRadial {
   bool ok;   // false: singular envelope at r = 0
 };
 
+// Per-pair parameters staged as 16 doubles: transform[6], p, q, envelope
+// kind, envelope[5] (RADP_W; see stage_radial_params).
+constexpr int RADP_W = 16;
+
+// sp: the staged parameters of the family (shared memory), or null to read
+// them from the family's global tables.
 template <class T>
-__device__ __forceinline__ EdgeRadial<T> edge_radial(const RadialDev& f, int pidx, T r) {
+__device__ __forceinline__ EdgeRadial<T> edge_radial(const RadialDev& f, int pidx, T r, const double* sp = nullptr) {
   EdgeRadial<T> o;
   o.ok = true;
-  const double* t = f.transform + 6 * pidx;
+  const double* t;
+  const double* ep;
+  int p, q, kind;
+  if (sp) {
+    t = sp + RADP_W * pidx;
+    p = (int)t[6];
+    q = (int)t[7];
+    kind = (int)t[8];
+    ep = t + 9;
+  } else {
+    t = f.transform + 6 * pidx;
+    p = f.powers[2 * pidx];
+    q = f.powers[2 * pidx + 1];
+    kind = f.env_kind[pidx];
+    ep = f.env + 5 * pidx;
+  }
   const T a = (T)t[0], rin = (T)t[1], r0 = (T)t[2], yin = (T)t[3], ycut = (T)t[4];
-  const int p = f.powers[2 * pidx], q = f.powers[2 * pidx + 1];
   const T s = (r - rin) / (r0 - rin);
   const int h = q - p;
   T y = r <= rin ? T(1) : T(1) / (T(1) + a * ipow(s, q) / (T(1) + ipow(s, h)));
@@ -72,8 +92,6 @@ __device__ __forceinline__ EdgeRadial<T> edge_radial(const RadialDev& f, int pid
     const T w = T(1) + a * uu;
     dx = T(-2) * a * dd / ((w * w) * (ycut - yin));
   }
-  const double* ep = f.env + 5 * pidx;
-  const int kind = f.env_kind[pidx];
   if (kind == 1) {  // PolyEnvelope2sX
     const T x1 = (T)ep[0], x2 = (T)ep[1], sc = (T)ep[4];
     const int p1 = (int)ep[2], p2 = (int)ep[3];
@@ -127,6 +145,20 @@ __device__ __forceinline__ EdgeRadial<T> edge_radial(const RadialDev& f, int pid
   o.u = (x - (T)nd[k - 1]) / step;
   o.du = dx / step;
   return o;
+}
+
+// The per-pair parameters of a family in the RADP_W layout (block-strided copy).
+__device__ __forceinline__ void stage_radial_params(const RadialDev& f, double* out, int tid, int nthreads) {
+  const int np = f.nz * f.nz;
+  for (int k = tid; k < np * RADP_W; k += nthreads) {
+    const int pidx = k / RADP_W, j = k - pidx * RADP_W;
+    double v = 0.0;
+    if (j < 6) v = f.transform[6 * pidx + j];
+    else if (j < 8) v = (double)f.powers[2 * pidx + (j - 6)];
+    else if (j == 8) v = (double)f.env_kind[pidx];
+    else if (j < 14) v = f.env[5 * pidx + (j - 9)];
+    out[k] = v;
+  }
 }
 
 // Channel n value and d/dr from the interval coefficients c[0..3].

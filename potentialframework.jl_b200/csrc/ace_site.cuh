@@ -92,7 +92,7 @@ struct AceLayout {
   int sur;     // surrogate pass: 1 features, 2 pullback with per-site weights
   int gtab;    // tables read from global memory (L1-cached) instead of staged:
                // bit 0 the adjoint terms, bit 1 the products (large models)
-  size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, tables_end;
+  size_t prods, terms, term_off, density, dn_off, dn, dm_off, dm, radp, tables_end;
   size_t group_bytes, total;
   // group-relative double offsets
   int A, dA, Y, dY, R, dR, T1, T2, esc, F, QV, WK, WQ, DD, QD, ints;
@@ -114,6 +114,7 @@ struct AceLayout {
     dn = o; o = align16(o + sizeof(int2) * t.D);
     dm_off = o; o = align16(o + sizeof(int) * (t.nY + 1));
     dm = o; o = align16(o + sizeof(int2) * t.D);
+    radp = o; o = align16(o + sizeof(double) * 2 * RADP_W * t.nz * t.nz);  // R and pair parameters
     tables_end = o;
     RS = t.nR | 1;
     YS = t.nY | 1;
@@ -201,7 +202,7 @@ template <int L, class T, bool Grad>
 __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbase, const AceLayout& lay,
                                                 const EdgeScalars<T>& es, const double4* __restrict__ edge_d, int e0,
                                                 int nc, int iz, int lt, double& e_acc, int* status,
-                                                const double* wq = nullptr) {
+                                                const double* wq = nullptr, const double* radp = nullptr) {
   const int tpe = ACE_GROUP / lay.CH, tsh = 31 - __clz(tpe);
   const int t = lt >> tsh, q = lt & (tpe - 1);
   if (t >= nc) return;
@@ -219,7 +220,7 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
     es.dx[t] = dx;
     es.dy[t] = dy;
     es.dz[t] = dz;
-    er = edge_radial<T>(p.R, pidx, r);
+    er = edge_radial<T>(p.R, pidx, r, radp);
     es.k0[t] = er.k0;
     es.pidx[t] = pidx;
     es.u[t] = er.u;
@@ -227,7 +228,7 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
     es.de[t] = er.de;
     es.du[t] = er.du;
   } else if (q == 1 && pair) {
-    eq = edge_radial<T>(p.Q, pidx, r);
+    eq = edge_radial<T>(p.Q, pidx, r, radp ? radp + RADP_W * p.nz * p.nz : nullptr);
     if (!eq.ok) atomicOr(status, 2);
   }
   // the radial set-ups from the edge's first two threads (the tpe threads of
@@ -331,6 +332,9 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
   }
   for (int k = threadIdx.x; k <= p.nR; k += blockDim.x) s_dnoff[k] = p.dn_off[k];
   for (int k = threadIdx.x; k <= p.nY; k += blockDim.x) s_dmoff[k] = p.dm_off[k];
+  double* s_radp = reinterpret_cast<double*>(smem + lay.radp);
+  stage_radial_params(p.R, s_radp, threadIdx.x, blockDim.x);
+  if (p.nQ > 0) stage_radial_params(p.Q, s_radp + RADP_W * p.nz * p.nz, threadIdx.x, blockDim.x);
   __syncthreads();
 
   const int g = threadIdx.x / ACE_GROUP, lt = threadIdx.x % ACE_GROUP;
@@ -383,7 +387,7 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
     for (int c0 = 0; c0 < (SUR == 2 ? 0 : E); c0 += CH) {
       const int nc = min(CH, E - c0);
       group_sync(g);
-      ace_chunk_edges<L, T, false>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, e_acc, status);
+      ace_chunk_edges<L, T, false>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, e_acc, status, nullptr, s_radp);
       group_sync(g);
       if (lay.feat)  // Σ_j Q[j,n] of the centre's species block (fitting.jl:29)
         for (int n = lt; n < p.nQ; n += ACE_GROUP) {
@@ -465,7 +469,7 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         const int nc = min(CH, E - c0);
         group_sync(g);
         double dummy = 0.0;
-        ace_chunk_edges<L, T, true>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, dummy, status, wq);
+        ace_chunk_edges<L, T, true>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, dummy, status, wq, s_radp);
         group_sync(g);
         for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
           const int t = idx / nR, n = idx - t * nR;
