@@ -898,9 +898,9 @@ void ace_batch_graph_sync(pfw_ws* ws) {
 static AceLayout choose_design_layout(const AceTables& p, int device) {
   int optin = 0;
   PFW_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-  const int cand[][2] = {{16, 4}, {8, 8}, {16, 2}, {8, 4}, {8, 2}, {8, 1}};
+  const int cand[][2] = {{16, 4}, {16, 2}, {8, 4}, {8, 2}, {8, 1}};
   for (auto& c : cand) {
-    if (c[0] > ACE_MAX_CHUNK || c[1] > ACE_MAX_GROUPS) continue;
+    if (c[0] > ACE_MAX_CHUNK || c[1] > ACE_DESIGN_MAX_GROUPS) continue;
     for (int gt : {1, 3}) {
       AceLayout lay;
       lay.make(p, c[0], c[1], 0, 0, gt, 1);

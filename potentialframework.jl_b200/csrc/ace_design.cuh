@@ -31,8 +31,10 @@
 
 namespace pfw {
 
+constexpr int ACE_DESIGN_MAX_GROUPS = 4;  // the ∂A tables leave room for at most 4 groups
+
 template <int L>
-__global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
+__global__ void __launch_bounds__(ACE_DESIGN_MAX_GROUPS * ACE_GROUP)
     k_ace_design(AceTables p, AceLayout lay, int nsys, const SysGeom* __restrict__ sysv, int cap,
                  const int* __restrict__ edge_off, const int* __restrict__ edge_j, const double4* __restrict__ edge_d,
                  const double4* __restrict__ pos, const int* __restrict__ perm, double4* __restrict__ gscratch,

@@ -114,7 +114,7 @@ struct AceLayout {
     dn = o; o = align16(o + sizeof(int2) * t.D);
     dm_off = o; o = align16(o + sizeof(int) * (t.nY + 1));
     dm = o; o = align16(o + sizeof(int2) * t.D);
-    radp = o; o = align16(o + sizeof(double) * 2 * RADP_W * t.nz * t.nz);  // R and pair parameters
+    radp = o; o = align16(o + (design ? 0 : sizeof(double) * 2 * RADP_W * t.nz * t.nz));  // R and pair parameters
     tables_end = o;
     RS = t.nR | 1;
     YS = t.nY | 1;
