@@ -138,3 +138,25 @@ def test_may30_rows_reproduce_predictions():
     # rows' scale (a dot product over 6,495 columns)
     pf = rows_of(float(fr["f0_energy"]), fr["f0_forces"], fr["f0_virial"])
     assert np.all(np.abs(pred - pf) <= RTOL * np.abs(pf).max())
+
+
+def test_open_cluster_columns_and_buffer_errors(tial):
+    m, d = tial
+    f = frame(d, 32)
+    cl = WL.System(f.X, f.H, (0, 0, 0), f.species)  # the same atoms as an open cluster
+    calc = api.ACECalculator(m)
+    A = FT.design_matrix(cl, calc)["matrix"]
+    rng = np.random.default_rng(11)
+    for c in rng.choice(A.shape[1], 24, replace=False):
+        ref = O.AceOracle(unit_model(m, int(c))).evaluate(cl.X, cl.H, cl.pbc, cl.species)
+        want = rows_of(ref["energy"], ref["forces"], ref["virial"])
+        assert np.all(np.abs(A[:, c] - want) <= RTOL * max(1.0, float(np.abs(want).max())))
+    h = lib.Handle(lib.FP64)
+    h.ace(m)
+    h.set_geometry(cl.X, cl.H, cl.pbc, cl.species)
+    rows, cols = h.design_shape()
+    small = np.zeros((rows - 1, cols))
+    with pytest.raises(lib.PFWError) as ei:
+        h.check(h.L.pfw_ace_design_matrix(h.ws, small.ctypes.data_as(lib.C.POINTER(lib.C.c_double)), cols,
+                                          rows - 1, None))
+    assert ei.value.code == lib.ESHAPE
