@@ -6,3 +6,4 @@ from .api import (ACECalculator, Energy, EnergyForcesVirial, EnergyOnly, Forces,
                   neighbour_list, neighbours, potential_energy, save_calculator, trainable_parameters, virial,
                   with_parameters)
 from .lib import ArgumentError, DimensionMismatch, DomainError, PFWError  # noqa: F401
+from .precision import compare_precision  # noqa: F401
