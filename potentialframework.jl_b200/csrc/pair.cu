@@ -49,11 +49,147 @@ __device__ __forceinline__ void write_cell_parts(double* cellpart, int cell, int
   }
 }
 
-// 5 resident 4-warp blocks per SM: 96 registers/thread and 5 × 42 KB of
-// candidate lists fit one SM; measured faster than register-limited 4.
+// 5 resident 4-warp blocks per SM: 96 registers/thread and 5 × 44.5 KB of
+// traversal state (56 list slots per lane) fit one SM; measured faster than 4
+// blocks with 64 or 48 slots, or 6 with 40.
 #ifndef PFW_PAIR_MINBLOCKS
 #define PFW_PAIR_MINBLOCKS 5
 #endif
+#ifndef PFW_PAIR_LIST_K
+#define PFW_PAIR_LIST_K 56
+#endif
+using PairStage = WarpStageK<PFW_PAIR_LIST_K>;
+
+// Flat drain of the lanes' lists: the warp treats them as ONE owner-major
+// sequence (lane 0's entries, then lane 1's, ...) and gives each lane a
+// contiguous 1/32 of it, so every lane evaluates the same number of entries
+// whatever the number of home atoms and the spread of the per-lane counts.
+// A lane accumulates the gradient of its current owner in registers and, when
+// the owner changes, stores that partial sum in slot (lane + owner) — unique,
+// because along the sequence either the lane or the owner grows.  Each owner
+// then adds the partials of the lanes its entries went to, in lane order: the
+// result is deterministic.  Energy and virial accumulate on the lane that
+// evaluated the entry (inside eval).
+template <class T>
+struct FlatScratch {
+  T part[63][3];  // partial gradient sums, slot lane + owner
+  int off[33];    // exclusive scan of the lanes' counts; off[32] = total
+};
+
+// eval(ph, ownh, pj, d, r2, gx, gy, gz): the pair at exact squared distance
+// r2 < c² of home atom ph (owning its E/W share when ownh) and neighbour pj;
+// it returns the gradient g (force on ph += g) and accumulates E and W.
+template <int MODE, class T, class Eval>
+__device__ __forceinline__ void flat_drain(const SysGeom& g, const double4* __restrict__ pos,
+                                           const PairStage& stage, FlatScratch<T>& fs, int lane, int i0,
+                                           unsigned ownmask, int& cnt, T f[3], Eval&& eval) {
+  constexpr unsigned FULL = 0xffffffffu;
+  __syncwarp();
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int off = incl - cnt;
+  const int total = __shfl_sync(FULL, incl, 31);
+  fs.off[lane] = off;
+  if (lane == 31) fs.off[32] = total;
+  __syncwarp();
+  const int R = (total + 31) >> 5;  // entries per lane
+  int q = lane * R;
+  const int qend = min(q + R, total);
+  if (q < qend) {
+    int h = 0;  // owner of q: last lane with off <= q
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1)
+      if (fs.off[h + st] <= q) h += st;
+    int hoff = fs.off[h], hend = fs.off[h + 1];
+    double4 ph = pos[i0 + h];
+    bool ownh = (ownmask >> h) & 1u;
+    T px = 0, py = 0, pz = 0;
+    for (; q < qend; ++q) {
+      if (q >= hend) {  // the next owner with entries
+        fs.part[lane + h][0] = px; fs.part[lane + h][1] = py; fs.part[lane + h][2] = pz;
+        px = py = pz = 0;
+        do {
+          ++h;
+        } while (fs.off[h + 1] <= q);
+        hoff = fs.off[h];
+        hend = fs.off[h + 1];
+        ph = pos[i0 + h];
+        ownh = (ownmask >> h) & 1u;
+      }
+      const unsigned item = stage.list[list_slot(q - hoff, h)];
+      const double4 pj = pos[item & 0xFFFFFFu];
+      const StencilEntry& se = stage.ent[item >> 24];
+      double d[3];
+      if (MODE == 0) {
+        d[0] = xadd(xsub(pj.x, ph.x), se.sh[0]);
+        d[1] = xadd(xsub(pj.y, ph.y), se.sh[1]);
+        d[2] = xadd(xsub(pj.z, ph.z), se.sh[2]);
+      } else {
+        displacement(g, se, ph.x, ph.y, ph.z, pj.x, pj.y, pj.z, d);
+      }
+      const double r2 = xr2(d[0], d[1], d[2]);
+      if (r2 < g.c2) {
+        T gx, gy, gz;
+        eval(ph, ownh, pj, d, r2, gx, gy, gz);
+        px += gx; py += gy; pz += gz;
+      }
+    }
+    fs.part[lane + h][0] = px; fs.part[lane + h][1] = py; fs.part[lane + h][2] = pz;
+  }
+  __syncwarp();
+  if (cnt > 0) {  // this lane's entries [off, off + cnt) went to lanes off / R .. (off + cnt - 1) / R
+    const int la = off / R, lb = (off + cnt - 1) / R;
+    for (int l = la; l <= lb; ++l) {
+      f[0] += fs.part[l + lane][0];
+      f[1] += fs.part[l + lane][1];
+      f[2] += fs.part[l + lane][2];
+    }
+  }
+  cnt = 0;
+  __syncwarp();
+}
+
+// One home cell of a pair kernel: the prefilter, the flat drains, and the
+// force of each home atom written once, in place, at the end of its chunk.
+template <int MODE, class T, class Eval>
+__device__ __forceinline__ void pair_cell(const SysGeom& g, int cell, const int* __restrict__ cell_start,
+                                          const double4* __restrict__ pos, const int* __restrict__ perm,
+                                          const PairParams& prm, PairStage& stage, FlatScratch<T>& fs, int lane,
+                                          double* __restrict__ F, Eval&& eval) {
+  T f[3] = {0, 0, 0};
+  unsigned ownmask = 0u;  // home atoms of the chunk that own their E/W shares
+  int cur = -1;
+  traverse_lists<MODE>(
+      g, cell, cell_start, pos, stage, lane,
+      [&](bool have, int i, const double4&, int& cnt) {
+        if (i != cur) {
+          cur = i;
+          ownmask = __ballot_sync(0xffffffffu, have && perm[i] < prm.n_owned);
+        }
+        flat_drain<MODE>(g, pos, stage, fs, lane, i - lane, ownmask, cnt, f, eval);
+      },
+      [&](bool have, int i, const double4&) {
+        if (have && prm.want_f) {
+          const int o = perm[i];
+          F[3 * o] = f[0]; F[3 * o + 1] = f[1]; F[3 * o + 2] = f[2];
+        }
+        f[0] = f[1] = f[2] = 0;
+      });
+}
+
+__device__ __forceinline__ void load_amplitudes(const PairParams& prm, int kind, double* sA) {
+  if (threadIdx.x < 16) {
+    const int a = threadIdx.x >> 2, b = threadIdx.x & 3;
+    sA[threadIdx.x] = (kind == 0 && a < prm.nz && b < prm.nz) ? prm.A[a * prm.nz + b] : 0.0;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ int species_index(double w) { return min(max((int)w, 0), 3); }
 
 // Plain FP64 path.  MODE 0: displacement = (x_j - x_i) + cell shift;
 // MODE 1: per-pair minimum image (small boxes).
@@ -62,52 +198,31 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
     k_pair64(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
              const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
              double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
-  __shared__ WarpStage stage[PAIR_WARPS];
+  __shared__ PairStage stage[PAIR_WARPS];
+  __shared__ FlatScratch<double> scratch[PAIR_WARPS];
+  __shared__ double sA[16];  // SmoothPair amplitudes A[zi][zj], 4 × 4, zero-padded
+  load_amplitudes(prm, KIND, sA);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * PAIR_WARPS + warp;
   if (cell >= ncells) return;
   const SysGeom& g = sysv[cell_sys[cell]];
-  double acc_e = 0, w[6] = {0, 0, 0, 0, 0, 0};
+  double e = 0, w[6] = {0, 0, 0, 0, 0, 0};
   unsigned long long np = 0;
-  int cur = -1;
-  bool own = true;
-  double fx = 0, fy = 0, fz = 0;
-  double arow[4] = {0, 0, 0, 0};
-  const bool want_f = prm.want_f;
-  warp_traverse_cell<MODE>(
-      g, cell, cell_start, pos, stage[warp], lane,
-      [&](int i, int, const double4& pi, const double4& pj, const StencilEntry&, const double* d, double r2) {
-        if (i != cur) {
-          if (cur >= 0 && want_f) {
-            const int o = perm[cur];
-            F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
-          }
-          cur = i;
-          own = perm[i] < prm.n_owned;
-          fx = fy = fz = 0;
-          if (KIND == 0) {
-            const int zi = min(max((int)pi.w, 0), prm.nz - 1);
-#pragma unroll
-            for (int z = 0; z < 4; ++z) arow[z] = z < prm.nz ? prm.A[zi * prm.nz + z] : 0.0;
-          }
-        }
+  pair_cell<MODE, double>(
+      g, cell, cell_start, pos, perm, prm, stage[warp], scratch[warp], lane, F,
+      [&](const double4& ph, bool ownh, const double4& pj, const double* d, double r2, double& gx, double& gy,
+          double& gz) {
         ++np;
         double en, coef;
-        const int zj = (int)pj.w;
-        pair_term<KIND>(prm, zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3], r2, en, coef);
-        const double gx = coef * d[0], gy = coef * d[1], gz = coef * d[2];
-        fx += gx; fy += gy; fz += gz;
-        if (own) {
-          acc_e += en;
+        pair_term<KIND>(prm, KIND == 0 ? sA[species_index(ph.w) * 4 + species_index(pj.w)] : 0.0, r2, en, coef);
+        gx = coef * d[0]; gy = coef * d[1]; gz = coef * d[2];
+        if (ownh) {
+          e += en;
           w[0] += d[0] * gx; w[1] += d[1] * gy; w[2] += d[2] * gz;
           w[3] += d[0] * gy; w[4] += d[0] * gz; w[5] += d[1] * gz;
         }
       });
-  if (cur >= 0 && want_f) {
-    const int o = perm[cur];
-    F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
-  }
-  write_cell_parts(cellpart, cell, lane, acc_e, w, np, npairs);
+  write_cell_parts(cellpart, cell, lane, e, w, np, npairs);
 }
 
 // Mixed form: the same traversal and the same FP64 cutoff decision as the
@@ -127,7 +242,10 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
     k_pair32(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
              const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
              double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
-  __shared__ WarpStage stage[PAIR_WARPS];
+  __shared__ PairStage stage[PAIR_WARPS];
+  __shared__ FlatScratch<float> scratch[PAIR_WARPS];
+  __shared__ double sA[16];
+  load_amplitudes(prm, KIND, sA);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * PAIR_WARPS + warp;
   if (cell >= ncells) return;
@@ -136,11 +254,6 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
   float ce = 0.f, cw[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   int cn = 0;
   unsigned long long np = 0;
-  int cur = -1;
-  bool own = true;
-  float fx = 0.f, fy = 0.f, fz = 0.f;
-  float arow[4] = {0.f, 0.f, 0.f, 0.f};
-  const bool want_f = prm.want_f;
   const float invc2 = (float)prm.invc2, eps4 = (float)prm.eps4, eps24 = (float)prm.eps24,
               sigma2 = (float)prm.sigma2, shift = (float)prm.shift;
   auto fold = [&]() {
@@ -153,30 +266,16 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
     ce = 0.f;
     cn = 0;
   };
-  warp_traverse_cell<MODE>(
-      g, cell, cell_start, pos, stage[warp], lane,
-      [&](int i, int, const double4& pi, const double4& pj, const StencilEntry&, const double* d, double r2d) {
-        if (i != cur) {
-          if (cur >= 0 && want_f) {
-            const int o = perm[cur];
-            F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
-          }
-          cur = i;
-          own = perm[i] < prm.n_owned;
-          fx = fy = fz = 0.f;
-          if (KIND == 0) {
-            const int zi = min(max((int)pi.w, 0), prm.nz - 1);
-#pragma unroll
-            for (int z = 0; z < 4; ++z) arow[z] = z < prm.nz ? (float)prm.A[zi * prm.nz + z] : 0.f;
-          }
-        }
+  pair_cell<MODE, float>(
+      g, cell, cell_start, pos, perm, prm, stage[warp], scratch[warp], lane, F,
+      [&](const double4& ph, bool ownh, const double4& pj, const double* d, double r2d, float& gx, float& gy,
+          float& gz) {
         ++np;
         const float d0 = (float)d[0], d1 = (float)d[1], d2 = (float)d[2];
         const float r2 = (float)r2d;
         float en, coef;
         if (KIND == 0) {
-          const int zj = (int)pj.w;
-          const float a = zj == 0 ? arow[0] : zj == 1 ? arow[1] : zj == 2 ? arow[2] : arow[3];
+          const float a = (float)sA[species_index(ph.w) * 4 + species_index(pj.w)];
           const float q = 1.f - r2 * invc2;
           const float aq2 = a * q * q;
           en = aq2 * q;
@@ -188,19 +287,14 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
           en = eps4 * (s6 * s6 - s6) - shift;
           coef = eps24 * (s6 - 2.f * s6 * s6) * ir2;
         }
-        const float gx = coef * d0, gy = coef * d1, gz = coef * d2;
-        fx += gx; fy += gy; fz += gz;
-        if (own) {
+        gx = coef * d0; gy = coef * d1; gz = coef * d2;
+        if (ownh) {
           ce += en;
           cw[0] += d0 * gx; cw[1] += d1 * gy; cw[2] += d2 * gz;
           cw[3] += d0 * gy; cw[4] += d0 * gz; cw[5] += d1 * gz;
           if (++cn == MIXED_CHUNK) fold();
         }
       });
-  if (cur >= 0 && want_f) {
-    const int o = perm[cur];
-    F[3 * o] = fx; F[3 * o + 1] = fy; F[3 * o + 2] = fz;
-  }
   fold();
   double w[6];
 #pragma unroll

@@ -12,6 +12,12 @@
 // re-tests with the exact reference arithmetic
 // (NeighbourList/geometry.jl:5-19) and calls visit for pairs with r² < c².
 //
+// Pair kernels drain the lists differently (traverse_lists below takes the
+// drain as a callable): the warp walks all lanes' lists as one sequence.  For
+// that the list is stored with the lane index xor-ed with the slot, so that
+// 32 consecutive slots of ONE lane sit in 32 distinct banks, while one slot
+// of all lanes still does.
+//
 // The FP32 test can only reject pairs whose exact r² exceeds c²: with
 // coordinates relative to a point at most R away, |r²₃₂ - r²| ≤ c²·(4e-7·R/c
 // + 2e-7), far inside the 2⁻¹⁰ guard for any R < 1000 c.  The visited set is
@@ -35,19 +41,25 @@ constexpr float PREFILTER_GUARD = 1.0f + 1.0f / 1024.0f;
 #define PFW_DRAIN_UNROLL 1
 #endif
 
-struct WarpStage {
+// Per-warp traversal state; K is the list capacity per lane (> TRAVERSE_STAGE).
+template <int K>
+struct WarpStageK {
+  static constexpr int capacity = K;
   float2 x2[TRAVERSE_STAGE / 2], y2[TRAVERSE_STAGE / 2], z2[TRAVERSE_STAGE / 2];
   int sj[TRAVERSE_STAGE];           // staged atom: sorted index
   int sk[TRAVERSE_STAGE];           // staged atom: stencil entry slot
   int start[LIST_NE + 1];           // flat-list offsets of the entries
   StencilEntry ent[LIST_NE];
-  unsigned int list[LIST_K][32];    // [slot][lane]: j | entry << 24
+  unsigned int list[K * 32];        // list_slot(slot, lane): j | entry << 24
 };
+using WarpStage = WarpStageK<LIST_K>;
+
+__device__ __forceinline__ int list_slot(int slot, int lane) { return slot * 32 + (lane ^ (slot & 31)); }
 
 // Walk the lane's list: PFW_DRAIN_UNROLL neighbour loads are issued before
 // any of them is used, so their latencies overlap.
-template <int MODE, class Visit>
-__device__ __forceinline__ void drain_lists(const SysGeom& g, const double4* __restrict__ pos, WarpStage& stage,
+template <int MODE, class Stage, class Visit>
+__device__ __forceinline__ void drain_lists(const SysGeom& g, const double4* __restrict__ pos, Stage& stage,
                                             int lane, bool have, int i, const double4& pi, int& cnt, Visit& visit) {
   constexpr int U = PFW_DRAIN_UNROLL;
   __syncwarp();
@@ -57,7 +69,7 @@ __device__ __forceinline__ void drain_lists(const SysGeom& g, const double4* __r
       double4 pj[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        item[u] = stage.list[min(q0 + u, cnt - 1)][lane];
+        item[u] = stage.list[list_slot(min(q0 + u, cnt - 1), lane)];
         pj[u] = pos[item[u] & 0xFFFFFFu];
       }
 #pragma unroll
@@ -82,10 +94,13 @@ __device__ __forceinline__ void drain_lists(const SysGeom& g, const double4* __r
   __syncwarp();
 }
 
-template <int MODE, class Visit>
-__device__ __forceinline__ void warp_traverse_cell(const SysGeom& g, int cell, const int* __restrict__ cell_start,
-                                                   const double4* __restrict__ pos, WarpStage& stage, int lane,
-                                                   Visit&& visit) {
+// The prefilter of one home cell.  drain(have, i, pi, cnt) consumes the
+// lanes' lists (and sets cnt to 0); chunk_end(have, i, pi) runs after each
+// chunk of 32 home atoms.
+template <int MODE, class Stage, class Drain, class ChunkEnd>
+__device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const int* __restrict__ cell_start,
+                                               const double4* __restrict__ pos, Stage& stage, int lane,
+                                               Drain&& drain, ChunkEnd&& chunk_end) {
   const int b = cell_start[cell], e = cell_start[cell + 1];
   if (b == e) return;
   const int local = cell - g.cell_begin;
@@ -192,15 +207,29 @@ __device__ __forceinline__ void warp_traverse_cell(const SysGeom& g, int cell, c
           mask &= mask - 1u;
           const int j = stage.sj[t], k = stage.sk[t];
           if (j == i && stage.ent[k].zero) continue;  // the zero-shift self pair
-          stage.list[cnt++][lane] = (unsigned)j | ((unsigned)k << 24);
+          stage.list[list_slot(cnt++, lane)] = (unsigned)j | ((unsigned)k << 24);
         }
-        if (__reduce_max_sync(0xffffffffu, cnt) > LIST_K - TRAVERSE_STAGE)
-          drain_lists<MODE>(g, pos, stage, lane, have, i, pi, cnt, visit);
+        if (__reduce_max_sync(0xffffffffu, cnt) > Stage::capacity - TRAVERSE_STAGE) drain(have, i, pi, cnt);
       }
       // entries are reused by the next block: drain what refers to them
-      drain_lists<MODE>(g, pos, stage, lane, have, i, pi, cnt, visit);
+      drain(have, i, pi, cnt);
     }
+    chunk_end(have, i, pi);
   }
+}
+
+// Every directed neighbour of the home cell's atoms, visited on the lane that
+// owns the centre: visit(i, j, pi, pj, se, d, r2).
+template <int MODE, class Visit>
+__device__ __forceinline__ void warp_traverse_cell(const SysGeom& g, int cell, const int* __restrict__ cell_start,
+                                                   const double4* __restrict__ pos, WarpStage& stage, int lane,
+                                                   Visit&& visit) {
+  traverse_lists<MODE>(
+      g, cell, cell_start, pos, stage, lane,
+      [&](bool have, int i, const double4& pi, int& cnt) {
+        drain_lists<MODE>(g, pos, stage, lane, have, i, pi, cnt, visit);
+      },
+      [](bool, int, const double4&) {});
 }
 
 // Integer image of the directed pair i→j relative to the ORIGINAL
