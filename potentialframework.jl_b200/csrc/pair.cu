@@ -49,16 +49,17 @@ __device__ __forceinline__ void write_cell_parts(double* cellpart, int cell, int
   }
 }
 
-// 5 resident 4-warp blocks per SM: 96 registers/thread and 5 × 44.5 KB of
-// traversal state (56 list slots per lane) fit one SM; measured faster than 4
-// blocks with 64 or 48 slots, or 6 with 40.
+// 5 resident 4-warp blocks per SM: 96 registers/thread and 5 × 44 KB of
+// traversal state (52 list slots per lane, the 64-slot pruned staging ring)
+// fit one SM; 5 blocks measured faster than 4 with longer lists or 6 with
+// shorter ones.
 #ifndef PFW_PAIR_MINBLOCKS
 #define PFW_PAIR_MINBLOCKS 5
 #endif
 #ifndef PFW_PAIR_LIST_K
-#define PFW_PAIR_LIST_K 56
+#define PFW_PAIR_LIST_K 52
 #endif
-using PairStage = WarpStageK<PFW_PAIR_LIST_K>;
+using PairStage = WarpStageK<PFW_PAIR_LIST_K, 2 * TRAVERSE_STAGE>;
 
 // Flat drain of the lanes' lists: the warp treats them as ONE owner-major
 // sequence (lane 0's entries, then lane 1's, ...) and gives each lane a
@@ -76,9 +77,24 @@ struct FlatScratch {
   int off[33];    // exclusive scan of the lanes' counts; off[32] = total
 };
 
-// eval(ph, ownh, pj, d, r2, gx, gy, gz): the pair at exact squared distance
-// r2 < c² of home atom ph (owning its E/W share when ownh) and neighbour pj;
-// it returns the gradient g (force on ph += g) and accumulates E and W.
+// eval(ph, ownh, pj, d, r2, hit, gx, gy, gz): the pair of home atom ph
+// (owning its E/W share when ownh) and neighbour pj at exact squared distance
+// r2; it returns the gradient g (force on ph += g), zero unless hit (r2 < c²),
+// and accumulates E and W of hits.  It is evaluated without branches, so two
+// entries of one owner run as independent instruction streams.
+template <int MODE>
+__device__ __forceinline__ double entry_geometry(const SysGeom& g, const StencilEntry& se, const double4& ph,
+                                                 const double4& pj, double d[3]) {
+  if (MODE == 0) {
+    d[0] = xadd(xsub(pj.x, ph.x), se.sh[0]);
+    d[1] = xadd(xsub(pj.y, ph.y), se.sh[1]);
+    d[2] = xadd(xsub(pj.z, ph.z), se.sh[2]);
+  } else {
+    displacement(g, se, ph.x, ph.y, ph.z, pj.x, pj.y, pj.z, d);
+  }
+  return xr2(d[0], d[1], d[2]);
+}
+
 template <int MODE, class T, class Eval>
 __device__ __forceinline__ void flat_drain(const SysGeom& g, const double4* __restrict__ pos,
                                            const PairStage& stage, FlatScratch<T>& fs, int lane, int i0,
@@ -108,7 +124,7 @@ __device__ __forceinline__ void flat_drain(const SysGeom& g, const double4* __re
     double4 ph = pos[i0 + h];
     bool ownh = (ownmask >> h) & 1u;
     T px = 0, py = 0, pz = 0;
-    for (; q < qend; ++q) {
+    while (q < qend) {
       if (q >= hend) {  // the next owner with entries
         fs.part[lane + h][0] = px; fs.part[lane + h][1] = py; fs.part[lane + h][2] = pz;
         px = py = pz = 0;
@@ -120,23 +136,20 @@ __device__ __forceinline__ void flat_drain(const SysGeom& g, const double4* __re
         ph = pos[i0 + h];
         ownh = (ownmask >> h) & 1u;
       }
-      const unsigned item = stage.list[list_slot(q - hoff, h)];
-      const double4 pj = pos[item & 0xFFFFFFu];
-      const StencilEntry& se = stage.ent[item >> 24];
-      double d[3];
-      if (MODE == 0) {
-        d[0] = xadd(xsub(pj.x, ph.x), se.sh[0]);
-        d[1] = xadd(xsub(pj.y, ph.y), se.sh[1]);
-        d[2] = xadd(xsub(pj.z, ph.z), se.sh[2]);
-      } else {
-        displacement(g, se, ph.x, ph.y, ph.z, pj.x, pj.y, pj.z, d);
-      }
-      const double r2 = xr2(d[0], d[1], d[2]);
-      if (r2 < g.c2) {
-        T gx, gy, gz;
-        eval(ph, ownh, pj, d, r2, gx, gy, gz);
-        px += gx; py += gy; pz += gz;
-      }
+      // entries q and q + 1 when both are this owner's (else q twice, the copy masked)
+      const bool two = q + 1 < min(qend, hend);
+      const unsigned ia = stage.list[list_slot(q - hoff, h)];
+      const unsigned ib = stage.list[list_slot(q - hoff + (two ? 1 : 0), h)];
+      const double4 pa = pos[ia & 0xFFFFFFu], pb = pos[ib & 0xFFFFFFu];
+      double da[3], db[3];
+      const double r2a = entry_geometry<MODE>(g, stage.ent[ia >> 24], ph, pa, da);
+      const double r2b = entry_geometry<MODE>(g, stage.ent[ib >> 24], ph, pb, db);
+      T ax, ay, az, bx, by, bz;
+      eval(ph, ownh, pa, da, r2a, r2a < g.c2, ax, ay, az);
+      eval(ph, ownh, pb, db, r2b, two && r2b < g.c2, bx, by, bz);
+      px += ax; py += ay; pz += az;
+      px += bx; py += by; pz += bz;
+      q += two ? 2 : 1;
     }
     fs.part[lane + h][0] = px; fs.part[lane + h][1] = py; fs.part[lane + h][2] = pz;
   }
@@ -210,17 +223,17 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
   unsigned long long np = 0;
   pair_cell<MODE, double>(
       g, cell, cell_start, pos, perm, prm, stage[warp], scratch[warp], lane, F,
-      [&](const double4& ph, bool ownh, const double4& pj, const double* d, double r2, double& gx, double& gy,
-          double& gz) {
-        ++np;
+      [&](const double4& ph, bool ownh, const double4& pj, const double* d, double r2, bool hit, double& gx,
+          double& gy, double& gz) {
+        np += hit;
         double en, coef;
         pair_term<KIND>(prm, KIND == 0 ? sA[species_index(ph.w) * 4 + species_index(pj.w)] : 0.0, r2, en, coef);
+        coef = hit ? coef : 0.0;
         gx = coef * d[0]; gy = coef * d[1]; gz = coef * d[2];
-        if (ownh) {
-          e += en;
-          w[0] += d[0] * gx; w[1] += d[1] * gy; w[2] += d[2] * gz;
-          w[3] += d[0] * gy; w[4] += d[0] * gz; w[5] += d[1] * gz;
-        }
+        const double o = ownh ? 1.0 : 0.0;  // W terms of non-hits are zero already
+        e += (hit && ownh) ? en : 0.0;
+        w[0] += o * (d[0] * gx); w[1] += o * (d[1] * gy); w[2] += o * (d[2] * gz);
+        w[3] += o * (d[0] * gy); w[4] += o * (d[0] * gz); w[5] += o * (d[1] * gz);
       });
   write_cell_parts(cellpart, cell, lane, e, w, np, npairs);
 }
@@ -268,8 +281,12 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
   };
   pair_cell<MODE, float>(
       g, cell, cell_start, pos, perm, prm, stage[warp], scratch[warp], lane, F,
-      [&](const double4& ph, bool ownh, const double4& pj, const double* d, double r2d, float& gx, float& gy,
-          float& gz) {
+      [&](const double4& ph, bool ownh, const double4& pj, const double* d, double r2d, bool hit, float& gx,
+          float& gy, float& gz) {
+        if (!hit) {
+          gx = gy = gz = 0.f;
+          return;
+        }
         ++np;
         const float d0 = (float)d[0], d1 = (float)d[1], d2 = (float)d[2];
         const float r2 = (float)r2d;

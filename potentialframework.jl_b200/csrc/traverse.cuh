@@ -21,7 +21,10 @@
 // The FP32 test can only reject pairs whose exact r² exceeds c²: with
 // coordinates relative to a point at most R away, |r²₃₂ - r²| ≤ c²·(4e-7·R/c
 // + 2e-7), far inside the 2⁻¹⁰ guard for any R < 1000 c.  The visited set is
-// therefore exactly the reference's, and visit(i, j, pi, pj, se, d, r2) runs
+// therefore exactly the reference's.  The box prune is as safe: the box
+// distance of the FP32 coordinates is at most their distance to any home
+// atom, so a staged atom within c of a home atom has a box distance below
+// c²·(1 + 2⁻¹⁰) by the same bound.  visit(i, j, pi, pj, se, d, r2) runs
 // on the lane owning sorted atom i in a fixed order (stencil entry, then the
 // neighbour cell's sorted order).
 #pragma once
@@ -42,12 +45,16 @@ constexpr float PREFILTER_GUARD = 1.0f + 1.0f / 1024.0f;
 #endif
 
 // Per-warp traversal state; K is the list capacity per lane (> TRAVERSE_STAGE).
-template <int K>
+// RING = 64 turns on the box prune (MODE 0): a staged atom farther than the
+// cutoff from the bounding box of the home atoms cannot be a neighbour of any
+// of them and is dropped before the per-lane test; the survivors are packed
+// into a ring of 64 slots so that each per-lane test still sees 32 of them.
+template <int K, int RING = TRAVERSE_STAGE>
 struct WarpStageK {
   static constexpr int capacity = K;
-  float2 x2[TRAVERSE_STAGE / 2], y2[TRAVERSE_STAGE / 2], z2[TRAVERSE_STAGE / 2];
-  int sj[TRAVERSE_STAGE];           // staged atom: sorted index
-  int sk[TRAVERSE_STAGE];           // staged atom: stencil entry slot
+  static constexpr int ring = RING;
+  float2 x2[RING / 2], y2[RING / 2], z2[RING / 2];
+  unsigned sitem[RING];             // staged atom: j | entry << 24
   int start[LIST_NE + 1];           // flat-list offsets of the entries
   StencilEntry ent[LIST_NE];
   unsigned int list[K * 32];        // list_slot(slot, lane): j | entry << 24
@@ -108,6 +115,8 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
   const int cnt0 = stencil_count(g, 0), cnt1 = stencil_count(g, 1), cnt2 = stencil_count(g, 2);
   const int nstencil = cnt0 * cnt1 * cnt2;
   const float c2hi = (float)g.c2 * PREFILTER_GUARD;
+  constexpr int RING = Stage::ring;
+  constexpr bool PRUNE = MODE == 0 && RING == 2 * TRAVERSE_STAGE;
   const double4 ref = pos[b];
   for (int i0 = b; i0 < e; i0 += 32) {
     const int i = i0 + lane;
@@ -116,6 +125,20 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
     const float2 nx = make_float2(-(float)(pi.x - ref.x), -(float)(pi.x - ref.x));
     const float2 ny = make_float2(-(float)(pi.y - ref.y), -(float)(pi.y - ref.y));
     const float2 nz = make_float2(-(float)(pi.z - ref.z), -(float)(pi.z - ref.z));
+    // bounding box of the home atoms' FP32 coordinates (lanes without an atom
+    // sit at ref, an atom of the home cell, so they only widen it)
+    float3 box_lo = make_float3(-nx.x, -ny.x, -nz.x), box_hi = box_lo;
+    if (PRUNE) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        box_lo.x = fminf(box_lo.x, __shfl_xor_sync(0xffffffffu, box_lo.x, o));
+        box_lo.y = fminf(box_lo.y, __shfl_xor_sync(0xffffffffu, box_lo.y, o));
+        box_lo.z = fminf(box_lo.z, __shfl_xor_sync(0xffffffffu, box_lo.z, o));
+        box_hi.x = fmaxf(box_hi.x, __shfl_xor_sync(0xffffffffu, box_hi.x, o));
+        box_hi.y = fmaxf(box_hi.y, __shfl_xor_sync(0xffffffffu, box_hi.y, o));
+        box_hi.z = fmaxf(box_hi.z, __shfl_xor_sync(0xffffffffu, box_hi.z, o));
+      }
+    }
     int cnt = 0;
     for (int s0 = 0; s0 < nstencil; s0 += LIST_NE) {
       // ---- resolve up to 32 stencil entries, one per lane ----
@@ -148,12 +171,45 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
       const int jb_lane = jb;
       __syncwarp();
       // ---- stage the flat list 32 atoms at a time ----
+      // slots [rpos, wpos) of the ring hold staged atoms not yet tested;
+      // rpos is a multiple of 32 whenever a test starts.
+      int wpos = 0, rpos = 0;
+      auto test_window = [&](int n) {
+        const int base = rpos & (RING - 1);
+        unsigned mask;
+        if (MODE == 0) {
+          mask = 0u;
+          const float2 lim = make_float2(c2hi, c2hi);
+          const int npair = (n + 1) >> 1;
+#pragma unroll 4
+          for (int u = 0; u < npair; ++u) {
+            const float2 dx = __fadd2_rn(stage.x2[(base >> 1) + u], nx);
+            const float2 dy = __fadd2_rn(stage.y2[(base >> 1) + u], ny);
+            const float2 dz = __fadd2_rn(stage.z2[(base >> 1) + u], nz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            mask |= ((r2.x < lim.x ? 1u : 0u) | (r2.y < lim.y ? 2u : 0u)) << (2 * u);
+          }
+          if (n < 32) mask &= (1u << n) - 1u;
+        } else {
+          mask = n == 32 ? 0xffffffffu : ((1u << n) - 1u);
+        }
+        if (!have) mask = 0u;
+        while (mask) {
+          const int t = __ffs(mask) - 1;
+          mask &= mask - 1u;
+          const unsigned it = stage.sitem[base + t];
+          if ((int)(it & 0xFFFFFFu) == i && stage.ent[it >> 24].zero) continue;  // the zero-shift self pair
+          stage.list[list_slot(cnt++, lane)] = it;
+        }
+        rpos += n;
+        if (__reduce_max_sync(0xffffffffu, cnt) > Stage::capacity - TRAVERSE_STAGE) drain(have, i, pi, cnt);
+      };
       for (int f0 = 0; f0 < total; f0 += TRAVERSE_STAGE) {
         const int nj = min(TRAVERSE_STAGE, total - f0);
         __syncwarp();
         {
           float px = 1e30f, py = 1e30f, pz = 1e30f;
-          int jj = -1, kk = 0;
+          int jj = 0, kk = 0;
           if (lane < nj) {
             const int f = f0 + lane;
             int lo = 0, hi = 31;  // last entry with start <= f
@@ -166,7 +222,8 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
           }
           // atom index of the flat position: entry kk's first atom + offset
           const int jbk = __shfl_sync(0xffffffffu, jb_lane, kk);
-          if (lane < nj) {
+          bool keep = lane < nj;
+          if (keep) {
             jj = jbk + (f0 + lane - stage.start[kk]);
             if (MODE == 0) {
               const double4 q = pos[jj];
@@ -174,43 +231,30 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
               px = (float)((q.x + se.sh[0]) - ref.x);
               py = (float)((q.y + se.sh[1]) - ref.y);
               pz = (float)((q.z + se.sh[2]) - ref.z);
+              if (PRUNE) {
+                const float ex = fmaxf(fmaxf(box_lo.x - px, px - box_hi.x), 0.f);
+                const float ey = fmaxf(fmaxf(box_lo.y - py, py - box_hi.y), 0.f);
+                const float ez = fmaxf(fmaxf(box_lo.z - pz, pz - box_hi.z), 0.f);
+                keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < c2hi;
+              }
             }
           }
-          if (MODE == 0) {
-            reinterpret_cast<float*>(stage.x2)[lane] = px;
-            reinterpret_cast<float*>(stage.y2)[lane] = py;
-            reinterpret_cast<float*>(stage.z2)[lane] = pz;
+          const unsigned kb = __ballot_sync(0xffffffffu, keep);
+          if (keep) {
+            const int slot = (wpos + __popc(kb & ((1u << lane) - 1u))) & (RING - 1);
+            if (MODE == 0) {
+              reinterpret_cast<float*>(stage.x2)[slot] = px;
+              reinterpret_cast<float*>(stage.y2)[slot] = py;
+              reinterpret_cast<float*>(stage.z2)[slot] = pz;
+            }
+            stage.sitem[slot] = (unsigned)jj | ((unsigned)kk << 24);
           }
-          stage.sj[lane] = jj;
-          stage.sk[lane] = kk;
+          wpos += __popc(kb);
         }
         __syncwarp();
-        unsigned mask;
-        if (MODE == 0) {
-          mask = 0u;
-          const float2 lim = make_float2(c2hi, c2hi);
-          const int npair = (nj + 1) >> 1;
-#pragma unroll 4
-          for (int u = 0; u < npair; ++u) {
-            const float2 dx = __fadd2_rn(stage.x2[u], nx);
-            const float2 dy = __fadd2_rn(stage.y2[u], ny);
-            const float2 dz = __fadd2_rn(stage.z2[u], nz);
-            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-            mask |= ((r2.x < lim.x ? 1u : 0u) | (r2.y < lim.y ? 2u : 0u)) << (2 * u);
-          }
-        } else {
-          mask = nj == 32 ? 0xffffffffu : ((1u << nj) - 1u);
-        }
-        if (!have) mask = 0u;
-        while (mask) {
-          const int t = __ffs(mask) - 1;
-          mask &= mask - 1u;
-          const int j = stage.sj[t], k = stage.sk[t];
-          if (j == i && stage.ent[k].zero) continue;  // the zero-shift self pair
-          stage.list[list_slot(cnt++, lane)] = (unsigned)j | ((unsigned)k << 24);
-        }
-        if (__reduce_max_sync(0xffffffffu, cnt) > Stage::capacity - TRAVERSE_STAGE) drain(have, i, pi, cnt);
+        if (wpos - rpos >= TRAVERSE_STAGE) test_window(TRAVERSE_STAGE);
       }
+      if (wpos > rpos) test_window(wpos - rpos);
       // entries are reused by the next block: drain what refers to them
       drain(have, i, pi, cnt);
     }
