@@ -49,15 +49,16 @@ __device__ __forceinline__ void write_cell_parts(double* cellpart, int cell, int
   }
 }
 
-// 5 resident 4-warp blocks per SM: 96 registers/thread and 5 × 44 KB of
-// traversal state (52 list slots per lane, the 64-slot pruned staging ring)
-// fit one SM; 5 blocks measured faster than 4 with longer lists or 6 with
-// shorter ones.
+// 4 resident 4-warp blocks per SM: 128 registers/thread and 4 × 54 KB of
+// traversal state (72 list slots per lane, the 64-slot pruned staging ring,
+// the drain's partial sums) in dynamic shared memory.  Longer lists mean
+// fewer drains: 72 slots measured faster than 60-68, and than 5 blocks with
+// 40-56 slots.
 #ifndef PFW_PAIR_MINBLOCKS
-#define PFW_PAIR_MINBLOCKS 5
+#define PFW_PAIR_MINBLOCKS 4
 #endif
 #ifndef PFW_PAIR_LIST_K
-#define PFW_PAIR_LIST_K 52
+#define PFW_PAIR_LIST_K 72
 #endif
 using PairStage = WarpStageK<PFW_PAIR_LIST_K, 2 * TRAVERSE_STAGE>;
 
@@ -142,11 +143,17 @@ __device__ __forceinline__ void flat_drain(const SysGeom& g, const double4* __re
       const unsigned ib = stage.list[list_slot(q - hoff + (two ? 1 : 0), h)];
       const double4 pa = pos[ia & 0xFFFFFFu], pb = pos[ib & 0xFFFFFFu];
       double da[3], db[3];
-      const double r2a = entry_geometry<MODE>(g, stage.ent[ia >> 24], ph, pa, da);
-      const double r2b = entry_geometry<MODE>(g, stage.ent[ib >> 24], ph, pb, db);
+      const StencilEntry& ea = stage.ent[ia >> 24];
+      const StencilEntry& eb = stage.ent[ib >> 24];
+      const double r2a = entry_geometry<MODE>(g, ea, ph, pa, da);
+      const double r2b = entry_geometry<MODE>(g, eb, ph, pb, db);
+      // the zero-shift self pair is in the list (the prefilter does not see owners)
+      const int ih = i0 + h;
+      const bool hita = r2a < g.c2 && !((int)(ia & 0xFFFFFFu) == ih && ea.zero);
+      const bool hitb = two && r2b < g.c2 && !((int)(ib & 0xFFFFFFu) == ih && eb.zero);
       T ax, ay, az, bx, by, bz;
-      eval(ph, ownh, pa, da, r2a, r2a < g.c2, ax, ay, az);
-      eval(ph, ownh, pb, db, r2b, two && r2b < g.c2, bx, by, bz);
+      eval(ph, ownh, pa, da, r2a, hita, ax, ay, az);
+      eval(ph, ownh, pb, db, r2b, hitb, bx, by, bz);
       px += ax; py += ay; pz += az;
       px += bx; py += by; pz += bz;
       q += two ? 2 : 1;
@@ -211,8 +218,9 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
     k_pair64(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
              const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
              double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
-  __shared__ PairStage stage[PAIR_WARPS];
-  __shared__ FlatScratch<double> scratch[PAIR_WARPS];
+  extern __shared__ __align__(16) unsigned char pair_smem[];
+  PairStage* stage = reinterpret_cast<PairStage*>(pair_smem);
+  FlatScratch<double>* scratch = reinterpret_cast<FlatScratch<double>*>(pair_smem + sizeof(PairStage) * PAIR_WARPS);
   __shared__ double sA[16];  // SmoothPair amplitudes A[zi][zj], 4 × 4, zero-padded
   load_amplitudes(prm, KIND, sA);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -255,8 +263,9 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
     k_pair32(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
              const double4* __restrict__ pos, const int* __restrict__ perm, int ncells, PairParams prm,
              double* __restrict__ F, double* __restrict__ cellpart, unsigned long long* __restrict__ npairs) {
-  __shared__ PairStage stage[PAIR_WARPS];
-  __shared__ FlatScratch<float> scratch[PAIR_WARPS];
+  extern __shared__ __align__(16) unsigned char pair_smem[];
+  PairStage* stage = reinterpret_cast<PairStage*>(pair_smem);
+  FlatScratch<float>* scratch = reinterpret_cast<FlatScratch<float>*>(pair_smem + sizeof(PairStage) * PAIR_WARPS);
   __shared__ double sA[16];
   load_amplitudes(prm, KIND, sA);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -374,6 +383,11 @@ PairParams make_pair_params(const pfw_ws* ws, uint32_t req) {
 // Device work of one pair evaluation on a planned cell list: cell-list build,
 // output clears, the pair kernel and the reductions (no allocation once the
 // buffers are sized, no host synchronisation: capturable).
+template <class T>
+constexpr int pair_smem_bytes() {
+  return (int)((sizeof(PairStage) + sizeof(FlatScratch<T>)) * PAIR_WARPS);
+}
+
 static void pair_launch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system,
                         bool wrapped) {
   const PairModel& m = ws->pair;
@@ -402,17 +416,17 @@ static void pair_launch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
     dim3 grid(grid_for(ncells, PAIR_WARPS)), block(PAIR_WARPS * 32);
     bool mixed = ws->opt.precision == PFW_PRECISION_MIXED;
     if (mixed && all_shift) {
-      if (m.kind == 0) k_pair32<0, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
-      else k_pair32<1, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      if (m.kind == 0) k_pair32<0, 0><<<grid, block, pair_smem_bytes<float>(), st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      else k_pair32<1, 0><<<grid, block, pair_smem_bytes<float>(), st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
     } else if (mixed) {
-      if (m.kind == 0) k_pair32<0, 1><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
-      else k_pair32<1, 1><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      if (m.kind == 0) k_pair32<0, 1><<<grid, block, pair_smem_bytes<float>(), st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      else k_pair32<1, 1><<<grid, block, pair_smem_bytes<float>(), st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
     } else if (all_shift) {
-      if (m.kind == 0) k_pair64<0, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
-      else k_pair64<1, 0><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      if (m.kind == 0) k_pair64<0, 0><<<grid, block, pair_smem_bytes<double>(), st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      else k_pair64<1, 0><<<grid, block, pair_smem_bytes<double>(), st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
     } else {
-      if (m.kind == 0) k_pair64<0, 1><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
-      else k_pair64<1, 1><<<grid, block, 0, st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      if (m.kind == 0) k_pair64<0, 1><<<grid, block, pair_smem_bytes<double>(), st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
+      else k_pair64<1, 1><<<grid, block, pair_smem_bytes<double>(), st>>>(dsys, cell_sys, cs, pos, perm, ncells, prm, F, parts, np);
     }
     ws->launches += 1;
   }
@@ -474,8 +488,10 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   // for the largest carveout
   for (const void* k : {(const void*)k_pair64<0, 0>, (const void*)k_pair64<1, 0>, (const void*)k_pair64<0, 1>,
                         (const void*)k_pair64<1, 1>, (const void*)k_pair32<0, 0>, (const void*)k_pair32<1, 0>,
-                        (const void*)k_pair32<0, 1>, (const void*)k_pair32<1, 1>})
+                        (const void*)k_pair32<0, 1>, (const void*)k_pair32<1, 1>}) {
     PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem_bytes<double>()));
+  }
   // cell list without a mid-call synchronisation: its input flags are read
   // once at the end (a bad input only makes clamped cells and NaN sums)
   const bool wrapped = prepare_plan(ws, m.cutoff);

@@ -116,11 +116,13 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
   const int nstencil = cnt0 * cnt1 * cnt2;
   const float c2hi = (float)g.c2 * PREFILTER_GUARD;
   constexpr int RING = Stage::ring;
-  constexpr bool PRUNE = MODE == 0 && RING == 2 * TRAVERSE_STAGE;
+  constexpr bool PAIR = RING == 2 * TRAVERSE_STAGE;  // the pair kernels' staging
+  constexpr bool PRUNE = MODE == 0 && PAIR;
   const double4 ref = pos[b];
   for (int i0 = b; i0 < e; i0 += 32) {
     const int i = i0 + lane;
     const bool have = i < e;
+    const int nh = min(32, e - i0);  // home atoms of this chunk
     const double4 pi = have ? pos[i] : ref;
     const float2 nx = make_float2(-(float)(pi.x - ref.x), -(float)(pi.x - ref.x));
     const float2 ny = make_float2(-(float)(pi.y - ref.y), -(float)(pi.y - ref.y));
@@ -176,6 +178,44 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
       int wpos = 0, rpos = 0;
       auto test_window = [&](int n) {
         const int base = rpos & (RING - 1);
+        if (PAIR) {
+          // transposed: lane t holds staged atom t; the warp walks the home
+          // atoms two at a time and each ballot appends one home's survivors
+          // at consecutive slots of its list (the self pair is left to the
+          // drain, which sees the entry's owner)
+          const bool mine = lane < n;
+          const unsigned it = stage.sitem[base + (mine ? lane : 0)];
+          float2 cx = make_float2(1e30f, 1e30f), cy = cx, cz = cx;
+          if (MODE == 0 && mine) {
+            const float x = reinterpret_cast<const float*>(stage.x2)[base + lane];
+            const float y = reinterpret_cast<const float*>(stage.y2)[base + lane];
+            const float z = reinterpret_cast<const float*>(stage.z2)[base + lane];
+            cx = make_float2(x, x); cy = make_float2(y, y); cz = make_float2(z, z);
+          }
+          const unsigned below = (1u << lane) - 1u;
+          for (int h = 0; h < nh; h += 2) {
+            const int h1 = min(h + 1, 31);
+            bool a = mine, b = mine && h + 1 < nh;
+            if (MODE == 0) {
+              const float2 hx = make_float2(__shfl_sync(0xffffffffu, nx.x, h), __shfl_sync(0xffffffffu, nx.x, h1));
+              const float2 hy = make_float2(__shfl_sync(0xffffffffu, ny.x, h), __shfl_sync(0xffffffffu, ny.x, h1));
+              const float2 hz = make_float2(__shfl_sync(0xffffffffu, nz.x, h), __shfl_sync(0xffffffffu, nz.x, h1));
+              const float2 dx = __fadd2_rn(cx, hx), dy = __fadd2_rn(cy, hy), dz = __fadd2_rn(cz, hz);
+              const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+              a = a && r2.x < c2hi;
+              b = b && r2.y < c2hi;
+            }
+            const unsigned ma = __ballot_sync(0xffffffffu, a), mb = __ballot_sync(0xffffffffu, b);
+            const int ca = __shfl_sync(0xffffffffu, cnt, h), cb = __shfl_sync(0xffffffffu, cnt, h1);
+            if (a) stage.list[list_slot(ca + __popc(ma & below), h)] = it;
+            if (b) stage.list[list_slot(cb + __popc(mb & below), h1)] = it;
+            if (lane == h) cnt += __popc(ma);
+            if (lane == h + 1) cnt += __popc(mb);
+          }
+          rpos += n;
+          if (__reduce_max_sync(0xffffffffu, cnt) > Stage::capacity - TRAVERSE_STAGE) drain(have, i, pi, cnt);
+          return;
+        }
         unsigned mask;
         if (MODE == 0) {
           mask = 0u;
