@@ -96,10 +96,11 @@ __device__ __forceinline__ double entry_geometry(const SysGeom& g, const Stencil
   return xr2(d[0], d[1], d[2]);
 }
 
-template <int MODE, class T, class Eval>
+// tick() runs after every step of one or two entries.
+template <int MODE, class T, class Eval, class Tick>
 __device__ __forceinline__ void flat_drain(const SysGeom& g, const double4* __restrict__ pos,
                                            const PairStage& stage, FlatScratch<T>& fs, int lane, int i0,
-                                           unsigned ownmask, int& cnt, T f[3], Eval&& eval) {
+                                           unsigned ownmask, int& cnt, T f[3], Eval&& eval, Tick&& tick) {
   constexpr unsigned FULL = 0xffffffffu;
   __syncwarp();
   int incl = cnt;
@@ -157,6 +158,7 @@ __device__ __forceinline__ void flat_drain(const SysGeom& g, const double4* __re
       px += ax; py += ay; pz += az;
       px += bx; py += by; pz += bz;
       q += two ? 2 : 1;
+      tick();
     }
     fs.part[lane + h][0] = px; fs.part[lane + h][1] = py; fs.part[lane + h][2] = pz;
   }
@@ -175,11 +177,11 @@ __device__ __forceinline__ void flat_drain(const SysGeom& g, const double4* __re
 
 // One home cell of a pair kernel: the prefilter, the flat drains, and the
 // force of each home atom written once, in place, at the end of its chunk.
-template <int MODE, class T, class Eval>
+template <int MODE, class T, class Eval, class Tick>
 __device__ __forceinline__ void pair_cell(const SysGeom& g, int cell, const int* __restrict__ cell_start,
                                           const double4* __restrict__ pos, const int* __restrict__ perm,
                                           const PairParams& prm, PairStage& stage, FlatScratch<T>& fs, int lane,
-                                          double* __restrict__ F, Eval&& eval) {
+                                          double* __restrict__ F, Eval&& eval, Tick&& tick) {
   T f[3] = {0, 0, 0};
   unsigned ownmask = 0u;  // home atoms of the chunk that own their E/W shares
   int cur = -1;
@@ -190,7 +192,7 @@ __device__ __forceinline__ void pair_cell(const SysGeom& g, int cell, const int*
           cur = i;
           ownmask = __ballot_sync(0xffffffffu, have && perm[i] < prm.n_owned);
         }
-        flat_drain<MODE>(g, pos, stage, fs, lane, i - lane, ownmask, cnt, f, eval);
+        flat_drain<MODE>(g, pos, stage, fs, lane, i - lane, ownmask, cnt, f, eval, tick);
       },
       [&](bool have, int i, const double4&) {
         if (have && prm.want_f) {
@@ -242,7 +244,8 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR_MINBLOCKS)
         e += (hit && ownh) ? en : 0.0;
         w[0] += o * (d[0] * gx); w[1] += o * (d[1] * gy); w[2] += o * (d[2] * gz);
         w[3] += o * (d[0] * gy); w[4] += o * (d[0] * gz); w[5] += o * (d[1] * gz);
-      });
+      },
+      [] {});
   write_cell_parts(cellpart, cell, lane, e, w, np, npairs);
 }
 
@@ -292,11 +295,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
       g, cell, cell_start, pos, perm, prm, stage[warp], scratch[warp], lane, F,
       [&](const double4& ph, bool ownh, const double4& pj, const double* d, double r2d, bool hit, float& gx,
           float& gy, float& gz) {
-        if (!hit) {
-          gx = gy = gz = 0.f;
-          return;
-        }
-        ++np;
+        np += hit;
         const float d0 = (float)d[0], d1 = (float)d[1], d2 = (float)d[2];
         const float r2 = (float)r2d;
         float en, coef;
@@ -313,13 +312,15 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, PFW_PAIR32_MINBLOCKS)
           en = eps4 * (s6 * s6 - s6) - shift;
           coef = eps24 * (s6 - 2.f * s6 * s6) * ir2;
         }
+        coef = hit ? coef : 0.f;  // without branches: a miss has r2 >= c², finite terms
         gx = coef * d0; gy = coef * d1; gz = coef * d2;
-        if (ownh) {
-          ce += en;
-          cw[0] += d0 * gx; cw[1] += d1 * gy; cw[2] += d2 * gz;
-          cw[3] += d0 * gy; cw[4] += d0 * gz; cw[5] += d1 * gz;
-          if (++cn == MIXED_CHUNK) fold();
-        }
+        const float o = ownh ? 1.f : 0.f;
+        ce += (hit && ownh) ? en : 0.f;
+        cw[0] += o * (d0 * gx); cw[1] += o * (d1 * gy); cw[2] += o * (d2 * gz);
+        cw[3] += o * (d0 * gy); cw[4] += o * (d0 * gz); cw[5] += o * (d1 * gz);
+      },
+      [&] {  // at most MIXED_CHUNK pairs (two per step) in the FP32 partial sums
+        if (++cn == MIXED_CHUNK / 2) fold();
       });
   fold();
   double w[6];

@@ -12,11 +12,14 @@
 // re-tests with the exact reference arithmetic
 // (NeighbourList/geometry.jl:5-19) and calls visit for pairs with r² < c².
 //
-// Pair kernels drain the lists differently (traverse_lists below takes the
-// drain as a callable): the warp walks all lanes' lists as one sequence.  For
-// that the list is stored with the lane index xor-ed with the slot, so that
-// 32 consecutive slots of ONE lane sit in 32 distinct banks, while one slot
-// of all lanes still does.
+// Pair kernels (a staging ring of 64) test and drain differently.  The test
+// is transposed: lanes hold the staged atoms, the warp walks the home atoms
+// and a ballot appends each home atom's survivors at consecutive slots of its
+// list (the zero-shift self pair is left to the drain).  The drain is a
+// callable of traverse_lists: the pair kernels walk all lanes' lists as one
+// sequence.  For both, the list is stored with the lane index xor-ed with the
+// slot, so that 32 consecutive slots of ONE lane sit in 32 distinct banks,
+// while one slot of all lanes still does.
 //
 // The FP32 test can only reject pairs whose exact r² exceeds c²: with
 // coordinates relative to a point at most R away, |r²₃₂ - r²| ≤ c²·(4e-7·R/c
