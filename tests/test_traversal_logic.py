@@ -1,0 +1,98 @@
+"""Host-side checks of two arguments the pair kernels' traversal rests on
+(csrc/traverse.cuh, csrc/pair.cu), restated in numpy:
+
+* the box prune: a staged atom is dropped when the FP32 distance² from its
+  FP32 coordinates to the bounding box of the home atoms' FP32 coordinates is
+  not below c²·(1 + 2⁻¹⁰).  No atom within the exact FP64 cutoff of a home
+  atom may be dropped — checked on random home sets with candidates placed at
+  c·(1 ± 1e-7 … 1e-3) from a home atom, the hardest cases;
+* the flat drain: the lanes' lists form one owner-major sequence, lane l
+  takes entries [l·R, (l+1)·R) with R = ceil(total/32), stores the partial of
+  owner h in slot l + h, and owner h adds the slots of lanes off_h/R …
+  (off_h + cnt_h − 1)/R.  Slots must be unique, and each owner must collect
+  exactly its own entries — checked on random count vectors, zero counts
+  included.
+"""
+import numpy as np
+
+GUARD = np.float32(1.0 + 1.0 / 1024.0)
+
+
+def box_keep(cand32, lo32, hi32, c2hi):
+    """The kernel's FP32 box test: fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < c2hi."""
+    e = np.maximum(np.maximum(lo32 - cand32, cand32 - hi32), np.float32(0.0)).astype(np.float32)
+    ez2 = (e[..., 2] * e[..., 2]).astype(np.float32)
+    # fmaf: exact product and sum in float64, one rounding to float32
+    t = (e[..., 1].astype(np.float64) * e[..., 1] + ez2).astype(np.float32)
+    d2 = (e[..., 0].astype(np.float64) * e[..., 0] + t).astype(np.float32)
+    return d2 < c2hi
+
+
+def test_box_prune_never_drops_a_neighbour():
+    rng = np.random.default_rng(20)
+    for c in (2.0, 5.5, 8.5):
+        c2 = c * c
+        c2hi = np.float32(np.float32(c2) * GUARD)
+        for trial in range(200):
+            L = rng.uniform(0.5, 1.5) * c
+            base = rng.uniform(-300.0, 300.0, 3)  # absolute coordinates far from 0
+            home = base + rng.uniform(0.0, L, (rng.integers(1, 33), 3))
+            ref = home[0]
+            rel32 = (home - ref).astype(np.float32)
+            lo32, hi32 = rel32.min(axis=0), rel32.max(axis=0)
+            # candidates just inside the cutoff of a random home atom, in random directions
+            k = rng.integers(0, len(home), 256)
+            u = rng.normal(size=(256, 3))
+            u /= np.linalg.norm(u, axis=1)[:, None]
+            r = c * (1.0 - 10.0 ** rng.uniform(-7, -3, 256))
+            cand = home[k] + u * r[:, None]
+            d = cand - home[k]
+            exact = (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+            inside = exact < c2
+            cand32 = (cand - ref).astype(np.float32)
+            keep = box_keep(cand32, lo32, hi32, c2hi)
+            assert np.all(keep[inside]), (c, trial)
+
+
+def flat_partition(cnt, W=32):
+    cnt = np.asarray(cnt)
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    total = int(off[-1])
+    R = (total + W - 1) // W
+    slots = {}
+    for lane in range(W):
+        q0, q1 = lane * R, min(lane * R + R, total)
+        for q in range(q0, q1):
+            h = int(np.searchsorted(off[:W], q, side="right") - 1)  # last owner with off <= q
+            assert off[h] <= q < off[h + 1]
+            key = lane + h
+            if key in slots:
+                assert slots[key][0] == lane and slots[key][1] == h  # the same segment continues
+                slots[key][2].append(q)
+            else:
+                slots[key] = [lane, h, [q]]
+    # each owner's partials: lanes off_h / R .. (off_h + cnt_h - 1) / R
+    for h in range(W):
+        if cnt[h] == 0:
+            continue
+        la, lb = off[h] // R, (off[h] + cnt[h] - 1) // R
+        got = []
+        for lane in range(la, lb + 1):
+            seg = slots[lane + h]
+            assert seg[0] == lane and seg[1] == h
+            got += seg[2]
+        assert got == list(range(off[h], off[h + 1]))
+    assert max(slots) <= 62 if slots else True
+
+
+def test_flat_drain_slots_are_unique_and_complete():
+    rng = np.random.default_rng(5)
+    flat_partition([0] * 32)
+    flat_partition([1] + [0] * 31)
+    flat_partition([0] * 31 + [72])
+    flat_partition([72] * 32)
+    for _ in range(300):
+        nh = int(rng.integers(1, 33))
+        cnt = np.zeros(32, int)
+        cnt[:nh] = rng.integers(0, 73, nh) * (rng.random(nh) > 0.2)
+        flat_partition(cnt)
