@@ -342,25 +342,33 @@ int32_t pfw_stage_times(pfw_ws* ws, double* ms, int32_t cap);
  * hosts whose runtime owns every byte of device memory through its own pool,
  * and code that must not trigger the device-wide synchronisation a fresh
  * allocation can cause.  Evaluates SmoothPair (kind 0, params = nz×nz
- * amplitudes) or Lennard-Jones (kind 1, params = {epsilon, sigma}) energy,
- * forces and virial of one small system, brute force, with the reference's
- * minimum-image geometry.  Limits: n <= PFW_NOALLOC_MAX_ATOMS atoms, an
- * orthorhombic cell whose periodic lengths exceed 2·cutoff (open axes
- * allowed).  X_dev (3×n), species_dev (n) and the outputs E_dev (1), F_dev
- * (3×n, original order) and W_dev (9) are DEVICE memory owned by the caller;
- * H, pbc and params are host arrays.  Work is queued on `stream` (a
- * cudaStream_t, NULL = default stream) without synchronising.  The only
- * scratch is a fixed 4 KiB static device array (per-block partial sums) that
- * every GPU loading the library keeps until exit; the first call on a device
- * looks up its address, so make that first call before any stream capture.
- * Calls that overlap on the GPU share that array and race: serialise them.
- * A message is copied to errbuf (errlen bytes) on failure. */
+ * amplitudes, finite and symmetric) or Lennard-Jones (kind 1, params =
+ * {epsilon, sigma}) energy, forces and virial of one small system, brute
+ * force, with the reference's minimum-image geometry.  Limits: n <=
+ * PFW_NOALLOC_MAX_ATOMS atoms, an orthorhombic cell whose periodic lengths
+ * exceed 2·cutoff (open axes allowed).  X_dev (3×n), species_dev (n) and the
+ * outputs E_dev (1), F_dev (3×n, original order; required when forces are
+ * requested) and W_dev (9) are DEVICE memory owned by the caller; H, pbc and
+ * params are host arrays.  Work is queued on `stream` (a cudaStream_t, NULL =
+ * default stream) without synchronising, so errors that depend on the data
+ * arrive through status_dev (optional device int32, written when the queued
+ * work completes): PFW_OK; PFW_EINVAL for a species channel outside [0, nz)
+ * (SmoothPair) or negative, or a non-finite position; PFW_EDOMAIN for a
+ * non-finite energy or virial (coincident atoms with Lennard-Jones).  The
+ * outputs are undefined unless it reads PFW_OK.  The only scratch is a fixed
+ * static device array of 64 blocks × 8 doubles plus one status word (4 KiB)
+ * that every GPU loading the library keeps until exit; every call looks up
+ * its device address (the first call on a device also loads the module, so
+ * make that first call before any stream capture).  Calls that overlap on the
+ * GPU share that array and race: serialise them.  The caller's current
+ * device is left as it was.  A message is copied to errbuf (errlen bytes)
+ * when an argument is rejected. */
 #define PFW_NOALLOC_MAX_ATOMS 8192
 pfw_status pfw_pair_evaluate_noalloc(int32_t device, void* stream, int64_t n, const double* X_dev,
                                      const int32_t* species_dev, const double H[9], const uint8_t pbc[3],
                                      int32_t kind, int32_t nz, const double* params, double cutoff,
                                      uint32_t request, double* E_dev, double* F_dev, double* W_dev,
-                                     char* errbuf, int32_t errlen);
+                                     int32_t* status_dev, char* errbuf, int32_t errlen);
 
 #ifdef __cplusplus
 }

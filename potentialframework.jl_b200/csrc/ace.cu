@@ -711,7 +711,7 @@ static void ace_check(pfw_ws* ws, AceDevice* a) {
 void ace_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev) {
   AceDevice* a = ws->ace;
   if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
-  if (ws->max_species >= a->nz) throw Error(PFW_EINVAL, "ACE model has no element channel for a species");
+  check_species(ws, a->nz, "ACE model has no element channel for a species");
   cudaStream_t st = ws->stream;
   ws->prep.valid = false;
   ws->stage_begin(3);
@@ -796,7 +796,7 @@ static void batch_launch(pfw_ws* ws, AceDevice* a, uint32_t req, const AceLayout
 void ace_evaluate_batch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, double* feat_dev) {
   AceDevice* a = ws->ace;
   if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
-  if (ws->max_species >= a->nz) throw Error(PFW_EINVAL, "ACE model has no element channel for a species");
+  check_species(ws, a->nz, "ACE model has no element channel for a species");
   cudaStream_t st = ws->stream;
   ws->prep.valid = false;
   prepare(ws, a->cutoff);
@@ -949,7 +949,7 @@ void ace_design_shape(pfw_ws* ws, int64_t* rows, int64_t* cols) {
 void ace_design_matrix(pfw_ws* ws, double* A_dev, int64_t ld, int64_t rows_capacity, double* base_dev) {
   AceDevice* a = ws->ace;
   if (!a) throw Error(PFW_ESTATE, "no ACE model loaded");
-  if (ws->max_species >= a->nz) throw Error(PFW_EINVAL, "ACE model has no element channel for a species");
+  check_species(ws, a->nz, "ACE model has no element channel for a species");
   if (a->nQ > 4 * ACE_GROUP) throw Error(PFW_EINVAL, "design rows support at most 256 pair channels");
   int64_t rows = 0, cols = 0;
   ace_design_shape(ws, &rows, &cols);
@@ -1237,7 +1237,7 @@ __global__ void k_permute_rows(int n, int w, const double* __restrict__ in, cons
 void sur_features(pfw_ws* ws, double* out_dev) {
   SurDevice* d = ws->sur;
   if (!d) throw Error(PFW_ESTATE, "no surrogate feature model loaded");
-  if (ws->max_species >= d->nz) throw Error(PFW_EINVAL, "feature model has no element channel for a species");
+  check_species(ws, d->nz, "feature model has no element channel for a species");
   sur_prepare(ws, d);
   const int n = ws->prep.n;
   SiteLaunch s = sur_launch(ws, d, n, false);
@@ -1271,7 +1271,7 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   if (!full) throw Error(PFW_ESTATE, "the surrogate falls back to the ACE model: load it first");
   if (full->cutoff != d->fm->cutoff || full->nz != d->nz)
     throw Error(PFW_EINVAL, "surrogate feature model and ACE model differ in cutoff or species");
-  if (ws->max_species >= d->nz) throw Error(PFW_EINVAL, "feature model has no element channel for a species");
+  check_species(ws, d->nz, "feature model has no element channel for a species");
   if (ws->opt.precision != PFW_PRECISION_FP64) throw Error(PFW_EINVAL, "the surrogate path runs in the FP64 workspace");
   AceDevice* a = d->fm;
   cudaStream_t st = ws->stream;

@@ -474,6 +474,7 @@ pfw_status pfw_last_pair_count(pfw_ws* ws, int64_t* npairs) {
 
 pfw_status pfw_neighbour_count(pfw_ws* ws, double cutoff, int64_t* total) {
   return guarded(ws, [&] {
+    ws->species_limit = INT32_MAX;  // the snapshot needs no model: any nonnegative channel
     int64_t t = pfw::neighbour_build(ws, cutoff);
     if (total) *total = t;
   });

@@ -302,12 +302,23 @@ __global__ void k_cell_rank(int ncells, const int* __restrict__ cell_start, cons
   }
 }
 
+// Species channels are validated here, on the device, because geometry
+// uploaded from device memory is never seen by the host: a channel outside
+// [0, limit) (limit = the channel count of the model being evaluated) sets
+// bad_species, which prepare_check turns into PFW_EINVAL, and is stored as
+// channel 0 so that no kernel indexes a model table with it.
 __global__ void k_gather(int n, const int* __restrict__ perm, const double* __restrict__ wrapped,
-                         const int* __restrict__ species, double4* __restrict__ pos, int* __restrict__ inverse) {
+                         const int* __restrict__ species, double4* __restrict__ pos, int* __restrict__ inverse,
+                         int limit, int* __restrict__ bad_species) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   int i = perm[k];
-  pos[k] = make_double4(wrapped[3 * i], wrapped[3 * i + 1], wrapped[3 * i + 2], (double)species[i]);
+  int z = species[i];
+  if (z < 0 || z >= limit) {
+    atomicExch(bad_species, 1);
+    z = 0;
+  }
+  pos[k] = make_double4(wrapped[3 * i], wrapped[3 * i + 1], wrapped[3 * i + 2], (double)z);
   inverse[i] = k;
 }
 
@@ -495,6 +506,7 @@ bool prepare_plan(pfw_ws* ws, double cutoff) {
   P.n = n;
   P.any_image = any_image;
   P.cutoff = cutoff;
+  P.species_limit = ws->species_limit;
   ws->cell_count.ensure(sizeof(int) * (ncells + 1));
   ws->cell_start.ensure(sizeof(int) * (ncells + 1));
   ws->cellid.ensure(sizeof(int) * std::max(n, 1));
@@ -544,7 +556,8 @@ void prepare_launch(pfw_ws* ws, bool wrap) {
     k_cell_rank<<<grid_for((int64_t)ncells * 32, 256), 256, 0, st>>>((int)ncells, cell_start, ws->tmp_idx.as<int>(),
                                                                       ws->perm.as<int>());
     k_gather<<<grid_for(n, 256), 256, 0, st>>>(n, ws->perm.as<int>(), ws->wrapped.as<double>(),
-                                               ws->species.as<int>(), ws->pos.as<double4>(), ws->inverse.as<int>());
+                                               ws->species.as<int>(), ws->pos.as<double4>(), ws->inverse.as<int>(),
+                                               ws->species_limit, bad + 2);
     ws->launches += 3;
   }
   if (ncells > 0) {
@@ -563,12 +576,15 @@ void prepare_check(pfw_ws* ws) {
   PFW_CUDA(cudaGetLastError());
   if (hbad[0] == 1) throw Error(PFW_EINVAL, "positions must be finite");
   if (hbad[0] == 2) throw Error(PFW_EINVAL, "atom outside the open-axis cell grid");
+  if (hbad[2])
+    throw Error(PFW_EINVAL, "species channel outside the model's channels (must be >= 0 and < " +
+                                std::to_string(ws->species_limit) + ")");
   ws->prep.max_cell = hbad[4];
 }
 
 void prepare(pfw_ws* ws, double cutoff) {
   Prepared& P = ws->prep;
-  if (P.valid && P.cutoff == cutoff) return;
+  if (P.valid && P.cutoff == cutoff && P.species_limit == ws->species_limit) return;
   const bool wrapped = prepare_plan(ws, cutoff);
   prepare_launch(ws, !wrapped);
   prepare_check(ws);

@@ -29,11 +29,16 @@ namespace pfw {
 
 constexpr int NOALLOC_BLOCK = 128;
 constexpr int NOALLOC_MAX_BLOCKS = PFW_NOALLOC_MAX_ATOMS / NOALLOC_BLOCK;
+constexpr int NOALLOC_STATUS = NOALLOC_MAX_BLOCKS * 8;  // index of the status word (as 64-bit flags)
 
-// Scratch: 8 doubles (E, six virial components, pad) per block.  Every call
-// overwrites every entry it later reads, so nothing needs clearing between
-// calls; calls that overlap on the GPU race on this array.
-static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_BLOCKS * 8];
+// Scratch: 8 doubles (E, six virial components, pad) per block, then one
+// 64-bit word of input flags.  The partials are overwritten by every call
+// before they are read; the flag word is cleared by the first kernel of every
+// call.  Calls that overlap on the GPU race on this array.
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_MAX_BLOCKS * 8 + 8];
+
+// Input flags raised by the pair kernel (bits of the status word).
+constexpr unsigned long long NOALLOC_BAD_SPECIES = 1ull, NOALLOC_BAD_POSITION = 2ull;
 
 struct NoallocParams {
   int kind, nz, n;
@@ -45,10 +50,21 @@ struct NoallocParams {
   int want_f;
 };
 
+// A species channel outside [0, nz) or a non-finite position raises a flag
+// in the status word (the channel is then read as 0, so no table is indexed
+// out of range).
+__device__ __forceinline__ int noalloc_species(const NoallocParams& p, int z, unsigned long long* status) {
+  if (z < 0 || z >= p.nz) {
+    atomicOr(status, NOALLOC_BAD_SPECIES);
+    return 0;
+  }
+  return z;
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(NOALLOC_BLOCK)
     k_pair_noalloc(NoallocParams p, const double* __restrict__ X, const int* __restrict__ species,
-                   double* __restrict__ F, double* __restrict__ partials) {
+                   double* __restrict__ F, double* __restrict__ partials, unsigned long long* __restrict__ status) {
   __shared__ double stage[NOALLOC_BLOCK][4];
   __shared__ double red[7][NOALLOC_BLOCK];
   const int i = blockIdx.x * NOALLOC_BLOCK + threadIdx.x;
@@ -57,8 +73,12 @@ __global__ void __launch_bounds__(NOALLOC_BLOCK)
   int zi = 0;
   if (have) {
 #pragma unroll
-    for (int a = 0; a < 3; ++a) xi[a] = p.pbc[a] ? jl_mod(X[3 * i + a], p.L[a]) : X[3 * i + a];
-    zi = min(max(species[i], 0), p.nz - 1);
+    for (int a = 0; a < 3; ++a) {
+      const double x = X[3 * i + a];
+      if (!isfinite(x)) atomicOr(status, NOALLOC_BAD_POSITION);
+      xi[a] = p.pbc[a] ? jl_mod(x, p.L[a]) : x;
+    }
+    zi = noalloc_species(p, species[i], status);
   }
   double fx = 0, fy = 0, fz = 0, e = 0, w[6] = {0, 0, 0, 0, 0, 0};
   for (int j0 = 0; j0 < p.n; j0 += NOALLOC_BLOCK) {
@@ -67,7 +87,7 @@ __global__ void __launch_bounds__(NOALLOC_BLOCK)
     if (jj < p.n) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) stage[threadIdx.x][a] = p.pbc[a] ? jl_mod(X[3 * jj + a], p.L[a]) : X[3 * jj + a];
-      stage[threadIdx.x][3] = (double)min(max(species[jj], 0), p.nz - 1);
+      stage[threadIdx.x][3] = (double)min(max(species[jj], 0), p.nz - 1);  // flagged on its own row
     }
     __syncthreads();
     if (!have) continue;
@@ -120,8 +140,15 @@ __global__ void __launch_bounds__(NOALLOC_BLOCK)
   if (threadIdx.x < 8) partials[8 * blockIdx.x + threadIdx.x] = threadIdx.x < 7 ? red[threadIdx.x][0] : 0.0;
 }
 
-__global__ void k_reduce_noalloc(int nblocks, const double* __restrict__ partials, double* __restrict__ E,
-                                 double* __restrict__ W) {
+__global__ void k_noalloc_clear(unsigned long long* __restrict__ status) { *status = 0ull; }
+
+// Totals of the block partials in block order, and the call's status: the
+// input flags first (PFW_EINVAL), then a non-finite energy or virial
+// (PFW_EDOMAIN, as the allocating entry point reports coincident atoms of a
+// singular model).
+__global__ void k_reduce_noalloc(int nblocks, const double* __restrict__ partials,
+                                 const unsigned long long* __restrict__ flags, double* __restrict__ E,
+                                 double* __restrict__ W, int32_t* __restrict__ status_out) {
   if (threadIdx.x != 0) return;
   double s[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int b = 0; b < nblocks; ++b)
@@ -134,27 +161,22 @@ __global__ void k_reduce_noalloc(int nblocks, const double* __restrict__ partial
     W[2] = W[6] = s[5];
     W[5] = W[7] = s[6];
   }
+  if (status_out) {
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) finite = finite && isfinite(s[k]);
+    *status_out = *flags ? PFW_EINVAL : (finite ? PFW_OK : PFW_EDOMAIN);
+  }
 }
 
-// Device address of the scratch array, looked up once per device with that
-// device current (a host-side reference to the array is only a stand-in).
-static double* scratch_address(int device, cudaError_t* err) {
-  constexpr int MAXDEV = 64;
-  static std::mutex mu;
-  static double* addr[MAXDEV] = {};
-  if (device < 0 || device >= MAXDEV) {
-    *err = cudaErrorInvalidDevice;
-    return nullptr;
-  }
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[device]) {
-    void* ptr = nullptr;
-    *err = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
-    if (*err != cudaSuccess) return nullptr;
-    addr[device] = static_cast<double*>(ptr);
-  }
-  *err = cudaSuccess;
-  return addr[device];
+// Device address of the scratch array on the current device.  A host-side
+// reference to the array is only a stand-in, so the address is looked up on
+// every call (cheap once the module is loaded; no stale pointer survives a
+// device reset).
+static double* scratch_address(cudaError_t* err) {
+  void* ptr = nullptr;
+  *err = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+  return *err == cudaSuccess ? static_cast<double*>(ptr) : nullptr;
 }
 
 }  // namespace pfw
@@ -163,7 +185,7 @@ extern "C" pfw_status pfw_pair_evaluate_noalloc(int32_t device, void* stream, in
                                                 const int32_t* species_dev, const double H[9], const uint8_t pbc[3],
                                                 int32_t kind, int32_t nz, const double* params, double cutoff,
                                                 uint32_t request, double* E_dev, double* F_dev, double* W_dev,
-                                                char* errbuf, int32_t errlen) {
+                                                int32_t* status_dev, char* errbuf, int32_t errlen) {
   auto fail = [&](pfw_status code, const char* msg) {
     if (errbuf && errlen > 0) {
       std::strncpy(errbuf, msg, (size_t)errlen - 1);
@@ -175,6 +197,8 @@ extern "C" pfw_status pfw_pair_evaluate_noalloc(int32_t device, void* stream, in
   if (n < 0 || n > PFW_NOALLOC_MAX_ATOMS) return fail(PFW_EINVAL, "pfw_pair_evaluate_noalloc: at most 8192 atoms");
   if (!H || !pbc || !params || (n > 0 && (!X_dev || !species_dev)))
     return fail(PFW_EINVAL, "pfw_pair_evaluate_noalloc: null argument");
+  if ((request & PFW_REQ_FORCES) && n > 0 && !F_dev)
+    return fail(PFW_EINVAL, "pfw_pair_evaluate_noalloc: forces requested without a force buffer");
   if (!(std::isfinite(cutoff) && cutoff > 0)) return fail(PFW_EINVAL, "cutoff must be finite and positive (Å)");
   pfw::NoallocParams p{};
   p.n = (int)n;
@@ -191,6 +215,11 @@ extern "C" pfw_status pfw_pair_evaluate_noalloc(int32_t device, void* stream, in
   }
   if (kind == 0) {
     if (nz < 1 || nz > 4) return fail(PFW_EINVAL, "SmoothPair supports 1 to 4 species channels");
+    // the amplitude table must be finite and symmetric (PairPotentials/models.jl:39)
+    for (int a = 0; a < nz; ++a)
+      for (int b = 0; b < nz; ++b)
+        if (!std::isfinite(params[a * nz + b]) || params[a * nz + b] != params[b * nz + a])
+          return fail(PFW_EINVAL, "SmoothPair amplitudes must be finite and symmetric");
     for (int k = 0; k < nz * nz; ++k) p.A[k] = params[k];
     p.nz = nz;
     p.invc2 = 1.0 / (cutoff * cutoff);
@@ -198,7 +227,7 @@ extern "C" pfw_status pfw_pair_evaluate_noalloc(int32_t device, void* stream, in
     const double eps = params[0], sigma = params[1];
     if (!(eps > 0 && sigma > 0 && std::isfinite(eps) && std::isfinite(sigma)))
       return fail(PFW_EINVAL, "LJ parameters must be positive and finite");
-    p.nz = 1;
+    p.nz = INT32_MAX;  // any nonnegative species channel
     p.eps4 = 4.0 * eps;
     p.eps24 = 24.0 * eps;
     p.sigma2 = sigma * sigma;
@@ -207,24 +236,33 @@ extern "C" pfw_status pfw_pair_evaluate_noalloc(int32_t device, void* stream, in
   } else {
     return fail(PFW_EINVAL, "kind must be 0 (SmoothPair) or 1 (Lennard-Jones)");
   }
-  cudaError_t e = cudaSetDevice(device);
+  // the caller's current device is restored on every return below
+  int caller_device = -1;
+  cudaError_t e = cudaGetDevice(&caller_device);
   if (e != cudaSuccess) return fail(PFW_ECUDA, cudaGetErrorString(e));
-  double* partials = pfw::scratch_address(device, &e);
-  if (!partials) return fail(PFW_ECUDA, cudaGetErrorString(e));
+  auto done = [&](pfw_status code, const char* msg) {
+    cudaSetDevice(caller_device);
+    return code == PFW_OK ? code : fail(code, msg);
+  };
+  if (device != caller_device) {
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return done(PFW_ECUDA, cudaGetErrorString(e));
+  }
+  double* scratch = pfw::scratch_address(&e);
+  if (!scratch) return done(PFW_ECUDA, cudaGetErrorString(e));
+  unsigned long long* flags = reinterpret_cast<unsigned long long*>(scratch + pfw::NOALLOC_STATUS);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int blocks = std::max(1, (int)((n + pfw::NOALLOC_BLOCK - 1) / pfw::NOALLOC_BLOCK));
+  const int blocks = (int)((n + pfw::NOALLOC_BLOCK - 1) / pfw::NOALLOC_BLOCK);
+  pfw::k_noalloc_clear<<<1, 1, 0, st>>>(flags);
   if (n > 0) {
     if (kind == 0)
-      pfw::k_pair_noalloc<0><<<blocks, pfw::NOALLOC_BLOCK, 0, st>>>(p, X_dev, species_dev, F_dev, partials);
+      pfw::k_pair_noalloc<0><<<blocks, pfw::NOALLOC_BLOCK, 0, st>>>(p, X_dev, species_dev, F_dev, scratch, flags);
     else
-      pfw::k_pair_noalloc<1><<<blocks, pfw::NOALLOC_BLOCK, 0, st>>>(p, X_dev, species_dev, F_dev, partials);
-    pfw::k_reduce_noalloc<<<1, 32, 0, st>>>(blocks, partials, (request & PFW_REQ_ENERGY) ? E_dev : nullptr,
-                                            (request & PFW_REQ_VIRIAL) ? W_dev : nullptr);
-  } else {
-    pfw::k_reduce_noalloc<<<1, 32, 0, st>>>(0, partials, (request & PFW_REQ_ENERGY) ? E_dev : nullptr,
-                                            (request & PFW_REQ_VIRIAL) ? W_dev : nullptr);
+      pfw::k_pair_noalloc<1><<<blocks, pfw::NOALLOC_BLOCK, 0, st>>>(p, X_dev, species_dev, F_dev, scratch, flags);
   }
+  pfw::k_reduce_noalloc<<<1, 32, 0, st>>>(blocks, scratch, flags, (request & PFW_REQ_ENERGY) ? E_dev : nullptr,
+                                          (request & PFW_REQ_VIRIAL) ? W_dev : nullptr, status_dev);
   e = cudaGetLastError();
-  if (e != cudaSuccess) return fail(PFW_ECUDA, cudaGetErrorString(e));
-  return PFW_OK;
+  if (e != cudaSuccess) return done(PFW_ECUDA, cudaGetErrorString(e));
+  return done(PFW_OK, "");
 }

@@ -483,6 +483,7 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   if (m.kind < 0) throw Error(PFW_ESTATE, "no pair model loaded");
   if (m.kind == 0 && ws->max_species >= m.nz)
     throw Error(PFW_EINVAL, "potential has no parameters for species channel " + std::to_string(ws->max_species));
+  ws->species_limit = m.kind == 0 ? m.nz : INT32_MAX;
   if (!per_system && skin_pair_evaluate(ws, req, E_dev, F_dev, W_dev)) return;
   ws->prep.valid = false;  // evaluate! rebuilds topology on every call
   // the per-warp candidate lists make shared memory a residency limit: ask

@@ -68,6 +68,7 @@ struct Prepared {
   int32_t ncells = 0;
   int32_t nsys = 0;
   int32_t max_cell = 0;  // largest cell population
+  int32_t species_limit = INT32_MAX;  // species limit the sorted positions were validated against
   bool any_image = false;
   std::vector<SysGeom> sys;  // host copy
   bool valid = false;
@@ -94,6 +95,9 @@ struct pfw_ws {
   // geometry input (original order)
   int32_t n = 0;
   int32_t max_species = 0;  // largest species channel of host-uploaded geometry
+  // channel count of the model the next cell-list build serves: k_gather
+  // flags channels outside [0, species_limit) on the device (device uploads)
+  int32_t species_limit = INT32_MAX;
   std::vector<pfw::HostSystem> systems;
   uint64_t geometry_version = 0;  // bumped when the systems (count, sizes, cells) change
   int32_t n_owned = -1;           // atoms [0, n_owned) own E/W (domain decomposition); -1: all
@@ -188,4 +192,11 @@ void mlp_train(pfw_ws* ws, const pfw_mlp_shape* shape, float* params, int64_t n,
                const int32_t* species, const pfw_mlp_train_options* opt, float* epoch_loss);
 
 inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
+
+// A model with nz species channels is about to be evaluated: host-uploaded
+// species are checked here; device-uploaded ones by the next cell-list build.
+inline void check_species(pfw_ws* ws, int nz, const char* msg) {
+  if (ws->max_species >= nz) throw Error(PFW_EINVAL, msg);
+  ws->species_limit = nz;
+}
 }  // namespace pfw

@@ -53,10 +53,15 @@ void skin_free(pfw_ws* ws) {
   ws->skin_state = nullptr;
 }
 
+// out[0]: the largest squared displacement; out[1] set when a species channel
+// lies outside [0, limit) (device-uploaded species are only seen here on a
+// reuse step).
 __global__ void k_max_disp(int n, const double* __restrict__ X, const double* __restrict__ Xref,
-                           unsigned long long* __restrict__ out) {
+                           const int* __restrict__ species, int limit, unsigned long long* __restrict__ out) {
   double m = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int z = species[i];
+    if (z < 0 || z >= limit) out[1] = 1ull;
     const double dx = X[3 * i] - Xref[3 * i], dy = X[3 * i + 1] - Xref[3 * i + 1], dz = X[3 * i + 2] - Xref[3 * i + 2];
     const double d2 = dx * dx + dy * dy + dz * dz;
     m = (d2 > m || d2 != d2) ? (d2 != d2 ? INFINITY : d2) : m;  // a nonfinite position forces a rebuild
@@ -179,16 +184,20 @@ bool skin_pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
   const int n = ws->n;
   bool rebuild = !sk.valid || sk.cutoff != m.cutoff || sk.built_skin != ws->skin || sk.n != n ||
                  std::memcmp(sk.H, hs.H, sizeof(sk.H)) != 0 || std::memcmp(sk.pbc, hs.pbc, sizeof(sk.pbc)) != 0;
-  unsigned long long* dm = static_cast<unsigned long long*>(sk.dmax.ensure(sizeof(unsigned long long)));
+  unsigned long long* dm = static_cast<unsigned long long*>(sk.dmax.ensure(2 * sizeof(unsigned long long)));
   if (!rebuild && n > 0) {
-    PFW_CUDA(cudaMemsetAsync(dm, 0, sizeof(unsigned long long), st));
-    k_max_disp<<<std::min(grid_for(n, 256), 1184), 256, 0, st>>>(n, ws->X.as<double>(), sk.Xref.as<double>(), dm);
+    PFW_CUDA(cudaMemsetAsync(dm, 0, 2 * sizeof(unsigned long long), st));
+    k_max_disp<<<std::min(grid_for(n, 256), 1184), 256, 0, st>>>(n, ws->X.as<double>(), sk.Xref.as<double>(),
+                                                                  ws->species.as<int>(), ws->species_limit, dm);
     ws->launches += 1;
-    unsigned long long bits = 0;
-    PFW_CUDA(cudaMemcpyAsync(&bits, dm, sizeof(bits), cudaMemcpyDeviceToHost, st));
+    unsigned long long bits[2] = {0, 0};
+    PFW_CUDA(cudaMemcpyAsync(bits, dm, sizeof(bits), cudaMemcpyDeviceToHost, st));
     PFW_CUDA(cudaStreamSynchronize(st));
+    if (bits[1])
+      throw Error(PFW_EINVAL, "species channel outside the model's channels (must be >= 0 and < " +
+                                  std::to_string(ws->species_limit) + ")");
     double d2;
-    std::memcpy(&d2, &bits, sizeof(d2));
+    std::memcpy(&d2, &bits[0], sizeof(d2));
     if (!(2.0 * std::sqrt(d2) <= ws->skin)) rebuild = true;
   }
   if (rebuild) {

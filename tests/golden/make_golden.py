@@ -65,5 +65,11 @@ def main(ref):
     print("wrote", os.path.join(HERE, "tial_ace.npz"), "frames", len(frames))
 
 
+def reference_dir(arg=None):
+    """The reference checkout: the command-line argument, else $PFW_REFERENCE_DIR,
+    else the mount point this build's container uses."""
+    return arg or os.environ.get("PFW_REFERENCE_DIR") or "/root/reference"
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_dir(sys.argv[1] if len(sys.argv) > 1 else None))

@@ -53,5 +53,11 @@ def main(ref, frames_only=False):
           "products,", model.ndensity, "densities,", model.radial.nchannels, "radial channels")
 
 
+def reference_dir(arg=None):
+    """The reference checkout: the command-line argument, else $PFW_REFERENCE_DIR,
+    else the mount point this build's container uses."""
+    return arg or os.environ.get("PFW_REFERENCE_DIR") or "/root/reference"
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_dir(sys.argv[1] if len(sys.argv) > 1 else None))
