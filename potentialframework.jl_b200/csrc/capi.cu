@@ -182,7 +182,7 @@ void pfw_ws_destroy(pfw_ws* ws) {
   pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
                          &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
                          &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
-                         &ws->minmax, &ws->cellpart, &ws->out_E, &ws->out_F, &ws->out_W, &ws->out_feat, &ws->counters, &ws->red_partial,
+                         &ws->minmax, &ws->cellpart, &ws->out_E, &ws->out_F, &ws->out_W, &ws->out_feat, &ws->counters, &ws->red_partial, &ws->pair_slots,
                          &ws->nb_count, &ws->nb_offsets, &ws->nb_j, &ws->nb_S, &ws->nb_R};
   for (auto* b : bufs) b->release();
   for (auto& e : ws->ev)

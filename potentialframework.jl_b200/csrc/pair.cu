@@ -15,6 +15,7 @@
 #include <cstdint>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "pfw_internal.h"
 #include "pair_math.cuh"
@@ -402,7 +403,9 @@ static void pair_launch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
   double* parts = static_cast<double*>(ws->cellpart.ensure(sizeof(double) * 8 * std::max(ncells, 1)));
   unsigned long long* np = static_cast<unsigned long long*>(ws->counters.ensure(64)) + 4;
   PFW_CUDA(cudaMemsetAsync(np, 0, sizeof(unsigned long long), st));
-  if (F_dev && P.n > 0) PFW_CUDA(cudaMemsetAsync(F_dev, 0, sizeof(double) * 3 * P.n, st));
+  // the half-stencil path folds every atom's force into F (no clear needed)
+  const bool half = pair_half_eligible(P);
+  if (F_dev && P.n > 0 && !(half && prm.want_f)) PFW_CUDA(cudaMemsetAsync(F_dev, 0, sizeof(double) * 3 * P.n, st));
   bool all_shift = true;
   for (auto& g : P.sys)
     if (g.minimum_image && !g.fast_shift) all_shift = false;
@@ -413,7 +416,9 @@ static void pair_launch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
   const int* perm = ws->perm.as<int>();
   double* F = F_dev ? F_dev : static_cast<double*>(ws->out_F.ensure(sizeof(double) * 3 * std::max(P.n, 1)));
   ws->stage_begin(1);
-  if (ncells > 0) {
+  if (half) {
+    pair_half_kernel(ws, prm, parts, np);
+  } else if (ncells > 0) {
     dim3 grid(grid_for(ncells, PAIR_WARPS)), block(PAIR_WARPS * 32);
     bool mixed = ws->opt.precision == PFW_PRECISION_MIXED;
     if (mixed && all_shift) {
@@ -435,6 +440,7 @@ static void pair_launch(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, 
   double* E = E_dev ? E_dev : static_cast<double*>(ws->out_E.ensure(sizeof(double)));
   double* W = W_dev ? W_dev : static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
   ws->stage_begin(2);
+  if (half && prm.want_f) pair_half_fold(ws, F);
   if (per_system) {
     if (P.nsys > 0) {
       k_reduce_systems<<<P.nsys, 128, 0, st>>>(parts, dsys, 8, E_dev, W_dev);
@@ -486,13 +492,23 @@ void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, doubl
   ws->species_limit = m.kind == 0 ? m.nz : INT32_MAX;
   if (!per_system && skin_pair_evaluate(ws, req, E_dev, F_dev, W_dev)) return;
   ws->prep.valid = false;  // evaluate! rebuilds topology on every call
-  // the per-warp candidate lists make shared memory a residency limit: ask
-  // for the largest carveout
-  for (const void* k : {(const void*)k_pair64<0, 0>, (const void*)k_pair64<1, 0>, (const void*)k_pair64<0, 1>,
-                        (const void*)k_pair64<1, 1>, (const void*)k_pair32<0, 0>, (const void*)k_pair32<1, 0>,
-                        (const void*)k_pair32<0, 1>, (const void*)k_pair32<1, 1>}) {
-    PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem_bytes<double>()));
+  // the per-warp traversal state makes shared memory a residency limit: ask
+  // for the largest carveout (once per device)
+  static std::mutex attr_mu;
+  static bool attr_done[64] = {};
+  {
+    std::lock_guard<std::mutex> lock(attr_mu);
+    const int dev = ws->opt.device;
+    if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+      for (const void* k : {(const void*)k_pair64<0, 0>, (const void*)k_pair64<1, 0>, (const void*)k_pair64<0, 1>,
+                            (const void*)k_pair64<1, 1>, (const void*)k_pair32<0, 0>, (const void*)k_pair32<1, 0>,
+                            (const void*)k_pair32<0, 1>, (const void*)k_pair32<1, 1>}) {
+        PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        PFW_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, pair_smem_bytes<double>()));
+      }
+      pair_half_setup();
+      if (dev >= 0 && dev < 64) attr_done[dev] = true;
+    }
   }
   // cell list without a mid-call synchronisation: its input flags are read
   // once at the end (a bad input only makes clamped cells and NaN sums)

@@ -113,6 +113,7 @@ struct pfw_ws {
   // pair evaluation
   pfw::PairModel pair;
   pfw::DevBuf cellpart, out_E, out_F, out_W, out_feat, counters, red_partial, out_design, out_base;
+  pfw::DevBuf pair_slots;  // per-(slot, sorted atom) partial forces of the half-stencil pair kernel
   int64_t last_pairs = -1;
   // neighbour snapshot
   pfw::DevBuf nb_count, nb_offsets, nb_j, nb_S, nb_R;
@@ -159,6 +160,12 @@ void skin_stats(pfw_ws* ws, int64_t* builds, int64_t* reuses);
 // per_system: E[s] and W[9s..] for every system of a batch
 void pair_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double* W_dev, bool per_system = false);
 void pair_graph_free(pfw_ws* ws);
+// pair_half.cu: every unordered pair once (3×3×3 stencils with per-cell shifts)
+struct PairParams;
+bool pair_half_eligible(const Prepared& P);
+void pair_half_setup();
+void pair_half_kernel(pfw_ws* ws, const PairParams& prm, double* parts, unsigned long long* np);
+void pair_half_fold(pfw_ws* ws, double* F);
 // snapshot.cu
 int64_t neighbour_build(pfw_ws* ws, double cutoff, bool with_R = true);
 void neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);
