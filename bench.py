@@ -59,7 +59,7 @@ class Workload:
             self.params = dict(potential="lennard_jones", epsilon=WL.LJ_EPS, sigma=WL.LJ_SIGMA, cutoff=WL.LJ_CUTOFF)
             self.pair = ("lj", (WL.LJ_EPS, WL.LJ_SIGMA), WL.LJ_CUTOFF)
             self.flop_per_pair = 65.0
-            self.kernel = "k_pair64<LJ>"
+            self.kernel = "k_pair_half<LJ, double>"
             self.config = dict(workload=f"lj_fcc{nc}_{len(self.sys)}" + ("_shear0.2" if name == "lj_shear" else "")
                                + ("_skin1.0" if name == "lj_skin" else ""),
                                lattice_a=5.26, displacement_sigma=0.1, **self.params)
@@ -70,7 +70,7 @@ class Workload:
             self.sys = WL.smooth_fcc(seed=1)
             self.pair = ("smooth", WL.SMOOTH_A, WL.SMOOTH_CUTOFF)
             self.flop_per_pair = 52.0
-            self.kernel = "k_pair64<SmoothPair>"
+            self.kernel = "k_pair_half<SmoothPair, double>"
             self.config = dict(workload="smooth_fcc8_2048", potential="SmoothPair", amplitudes=WL.SMOOTH_A.tolist(),
                                cutoff=WL.SMOOTH_CUTOFF, lattice_a=1.6, displacement_sigma=0.05)
         elif name in ("ace", "ace_tial"):
@@ -138,7 +138,8 @@ class Workload:
         s = self.sys
         if self.kind == "pair":
             kind, params, c = self.pair
-            return lambda: O.pair_evaluate(s.X, s.H, s.pbc, s.species, kind, params, c, nthreads=nthreads)
+            O.lib_simd()  # built for this host before timing
+            return lambda: O.pair_evaluate(s.X, s.H, s.pbc, s.species, kind, params, c, nthreads=nthreads, simd=True)
         ace = O.AceOracle(self.ace)
         return lambda: ace.evaluate(s.X, s.H, s.pbc, s.species, nthreads=nthreads)
 
@@ -149,21 +150,6 @@ def measured_peaks():
         d = json.load(open(path))
         return d.get("hbm_gbs", FALLBACK_HBM), "measured"
     return FALLBACK_HBM, "fallback"
-
-
-def profile_traffic(name):
-    """Per-launch DRAM bytes of a kernel from a committed ncu summary line
-    `traffic_bytes_per_launch = N` in profiles/<name>.md (None if absent)."""
-    path = os.path.join(ROOT, "profiles", name + ".md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.strip().startswith("traffic_bytes_per_launch"):
-            try:
-                return float(line.split("=")[1].split()[0])
-            except Exception:
-                return None
-    return None
 
 
 class Clocks:
@@ -304,9 +290,108 @@ def cpu_baseline(w, seconds=12.0, max_reps=20):
         call()
         times.append(time.perf_counter() - t)
     med = statistics.median(times)
-    return dict(value=w.n / med, unit="atoms/s", cores=nthreads, kind="port",
-                sample=f"full {w.n}-atom {w.config['workload']} system, {len(times)} evaluations (median), "
-                       f"restated reference CPU algorithm (oracle/), {nthreads} threads")
+    out = dict(value=w.n / med, unit="atoms/s", cores=nthreads, kind="port",
+               sample=f"full {w.n}-atom {w.config['workload']} system, {len(times)} evaluations (median), "
+                      f"restated reference CPU algorithm (oracle/), {nthreads} threads")
+    out.update(REFERENCE_CPU_NOTE if w.kind == "pair" else {})
+    return out
+
+
+# the reference's own published CPU figure for the same-density argon LJ
+REFERENCE_CPU_NOTE = dict(
+    lanes="W = 4 lanes as SIMD double vectors (-O3 -march=native, no FMA contraction), phase-coloured cell "
+          "tasks on all host threads, serial prepare! (binning, sort, topology, colouring) inside each call",
+    reference_published="about 3.4e6 atoms/s: the reference's public CPU evaluator, width 4, parallel, "
+                        "32 threads on a Ryzen 9 9950X (16 cores), 97,556-atom argon FCC at this density "
+                        "(docs/implementation/GPU-PAIR-RESULTS.md:41)")
+
+
+def oracle_eval(w, nthreads):
+    """FP64 oracle E, F, W of a workload's system (restated reference CPU algorithm)."""
+    from oracle import oracle as O
+    s = w.sys
+    if w.kind == "pair":
+        kind, params, c = w.pair
+        E, F, W, _ = O.pair_evaluate(s.X, s.H, s.pbc, s.species, kind, params, c, nthreads=nthreads)
+        return E, F, W
+    r = O.AceOracle(w.ace).evaluate(s.X, s.H, s.pbc, s.species, nthreads=nthreads)
+    return r["energy"], r["forces"], r["virial"]
+
+
+def errors(res, ref):
+    """Force RMSE / max error, energy and virial error of a GPU result against the oracle."""
+    E, F, W = res
+    Eo, Fo, Wo = ref
+    dF = np.asarray(F).reshape(-1, 3) - np.asarray(Fo).reshape(-1, 3)
+    fs = max(float(np.abs(Fo).max()) if np.size(Fo) else 0.0, 1e-300)
+    return dict(force_rmse=float(np.sqrt(np.mean(dF ** 2))) if dF.size else 0.0,
+                force_max_err=float(np.abs(dF).max()) if dF.size else 0.0,
+                force_max_rel=float(np.abs(dF).max() / fs) if dF.size else 0.0,
+                energy_err=abs(float(E) - float(Eo)), energy_rel=abs(float(E) - float(Eo)) / max(abs(float(Eo)), 1.0),
+                virial_max_err=float(np.abs(np.asarray(W) - np.asarray(Wo)).max()))
+
+
+def cpu_baseline_leg(w, line, outputs, forms_out):
+    """The CPU-baseline leg: the restated reference CPU algorithm (oracle/)
+    timed on the headline workload, then the same oracle, as the checker, on
+    every configuration the GPU evaluated in this run: each GPU result (FP64
+    and mixed) gets its errors against the FP64 oracle (FP64 bar 1e-10
+    relative in forces, mixed bar 1e-3 eV/Å force RMSE), and the batch gets
+    them on a seeded sample of 64 systems that includes the smallest and the
+    largest."""
+    line["cpu_baseline"] = cpu_baseline(w)
+    nthreads = os.cpu_count() or 1
+    parity = {}
+    for name, res in outputs.items():
+        if name == "batch":
+            continue
+        wl = w if name == w.name else Workload(name)
+        t0 = time.perf_counter()
+        ref = oracle_eval(wl, nthreads)
+        entry = dict(oracle_s=time.perf_counter() - t0, atoms=wl.n)
+        for form in ("fp64", "mixed"):
+            if form in res:
+                entry[form] = errors(res[form], ref)
+                key = res.get(form + "_key")
+                if key in forms_out:
+                    forms_out[key]["vs_fp64_oracle"] = entry[form]
+        if "fp64" in entry:
+            entry["fp64_within_1e-10"] = bool(entry["fp64"]["force_max_rel"] <= 1e-10
+                                              and entry["fp64"]["energy_rel"] <= 1e-10)
+        if "mixed" in entry:
+            entry["mixed_within_1e-3_rmse"] = bool(entry["mixed"]["force_rmse"] <= 1e-3)
+        parity[wl.config["workload"]] = entry
+    b = outputs.get("batch")
+    if b:
+        from oracle import oracle as O
+        systems, offs = b["systems"], b["offsets"]
+        sizes = np.array([len(sy) for sy in systems])
+        rng = np.random.default_rng(64)
+        sample = sorted(set(rng.choice(len(systems), 62, replace=False).tolist())
+                        | {int(np.argmin(sizes)), int(np.argmax(sizes))})
+        ace = O.AceOracle(b["model"])
+        worst = {}
+        for sidx in sample:
+            sy = systems[sidx]
+            r = ace.evaluate(sy.X, sy.H, sy.pbc, sy.species)
+            ref = (r["energy"], r["forces"], r["virial"])
+            for form in ("fp64", "mixed"):
+                if form not in b:
+                    continue
+                E, F, W = b[form]
+                e = errors((E[sidx], F[offs[sidx]:offs[sidx + 1]], W[sidx]), ref)
+                acc = worst.setdefault(form, dict(force_rmse=0.0, force_max_err=0.0, force_max_rel=0.0,
+                                                  energy_rel=0.0, virial_max_err=0.0))
+                for k in acc:
+                    acc[k] = max(acc[k], e[k])
+        entry = dict(sample_systems=len(sample), worst_per_system=worst)
+        if "fp64" in worst:
+            entry["fp64_within_1e-10"] = bool(worst["fp64"]["force_max_rel"] <= 1e-10
+                                              and worst["fp64"]["energy_rel"] <= 1e-10)
+        parity["ace_batch4096"] = entry
+        if "ace_batch4096_fp64_graph" in forms_out:
+            forms_out["ace_batch4096_fp64_graph"]["vs_fp64_oracle"] = entry
+    line["parity_vs_oracle"] = parity
 
 
 # ---------------------------------------------------------------------------
@@ -338,19 +423,27 @@ def run_reference(args):
     call = w.cpu_call(nthreads)
     for _ in range(args.warmup):
         call()
+    # every step is one full evaluation; the timed steps stop after about
+    # 90 s so that a long --steps run still ends within a few minutes
     steps = max(args.steps, 1)
     t = time.perf_counter()
-    for _ in range(steps):
+    done = 0
+    while done < steps:
         call()
-    dt = (time.perf_counter() - t) / steps
+        done += 1
+        if time.perf_counter() - t > 90.0:
+            break
+    dt = (time.perf_counter() - t) / done
     v = w.n / dt
     cfg = dict(w.config, atoms=w.n, parallelism="cpu threads",
                note="reference is a Julia package (not installable here); its CPU algorithm restated in oracle/ is timed")
     line = dict(impl="reference", metric=METRIC, value=v, unit="atoms/s", n_gpus=args.gpus, steps=steps,
                 warmup=args.warmup, ms_per_step=dt * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f64", data="synthetic", config=cfg,
+                steps_timed=done,
                 cpu_baseline=dict(value=v, unit="atoms/s", cores=nthreads, kind="port",
-                                  sample=f"full {w.n}-atom system per step"),
+                                  sample=f"full {w.n}-atom system per step, {done} steps timed",
+                                  **(REFERENCE_CPU_NOTE if w.kind == "pair" else {})),
                 e2e=dict(value=v, unit="atoms/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
     return 0
@@ -394,6 +487,7 @@ def run_b200(args):
     value = world * w.n / (ms * 1e-3)
     kern_ms = float(stage[:, 1].mean())
     geom_ms = float(stage[:, 0].mean())
+    red_ms = float(stage[:, 2].mean())
     e2e_s, E_ref, F_ref = e2e_time(h, w, lib, min(max(args.steps // 4, 5), 200))
     if dist:
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
@@ -405,25 +499,23 @@ def run_b200(args):
         fp64_peak = h.probe_fp64()
         cfg = dict(w.config, atoms=w.n, parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                    l2="256 MB flush between steps, outside the per-step events", energy_eV=E_ref)
+        achieved_gbs = 49.0 * w.n / (kern_ms * 1e-3) / 1e9  # X 24 B + species 1 B read, F 24 B written per atom
+        hbm = dict(achieved=achieved_gbs, peak=peak, unit="GB/s", frac=achieved_gbs / peak, peak_source=peak_kind,
+                   algorithmic_bytes_per_launch=49.0 * w.n)
         if w.kind == "pair":
+            # pairs are FP64-pipe bound (arithmetic intensity far above the HBM ridge):
+            # algorithmic flops = in-cutoff unordered pairs x the per-pair count
             npairs = h.pair_count()
-            alg_bytes = 49.0 * w.n  # X 24 B + species 1 B read, F 24 B written per atom
             alg_flops = npairs * w.flop_per_pair
             cfg["unordered_pairs"] = npairs
-            traffic = profile_traffic("pair_lj_fp64") if args.workload == "lj" else None
-        else:
-            alg_bytes = 49.0 * w.n
-            alg_flops = None
-            traffic = profile_traffic("ace_sites_fp64") if args.workload == "ace" else None
-        achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
-        roof = dict(bound="hbm", kernel=w.kernel, achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
-                    peak_source=peak_kind, traffic=traffic, kernel_ms=kern_ms, geometry_ms=geom_ms,
-                    algorithmic_bytes_per_launch=alg_bytes)
-        if alg_flops:
             tf = alg_flops / (kern_ms * 1e-3) / 1e12
-            roof["fp64_pipe"] = dict(achieved_tflops=tf, peak_tflops=fp64_peak, frac=tf / fp64_peak,
-                                     peak_source="measured DFMA probe (pfw_probe_fp64_peak)",
-                                     algorithmic_flops_per_launch=alg_flops)
+            roof = dict(bound="fp64_pipe", kernel=w.kernel, achieved=tf, peak=fp64_peak, unit="TFLOP/s",
+                        frac=tf / fp64_peak, peak_source="measured live: DFMA probe (pfw_probe_fp64_peak) in this run",
+                        traffic=None, kernel_ms=kern_ms, geometry_ms=geom_ms, fold_and_reduce_ms=red_ms,
+                        algorithmic_flops_per_launch=alg_flops, flop_per_pair=w.flop_per_pair, hbm=hbm)
+        else:
+            roof = dict(bound="hbm", kernel=w.kernel, traffic=None, kernel_ms=kern_ms, geometry_ms=geom_ms,
+                        fold_and_reduce_ms=red_ms, **hbm)
         line = dict(
             metric=METRIC, value=value, unit="atoms/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
             ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
@@ -432,10 +524,11 @@ def run_b200(args):
                      h2d_bytes_per_step=28 * w.n, d2h_bytes_per_step=24 * w.n + 8 + 72,
                      api="pfw_set_geometry + pfw_evaluate (host buffers, pinned)"),
             gpu_launches=launches, clocks=clk)
+        outputs = {w.name: dict(fp64=h.evaluate(w.model_sel, 7), fp64_key="headline", headline_ms=ms)}
         if not args.no_forms and world == 1:  # single-GPU configurations; the other ranks would idle at a barrier
-            line["forms"] = forms(args, dev, stream, flush, F_ref)
+            line["forms"] = forms(args, dev, stream, flush, F_ref, outputs)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(w)
+            cpu_baseline_leg(w, line, outputs, line.get("forms", {}))
     h.close()
     if dist:
         dist.barrier()
@@ -445,12 +538,18 @@ def run_b200(args):
     return 0
 
 
-def forms(args, dev, stream, flush, F_head):
-    """The other configurations (plain FP64) and the mixed form, each timed with
-    a few device steps; reduced-precision forms report errors vs plain FP64."""
+MIXED_WORKLOADS = ("lj", "lj1m", "lj_shear", "smooth", "ace")
+
+
+def forms(args, dev, stream, flush, F_head, outputs):
+    """The other configurations (plain FP64) and the mixed form of every pair
+    and ACE configuration, each timed with a few device steps.  The E/F/W of
+    every evaluation are kept in `outputs` for the CPU-baseline leg, which
+    runs the FP64 oracle on the same systems and attaches the errors."""
     from pfw_b200 import lib
     out = {}
     steps = 10
+    fp64_ms = {}
     for name in ("lj1m", "lj_shear", "smooth", "ace", "ace_tial", "ace_may30"):
         if name == args.workload:
             continue
@@ -465,35 +564,37 @@ def forms(args, dev, stream, flush, F_head):
         w.tune(h)
         ms, stage, _ = time_device(h, w, dev, lib, steps, 3, flush, stream)
         ms = float(np.mean(ms))
-        out[w.config["workload"] + "_fp64"] = dict(value=w.n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms,
-                                                   kernel_ms=float(stage[:, 1].mean()))
+        key = w.config["workload"] + "_fp64"
+        fp64_ms[name] = ms
+        out[key] = dict(value=w.n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms, kernel_ms=float(stage[:, 1].mean()))
         if "schedule" in w.config:
-            out[w.config["workload"] + "_fp64"]["schedule"] = w.config["schedule"]
+            out[key]["schedule"] = w.config["schedule"]
+        h.set_geometry(w.sys.X, w.sys.H, w.sys.pbc, w.sys.species)
+        outputs[name] = dict(fp64=h.evaluate(w.model_sel, 7), fp64_key=key)
         h.close()
-    out["lj_fcc40_256000_skin1.0_md"] = skin_form(dev, stream, flush)
-    out["ace_batch4096_fp64_graph"] = batch_form(dev, stream, flush)
-    out["surrogate_b2_80_1024000"] = surrogate_form(dev, stream, flush)
-    out["ace_design_rows_1024"] = design_form(dev, stream, flush)
-    for name in ("lj", "ace"):
+    for name in MIXED_WORKLOADS:
         w = Workload(name)
-        h64 = lib.Handle(lib.FP64, device=dev.index)
-        h64.set_geometry(w.sys.X, w.sys.H, w.sys.pbc, w.sys.species)
-        w.bind(h64)
-        E64, F64, W64 = h64.evaluate(w.model_sel, 7)
-        h64.close()
+        if name == args.workload:
+            fp64_ms[name] = outputs[name]["headline_ms"]
         h32 = lib.Handle(lib.MIXED, device=dev.index)
         h32.check(h32.L.pfw_set_stream(h32.ws, ctypes.c_void_p(stream.cuda_stream)))
         w.bind(h32)
-        h32.set_geometry(w.sys.X, w.sys.H, w.sys.pbc, w.sys.species)
-        E32, F32, W32 = h32.evaluate(w.model_sel, 7)
+        w.tune(h32)
         ms, stage, _ = time_device(h32, w, dev, lib, steps, 3, flush, stream)
         ms = float(np.mean(ms))
-        out[w.config["workload"] + "_mixed"] = dict(
-            value=w.n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms, kernel_ms=float(stage[:, 1].mean()),
-            force_rmse=float(np.sqrt(np.mean((F32 - F64) ** 2))), force_max_err=float(np.abs(F32 - F64).max()),
-            energy_err=abs(E32 - E64), virial_max_err=float(np.abs(W32 - W64).max()),
-            note="FP32 arithmetic, FP64 wrap/shift and FP64 (Kahan) energy/virial accumulation; errors vs plain FP64")
+        key = w.config["workload"] + "_mixed"
+        out[key] = dict(value=w.n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms, kernel_ms=float(stage[:, 1].mean()),
+                        speedup_vs_fp64=fp64_ms[name] / ms if name in fp64_ms else None,
+                        note="FP32 pair/ACE arithmetic; FP64 wrap/shift, exact FP64 cutoff re-test in the "
+                             "FP32 guard band, Kahan FP64 energy/virial; errors against the FP64 oracle")
+        h32.set_geometry(w.sys.X, w.sys.H, w.sys.pbc, w.sys.species)
+        outputs.setdefault(name, {})["mixed"] = h32.evaluate(w.model_sel, 7)
+        outputs[name]["mixed_key"] = key
         h32.close()
+    out["lj_fcc40_256000_skin1.0_md"] = skin_form(dev, stream, flush)
+    out["ace_batch4096_fp64_graph"] = batch_form(dev, stream, flush, outputs)
+    out["surrogate_b2_80_1024000"] = surrogate_form(dev, stream, flush)
+    out["ace_design_rows_1024"] = design_form(dev, stream, flush)
     return out
 
 
@@ -541,12 +642,13 @@ def skin_form(dev, stream, flush, steps=50, skin=1.0):
                 list_reuses=reuses, note="Verlet skin reuse (pfw_pair_set_skin); positions move 0.002 Å/step")
 
 
-def batch_form(dev, stream, flush, nsys=4096, steps=20):
+def batch_form(dev, stream, flush, outputs, nsys=4096, steps=20):
     """4096 independent triclinic systems (n log-uniform on [8, 256]) with the
     synthetic ACE model: per-system E, F, W and energy-row fitting features.
     Timed as CUDA-graph replays (cell lists, environments, site kernel, force
-    gather, per-system outputs) and as eager batch calls; a sample of systems
-    is compared with single-system FP64 evaluations."""
+    gather, per-system outputs) and as eager batch calls, in FP64 and in the
+    mixed form (graph replay); the per-system results go to the CPU-baseline
+    leg, which checks a sample against the FP64 oracle."""
     import torch
 
     from pfw_b200 import ace_generate as G
@@ -555,71 +657,66 @@ def batch_form(dev, stream, flush, nsys=4096, steps=20):
     from pfw_b200.ace_model import read_resolved
     model = read_resolved(G.generate_b2_model())
     systems = WL.batched(seed=5, nsys=nsys)
-    h = lib.Handle(lib.FP64, device=dev.index)
-    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
-    h.ace(model)
-    h.set_batch(systems)
-    n, nfeat = h.n, h.feature_count()
-    E = torch.zeros(nsys, dtype=torch.float64, device=dev)
-    F = torch.zeros(3 * n, dtype=torch.float64, device=dev)
-    W = torch.zeros(9 * nsys, dtype=torch.float64, device=dev)
-    X = torch.zeros(nsys * nfeat, dtype=torch.float64, device=dev)
-    ptrs = [ctypes.c_void_p(t.data_ptr()) for t in (E, F, W, X)]
-    torch.cuda.synchronize()
-
-    from pfw_b200 import autotune
-
-    def eager_sync():
-        h.evaluate_batch_device(lib.MODEL_ACE, 7, *ptrs)
-
-    c, g, tuned = autotune.tune(h, model, eager_sync, n, nsys,
-                                path=os.path.join(tempfile.gettempdir(), "pfw_b200_bench_autotune.json"))
-
-    def replay():
-        h.batch_graph_launch(7, *ptrs)
-
-    def eager():
-        h.evaluate_batch_device(lib.MODEL_ACE, 7, *ptrs)
-
-    res = {}
-    for label, fn in (("graph", replay), ("eager", eager)):
-        for _ in range(3):
-            fn()
-        h.batch_graph_sync()
-        st = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-        en = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-        l0 = h.launches
-        for k in range(steps):
-            flush.zero_()
-            st[k].record(stream)
-            fn()
-            en[k].record(stream)
+    res, result, tuned_sched = {}, {}, None
+    for prec in (lib.FP64, lib.MIXED):
+        h = lib.Handle(prec, device=dev.index)
+        h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+        h.ace(model)
+        h.set_batch(systems)
+        n, nfeat = h.n, h.feature_count()
+        E = torch.zeros(nsys, dtype=torch.float64, device=dev)
+        F = torch.zeros(3 * n, dtype=torch.float64, device=dev)
+        W = torch.zeros(9 * nsys, dtype=torch.float64, device=dev)
+        X = torch.zeros(nsys * nfeat, dtype=torch.float64, device=dev)
+        ptrs = [ctypes.c_void_p(t.data_ptr()) for t in (E, F, W, X)]
         torch.cuda.synchronize()
-        h.batch_graph_sync()
-        ms = float(np.mean([a.elapsed_time(b) for a, b in zip(st, en)]))
-        res[label] = dict(ms=ms, launches_per_step=(h.launches - l0) / steps)
-    Eb = E.cpu().numpy()
-    Fb = F.cpu().numpy().reshape(-1, 3)
-    offs = h.batch_offsets
-    h1 = lib.Handle(lib.FP64, device=dev.index)
-    h1.ace(model)
-    err_e = err_f = 0.0
-    for s in range(0, nsys, nsys // 32):
-        sy = systems[s]
-        h1.set_geometry(sy.X, sy.H, sy.pbc, sy.species)
-        e1, f1, _ = h1.evaluate(lib.MODEL_ACE, 7)
-        err_e = max(err_e, abs(e1 - Eb[s]))
-        err_f = max(err_f, float(np.abs(f1 - Fb[offs[s]:offs[s + 1]]).max()))
-    h1.close()
-    h.close()
-    ms = res["graph"]["ms"]
+
+        from pfw_b200 import autotune
+
+        def eager():
+            h.evaluate_batch_device(lib.MODEL_ACE, 7, *ptrs)
+
+        c, g, tuned = autotune.tune(h, model, eager, n, nsys,
+                                    path=os.path.join(tempfile.gettempdir(), "pfw_b200_bench_autotune.json"))
+        if prec == lib.FP64:
+            tuned_sched = dict(chunk=c, groups=g, tuned_ms={k: round(v, 2) for k, v in tuned.items()})
+
+        def replay():
+            h.batch_graph_launch(7, *ptrs)
+
+        runs = (("graph", replay), ("eager", eager)) if prec == lib.FP64 else (("graph", replay),)
+        for label, fn in runs:
+            for _ in range(3):
+                fn()
+            h.batch_graph_sync()
+            st = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+            en = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+            l0 = h.launches
+            for k in range(steps):
+                flush.zero_()
+                st[k].record(stream)
+                fn()
+                en[k].record(stream)
+            torch.cuda.synchronize()
+            h.batch_graph_sync()
+            ms = float(np.mean([a.elapsed_time(b) for a, b in zip(st, en)]))
+            res[(prec, label)] = dict(ms=ms, launches_per_step=(h.launches - l0) / steps)
+        result["fp64" if prec == lib.FP64 else "mixed"] = (E.cpu().numpy(), F.cpu().numpy().reshape(-1, 3),
+                                                           W.cpu().numpy().reshape(nsys, 3, 3).transpose(0, 2, 1))  # column-major 3x3 per system
+        offs = h.batch_offsets
+        h.close()
+    outputs["batch"] = dict(systems=systems, offsets=offs, model=model, **result)
+    ms = res[(lib.FP64, "graph")]["ms"]
+    ms_mixed = res[(lib.MIXED, "graph")]["ms"]
     return dict(value=n / (ms * 1e-3), unit="atoms/s", ms_per_step=ms, systems=nsys, atoms=n,
-                eager_ms_per_step=res["eager"]["ms"], eager_value=n / (res["eager"]["ms"] * 1e-3),
-                kernels_per_replay=res["graph"]["launches_per_step"], features_per_system=nfeat,
-                schedule=dict(chunk=c, groups=g, tuned_ms={k: round(v, 2) for k, v in tuned.items()}),
-                max_abs_err_vs_single_system=dict(energy=err_e, force=err_f, sample=32),
+                eager_ms_per_step=res[(lib.FP64, "eager")]["ms"],
+                eager_value=n / (res[(lib.FP64, "eager")]["ms"] * 1e-3),
+                kernels_per_replay=res[(lib.FP64, "graph")]["launches_per_step"], features_per_system=nfeat,
+                schedule=tuned_sched,
+                mixed=dict(value=n / (ms_mixed * 1e-3), unit="atoms/s", ms_per_step=ms_mixed,
+                           speedup_vs_fp64=ms / ms_mixed),
                 note="n log-uniform [8,256], triclinic lengths U[6,14] Å, angles U[70,110]°, hard core 1.6 Å, "
-                     "n/V <= 0.11 Å^-3 (cells redrawn), species 50/50; synthetic ACE model; FP64")
+                     "n/V <= 0.11 Å^-3 (cells redrawn), species 50/50; synthetic ACE model; FP64 and mixed")
 
 
 def design_form(dev, stream, flush, nsys=1024, steps=5):

@@ -22,29 +22,51 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+_simd = None
+
+
+def lib_simd():
+    """The timed CPU baseline's build (-O3 -march=native, SIMD lanes), compiled
+    for this host on first use into a temporary directory (never shipped: the
+    instruction set must be the running machine's)."""
+    global _simd
+    if _simd is None:
+        import tempfile
+        out = os.path.join(tempfile.gettempdir(), f"pfw_oracle_simd_{os.uname().nodename}_{os.getpid()}.so")
+        flags = ["-O3", "-march=native", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread", "-shared"]
+        subprocess.run([os.environ.get("CXX", "g++"), *flags, "-o", out, os.path.join(HERE, "pfw_oracle.cpp")],
+                       check=True, capture_output=True)
+        _simd = _bind(C.CDLL(out))
+    return _simd
+
+
 def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB):
             build()
-        L = C.CDLL(LIB)
-        dp, ip, i32p, u8p = C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_uint8)
-        L.pfo_last_error.restype = C.c_char_p
-        L.pfo_pair_evaluate.argtypes = [C.c_int64, dp, dp, u8p, i32p, C.c_int32, C.c_int32, dp, C.c_double,
-                                        C.c_int32, C.c_int32, C.c_uint32, C.c_int32, dp, dp, dp, ip]
-        L.pfo_neighbour_list.argtypes = [C.c_int64, dp, dp, u8p, C.c_double, C.c_int32, C.c_int64, ip, i32p,
-                                         i32p, dp, ip]
-        L.pfo_ace_model_create.restype = C.c_void_p
-        L.pfo_ace_model_create.argtypes = [C.c_void_p]
-        L.pfo_ace_model_destroy.argtypes = [C.c_void_p]
-        L.pfo_ace_evaluate.argtypes = [C.c_void_p, C.c_int64, dp, dp, u8p, i32p, C.c_int32, C.c_uint32, C.c_int32,
-                                       dp, dp, dp, dp, dp]
-        L.pfo_ace_set_scales.argtypes = [C.c_void_p, dp, dp]
-        L.pfo_radial_ed.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, dp, dp]
-        L.pfo_angular_ed.argtypes = [C.c_int32, dp, dp, dp]
-        L.pfo_solid_ed.argtypes = [C.c_int32, dp, dp, dp]
-        _lib = L
+        _lib = _bind(C.CDLL(LIB))
     return _lib
+
+
+def _bind(L):
+    """Argument and result types of the oracle's C entry points."""
+    dp, ip, i32p, u8p = C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_uint8)
+    L.pfo_last_error.restype = C.c_char_p
+    L.pfo_pair_evaluate.argtypes = [C.c_int64, dp, dp, u8p, i32p, C.c_int32, C.c_int32, dp, C.c_double,
+                                    C.c_int32, C.c_int32, C.c_uint32, C.c_int32, dp, dp, dp, ip]
+    L.pfo_neighbour_list.argtypes = [C.c_int64, dp, dp, u8p, C.c_double, C.c_int32, C.c_int64, ip, i32p,
+                                     i32p, dp, ip]
+    L.pfo_ace_model_create.restype = C.c_void_p
+    L.pfo_ace_model_create.argtypes = [C.c_void_p]
+    L.pfo_ace_model_destroy.argtypes = [C.c_void_p]
+    L.pfo_ace_evaluate.argtypes = [C.c_void_p, C.c_int64, dp, dp, u8p, i32p, C.c_int32, C.c_uint32, C.c_int32,
+                                   dp, dp, dp, dp, dp]
+    L.pfo_ace_set_scales.argtypes = [C.c_void_p, dp, dp]
+    L.pfo_radial_ed.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_double, dp, dp]
+    L.pfo_angular_ed.argtypes = [C.c_int32, dp, dp, dp]
+    L.pfo_solid_ed.argtypes = [C.c_int32, dp, dp, dp]
+    return L
 
 
 class OracleError(RuntimeError):
@@ -71,11 +93,12 @@ def _geom(X, H, pbc, species):
 
 
 def pair_evaluate(X, H, pbc, species, kind, params, cutoff, *, width=4, brute_threshold=32,
-                  request=7, nthreads=1):
+                  request=7, nthreads=1, simd=False):
     """Restated evaluate!(Workspace(width, bruteforce_threshold), sys, p; request).
 
     X: (n,3) positions, H: 3×3 with columns = cell vectors, kind 'smooth'
     (params = symmetric nz×nz amplitudes) or 'lj' (params = (eps, sigma)).
+    simd: the timed-baseline build with the W = 4 lanes as SIMD vectors.
     Returns (E, F (n,3), W (3,3), npairs)."""
     X, Hf, pbc, sp = _geom(X, H, pbc, species)
     n = X.shape[0]
@@ -91,8 +114,9 @@ def pair_evaluate(X, H, pbc, species, kind, params, cutoff, *, width=4, brute_th
     F = np.zeros((n, 3))
     W = np.zeros(9)
     npairs = np.zeros(1, np.int64)
-    _check(lib().pfo_pair_evaluate(n, _p(X, C.c_double), _p(Hf, C.c_double), _p(pbc, C.c_uint8),
-                                   _p(sp, C.c_int32), k, nz, _p(A, C.c_double), float(cutoff), width,
+    L = lib_simd() if simd else lib()
+    _check(L.pfo_pair_evaluate(n, _p(X, C.c_double), _p(Hf, C.c_double), _p(pbc, C.c_uint8),
+                                   _p(sp, C.c_int32), k, nz, _p(A, C.c_double), float(cutoff), -4 if simd else width,
                                    brute_threshold, request, nthreads, _p(E, C.c_double), _p(F, C.c_double),
                                    _p(W, C.c_double), _p(npairs, C.c_int64)))
     return float(E[0]), F, W.reshape(3, 3, order="F"), int(npairs[0])

@@ -522,6 +522,118 @@ static void cell_task(const Prepared& w, const PairModel& m, uint32_t req, int64
   for (int k = 0; k < 9; ++k) vir[k] = v[k];
 }
 
+// cell_task! again, with the W = 4 lanes as one SIMD vector of doubles (the
+// reference's SIMD.jl Vec{4} lanes, geometry.jl:9-27): geometry, cutoff mask,
+// safe geometry, pair function and gradient lane-parallel; lane sums and the
+// per-lane force scatter in lane order as execution.jl:189-209.  Only the
+// timed CPU baseline uses it (the checker runs the scalar cell_task).
+typedef double v4d __attribute__((vector_size(32)));
+
+static inline double lane_sum(v4d v) { return ((v[0] + v[1]) + v[2]) + v[3]; }
+
+static void cell_task_simd(const Prepared& w, const PairModel& m, uint32_t req, int64_t task,
+                           std::vector<double>& force, double& e_out, double vir[9], int64_t& npairs) {
+  constexpr int W = 4;
+  double e = 0;
+  double v[9] = {0};
+  const bool wantE = req & PFW_REQ_ENERGY, wantF = req & PFW_REQ_FORCES, wantV = req & PFW_REQ_VIRIAL;
+  const double c2 = w.c * w.c;
+  const double invc2 = 1.0 / (m.cutoff * m.cutoff);
+  double qc = 0;
+  if (m.kind == 1) {
+    const double rc = m.sigma / m.cutoff, qc2 = rc * rc;
+    qc = qc2 * qc2 * qc2;
+  }
+  auto [first_i, last_i] = w.ranges[task];
+  for (int64_t i = first_i; i <= last_i; ++i) {
+    double central[3] = {0, 0, 0};
+    const double xi = w.x[i], yi = w.y[i], zi = w.z[i];
+    for (const auto& img : w.images[task]) {
+      auto [rf, rl] = w.ranges[img.cell];
+      const int64_t lo = std::max(rf, i + (img.self ? 0 : 1));
+      for (int64_t j = lo; j <= rl; j += W) {
+        int64_t js[W];
+        v4d dx, dy, dz, structural;
+        for (int k = 0; k < W; ++k) {
+          js[k] = std::min(j + k, rl);
+          structural[k] = ((j + k <= rl) && (js[k] > i || (img.self && js[k] == i))) ? 1.0 : 0.0;
+          dx[k] = w.x[js[k]] - xi;
+          dy[k] = w.y[js[k]] - yi;
+          dz[k] = w.z[js[k]] - zi;
+        }
+        if (w.minimum_image) {
+          v4d* dd[3] = {&dx, &dy, &dz};
+          for (int a = 0; a < 3; ++a)
+            if (w.pbc[a]) {
+              v4d q = *dd[a] / w.L[a];
+              for (int k = 0; k < W; ++k) q[k] = __builtin_roundeven(q[k]);
+              *dd[a] = *dd[a] - q * w.L[a];
+            }
+        } else {
+          dx = dx + img.shift[0];
+          dy = dy + img.shift[1];
+          dz = dz + img.shift[2];
+        }
+        v4d r2 = dx * dx;
+        r2 = r2 + dy * dy;
+        r2 = r2 + dz * dz;
+        const auto act = (r2 < c2) & (structural != 0.0);
+        if (!(act[0] | act[1] | act[2] | act[3])) continue;
+        // safe geometry before the pair function (geometry.jl:21-27)
+        const v4d one = {1.0, 1.0, 1.0, 1.0}, zero = {0.0, 0.0, 0.0, 0.0};
+        dx = act ? dx : one;
+        dy = act ? dy : zero;
+        dz = act ? dz : zero;
+        v4d r = dx * dx;
+        r = r + dy * dy;
+        r = r + dz * dz;
+        for (int k = 0; k < W; ++k) r[k] = std::sqrt(r[k]);
+        v4d en, dedr;
+        if (m.kind == 0) {
+          v4d a;
+          for (int k = 0; k < W; ++k) a[k] = m.A[w.species[i] * m.nz + w.species[js[k]]];
+          const v4d q = 1.0 - r * r * invc2;
+          en = a * q * q * q;
+          dedr = -6.0 * a * q * q * invc2 * r;
+        } else {
+          const v4d ratio = m.sigma / r, ratio2 = ratio * ratio, q = ratio2 * ratio2 * ratio2;
+          en = 4.0 * m.eps * (q * q - q - qc * qc + qc);
+          dedr = 24.0 * m.eps * (q - 2.0 * q * q) / r;
+        }
+        en = act ? en : zero;
+        const v4d coef = dedr / (r > 0.0 ? r : one);
+        v4d gx = coef * dx, gy = coef * dy, gz = coef * dz;
+        gx = act ? gx : zero;
+        gy = act ? gy : zero;
+        gz = act ? gz : zero;
+        for (int k = 0; k < W; ++k) npairs += act[k] ? 1 : 0;
+        if (wantE) e += lane_sum(en);
+        if (wantF) {
+          central[0] += lane_sum(gx);
+          central[1] += lane_sum(gy);
+          central[2] += lane_sum(gz);
+          for (int k = 0; k < W; ++k) {
+            if (!act[k]) continue;
+            force[3 * js[k]] -= gx[k];
+            force[3 * js[k] + 1] -= gy[k];
+            force[3 * js[k] + 2] -= gz[k];
+          }
+        }
+        if (wantV) {
+          const v4d* d[3] = {&dx, &dy, &dz};
+          const v4d* g[3] = {&gx, &gy, &gz};
+          for (int b = 0; b < 3; ++b)
+            for (int a = 0; a < 3; ++a) v[a + 3 * b] -= lane_sum((*d[a]) * (*g[b]));
+        }
+      }
+    }
+    if (wantF)
+      for (int a = 0; a < 3; ++a) force[3 * i + a] += central[a];
+  }
+  e_out = e;
+  for (int k = 0; k < 9; ++k) vir[k] = v[k];
+}
+
 // ---------------------------------------------------------------------------
 // Neighbour snapshot (NeighbourList/interface.jl:85-143)
 // ---------------------------------------------------------------------------
@@ -979,16 +1091,17 @@ int pfo_pair_evaluate(int64_t n, const double* X, const double* H, const uint8_t
   int64_t ncell = (int64_t)w.keys.size();
   std::vector<double> force(3 * n, 0.0), energies(ncell, 0.0), virials(9 * ncell, 0.0);
   std::vector<int64_t> counts(ncell, 0);
+  // width -4: the W = 4 lanes as SIMD vectors (cell_task_simd), else scalar lanes
+  const bool simd = width == -4;
   int Wd = width > 0 ? width : 4;
+  auto task = [&](int64_t t) {
+    if (simd) cell_task_simd(w, m, request, t, force, energies[t], &virials[9 * t], counts[t]);
+    else cell_task(w, m, request, t, Wd, force, energies[t], &virials[9 * t], counts[t]);
+  };
   if (nthreads <= 1) {
-    for (int64_t t = 0; t < ncell; ++t)
-      cell_task(w, m, request, t, Wd, force, energies[t], &virials[9 * t], counts[t]);
+    for (int64_t t = 0; t < ncell; ++t) task(t);
   } else {
-    for (auto& phase : w.phases)
-      parallel_for(nthreads, (int64_t)phase.size(), [&](int64_t k) {
-        int64_t t = phase[k];
-        cell_task(w, m, request, t, Wd, force, energies[t], &virials[9 * t], counts[t]);
-      });
+    for (auto& phase : w.phases) parallel_for(nthreads, (int64_t)phase.size(), [&](int64_t k) { task(phase[k]); });
   }
   // outputs (evaluation.jl:8-25)
   if (E) {
