@@ -316,6 +316,32 @@ pfw_status pfw_mlp_train(pfw_ws* ws, const pfw_mlp_shape* shape, float* params, 
                          const float* y, const int32_t* species, const pfw_mlp_train_options* options,
                          float* epoch_loss);
 
+/* Energy + force training (feature_energy.jl:1-86 is the reference's CPU
+ * analogue of the head; the force term has no counterpart there).  One
+ * full-batch step over n samples on DEVICE buffers: X n × nin standardised
+ * features, y n standardised energy targets, V [members][n][nin] the force
+ * error of each member pulled back into standardised feature space (the
+ * change of each site's features along ΔF; NULL: energy only), c [n] the
+ * force weight of each sample; species is a HOST array.  The loss gradient
+ * is wE·(energy MSE gradient) + Σ c·∂/∂θ(V·∇_x y) per (species, member)
+ * model.  With grad_dev NULL it applies an Adam step (learning rate lr, step
+ * number >= 1, moments m1/m2 like params); else it writes the gradient there
+ * and leaves the parameters alone.  loss [nz·members] (host, may be NULL):
+ * the energy MSE per model before the step. */
+pfw_status pfw_mlp_ef_step(pfw_ws* ws, const pfw_mlp_shape* shape, float* params_dev, float* m1_dev, float* m2_dev,
+                           int64_t n, const float* X_dev, const float* y_dev, const int32_t* species,
+                           const float* V_dev, const float* c_dev, float wE, float lr, int64_t step, float* grad_dev,
+                           double* loss);
+/* ∂y/∂x (standardised) of every member at every sample: G_dev [members][n][nin]
+ * (device), species a host array. */
+pfw_status pfw_mlp_input_grad(pfw_ws* ws, const pfw_mlp_shape* shape, const float* params_dev, int64_t n,
+                              const float* X_dev, const int32_t* species, float* G_dev);
+/* Forces F_dev (3×n, original order, device) of the per-site feature
+ * gradient field dEdx_dev (n × nin dE_i/dfeature_i, original order, device)
+ * through the loaded surrogate feature model on the current geometry:
+ * F_k = -Σ_i dEdx_i·∂feature_i/∂r_k (the surrogate's pullback pass). */
+pfw_status pfw_surrogate_pullback(pfw_ws* ws, const double* dEdx_dev, double* F_dev);
+
 /* ---- device peak probe ------------------------------------------------- */
 /* Measured FP64 FMA throughput of the current device (TFLOP/s), used as the
  * FP64-pipe roofline denominator. */

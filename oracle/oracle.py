@@ -33,7 +33,7 @@ def lib_simd():
     if _simd is None:
         import tempfile
         out = os.path.join(tempfile.gettempdir(), f"pfw_oracle_simd_{os.uname().nodename}_{os.getpid()}.so")
-        flags = ["-O3", "-march=native", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread", "-shared"]
+        flags = ["-O3", "-march=native", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread", "-Wno-psabi", "-shared"]
         subprocess.run([os.environ.get("CXX", "g++"), *flags, "-o", out, os.path.join(HERE, "pfw_oracle.cpp")],
                        check=True, capture_output=True)
         _simd = _bind(C.CDLL(out))

@@ -1354,6 +1354,44 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   ace_check(ws, a);
 }
 
+// site_df[s] = dEdx[perm[s]] (sorted order), site energies zero.
+__global__ void k_gather_site_df(int n, int w, const double* __restrict__ dEdx, const int* __restrict__ perm,
+                                 double* __restrict__ site_df, double* __restrict__ site_e) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n * w) return;
+  const int s = k / w, i = k - s * w;
+  site_df[k] = dEdx[(size_t)perm[s] * w + i];
+  if (i == 0) site_e[s] = 0.0;
+}
+
+// Forces of a per-site dE/dfeature field through the feature model: the
+// feature pass (A-basis of the current geometry), then the surrogate's
+// pullback pass with the given field and the reverse-edge force gather.
+void sur_pullback(pfw_ws* ws, const double* dEdx_dev, double* F_dev) {
+  SurDevice* d = ws->sur;
+  if (!d) throw Error(PFW_ESTATE, "no surrogate feature model loaded");
+  if (!dEdx_dev || !F_dev) throw Error(PFW_EINVAL, "feature gradients and force output required");
+  if (ws->opt.precision != PFW_PRECISION_FP64) throw Error(PFW_EINVAL, "the surrogate path runs in the FP64 workspace");
+  check_species(ws, d->nz, "feature model has no element channel for a species");
+  sur_prepare(ws, d);
+  AceDevice* a = d->fm;
+  const int n = ws->prep.n;
+  cudaStream_t st = ws->stream;
+  SiteLaunch s = sur_launch(ws, d, n, false);
+  sur_feature_pass(ws, d, s);
+  if (n > 0) {
+    k_gather_site_df<<<grid_for((int64_t)n * d->nin, 256), 256, 0, st>>>(n, d->nin, dEdx_dev, ws->perm.as<int>(),
+                                                                          s.sur.site_df, s.sur.site_e);
+    s.want_grad = true;
+    const AceTables p = tables_of(a);
+    dispatch_sites<double, 2>(a->lmax, p, choose_sur_layout(p, ws->opt.device, 2), s, st, ws->opt.device);
+    k_ace_gather<<<grid_for(n, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(),
+                                                   a->edge_g.as<double>(), ws->perm.as<int>(), F_dev);
+    ws->launches += 3;
+  }
+  ace_check(ws, a);
+}
+
 void sur_stats(pfw_ws* ws, int64_t* fallback, int64_t* sites) {
   SurDevice* d = ws->sur;
   if (!d) throw Error(PFW_ESTATE, "no surrogate loaded");

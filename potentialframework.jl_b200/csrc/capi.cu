@@ -179,6 +179,7 @@ void pfw_ws_destroy(pfw_ws* ws) {
   pfw::sur_free(ws);
   pfw::skin_free(ws);
   pfw::pair_graph_free(ws);
+  pfw::mlp_scratch_free(ws);
   pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
                          &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
                          &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
@@ -457,6 +458,25 @@ pfw_status pfw_surrogate_stats(pfw_ws* ws, int64_t* fallback_sites, int64_t* sit
 pfw_status pfw_mlp_param_grad(pfw_ws* ws, const pfw_mlp_shape* shape, const float* params, int64_t n, const float* X,
                               const float* y, const int32_t* species, double* loss, float* grad) {
   return guarded(ws, [&] { pfw::mlp_param_grad(ws, shape, params, n, X, y, species, loss, grad); });
+}
+
+pfw_status pfw_mlp_ef_step(pfw_ws* ws, const pfw_mlp_shape* shape, float* params_dev, float* m1_dev, float* m2_dev,
+                           int64_t n, const float* X_dev, const float* y_dev, const int32_t* species,
+                           const float* V_dev, const float* c_dev, float wE, float lr, int64_t step, float* grad_dev,
+                           double* loss) {
+  return guarded(ws, [&] {
+    pfw::mlp_ef_step(ws, shape, params_dev, m1_dev, m2_dev, n, X_dev, y_dev, species, V_dev, c_dev, wE, lr, step,
+                     grad_dev, loss);
+  });
+}
+
+pfw_status pfw_mlp_input_grad(pfw_ws* ws, const pfw_mlp_shape* shape, const float* params_dev, int64_t n,
+                              const float* X_dev, const int32_t* species, float* G_dev) {
+  return guarded(ws, [&] { pfw::mlp_input_grad(ws, shape, params_dev, n, X_dev, species, G_dev); });
+}
+
+pfw_status pfw_surrogate_pullback(pfw_ws* ws, const double* dEdx_dev, double* F_dev) {
+  return guarded(ws, [&] { pfw::sur_pullback(ws, dEdx_dev, F_dev); });
 }
 
 pfw_status pfw_mlp_train(pfw_ws* ws, const pfw_mlp_shape* shape, float* params, int64_t n, const float* X,

@@ -85,6 +85,7 @@ struct AceDevice;  // ace.cu
 struct SurDevice;  // ace.cu (surrogate)
 struct SkinState;  // skin.cu
 struct PairGraph;  // pair.cu
+struct MlpScratch;  // mlp.cu
 
 }  // namespace pfw
 
@@ -104,6 +105,7 @@ struct pfw_ws {
   double skin = 0.0;              // pair neighbour-list skin (Å); 0: rebuild every call
   pfw::SkinState* skin_state = nullptr;
   pfw::PairGraph* pair_graph = nullptr;  // captured single-system pair evaluation
+  pfw::MlpScratch* mlp_scratch = nullptr;  // device scratch of the MLP training steps
   uint64_t model_version = 0;            // bumped by every pair-model change
   pfw::DevBuf X, species, atom_sys;  // X: 3n doubles
   // prepared geometry
@@ -197,6 +199,15 @@ void mlp_param_grad(pfw_ws* ws, const pfw_mlp_shape* shape, const float* params,
                     const float* y, const int32_t* species, double* loss, float* grad);
 void mlp_train(pfw_ws* ws, const pfw_mlp_shape* shape, float* params, int64_t n, const float* X, const float* y,
                const int32_t* species, const pfw_mlp_train_options* opt, float* epoch_loss);
+// mlp.cu: energy + force training steps on device buffers
+void mlp_ef_step(pfw_ws* ws, const pfw_mlp_shape* shape, float* params_dev, float* m1_dev, float* m2_dev, int64_t n,
+                 const float* X_dev, const float* y_dev, const int32_t* species, const float* V_dev,
+                 const float* c_dev, float wE, float lr, int64_t step, float* grad_dev, double* loss);
+void mlp_input_grad(pfw_ws* ws, const pfw_mlp_shape* shape, const float* params_dev, int64_t n, const float* X_dev,
+                    const int32_t* species, float* G_dev);
+void mlp_scratch_free(pfw_ws* ws);
+// ace.cu: forces of a per-site dE/dfeature field through the feature model
+void sur_pullback(pfw_ws* ws, const double* dEdx_dev, double* F_dev);
 
 inline int grid_for(int64_t n, int block) { return (int)((n + block - 1) / block); }
 

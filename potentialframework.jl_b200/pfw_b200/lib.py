@@ -92,6 +92,10 @@ def load():
                                      C.POINTER(C.c_float), i32p, dp, C.POINTER(C.c_float)]
     L.pfw_mlp_train.argtypes = [vp, vp, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_float),
                                 C.POINTER(C.c_float), i32p, vp, C.POINTER(C.c_float)]
+    L.pfw_mlp_ef_step.argtypes = [vp, vp, vp, vp, vp, C.c_int64, vp, vp, i32p, vp, vp, C.c_float, C.c_float,
+                                  C.c_int64, vp, dp]
+    L.pfw_mlp_input_grad.argtypes = [vp, vp, vp, C.c_int64, vp, i32p, vp]
+    L.pfw_surrogate_pullback.argtypes = [vp, vp, vp]
     _lib = L
     return L
 
@@ -112,6 +116,7 @@ class Handle:
             raise PFWError(rc, "pfw_ws_create failed (no CUDA device, or invalid options)")
         self.ws = h
         self.L = L
+        self.device = int(device)
 
     def check(self, rc):
         if rc != OK:
@@ -342,6 +347,28 @@ class Handle:
                                         ptr(y, C.c_float), ptr(Z, C.c_int32), C.byref(opt),
                                         ptr(hist, C.c_float)))
         return hist
+
+    # --- energy + force training on device buffers (torch tensors) -------
+    def mlp_ef_step(self, shape, P, m1, m2, X, y, Z, V, c, *, wE, lr, step, grad=None, with_loss=False):
+        """One full-batch Adam step (or, with grad, the gradient only); tensors
+        on the workspace's device, Z a host int32 array."""
+        Z = np.ascontiguousarray(Z, np.int32)
+        loss = np.zeros(shape.nz * shape.members) if with_loss else None
+        vp_ = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        self.check(self.L.pfw_mlp_ef_step(self.ws, C.byref(shape), vp_(P), vp_(m1), vp_(m2), len(Z), vp_(X), vp_(y),
+                                          ptr(Z, C.c_int32), vp_(V), vp_(c), float(wE), float(lr), int(step),
+                                          vp_(grad), ptr(loss, C.c_double)))
+        return loss
+
+    def mlp_input_grad(self, shape, P, X, Z, G):
+        """∂y/∂x of every member at every sample into G (device tensor [members, n, nin])."""
+        Z = np.ascontiguousarray(Z, np.int32)
+        self.check(self.L.pfw_mlp_input_grad(self.ws, C.byref(shape), C.c_void_p(P.data_ptr()), len(Z),
+                                             C.c_void_p(X.data_ptr()), ptr(Z, C.c_int32), C.c_void_p(G.data_ptr())))
+
+    def surrogate_pullback(self, dEdx, F):
+        """Forces (device tensor n×3) of a per-site dE/dfeature field (device tensor n×nin)."""
+        self.check(self.L.pfw_surrogate_pullback(self.ws, C.c_void_p(dEdx.data_ptr()), C.c_void_p(F.data_ptr())))
 
     def probe_fp64(self):
         v = np.zeros(1)

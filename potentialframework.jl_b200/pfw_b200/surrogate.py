@@ -180,6 +180,43 @@ def mlp_param_grad_reference(params, x, t, nin, H):
     return float(np.mean((y - t) ** 2)), g
 
 
+def _silu_parts(z):
+    a = 1.0 / (1.0 + np.exp(-z))
+    return z * a, a * (1 + z * (1 - a)), a * (1 - a) * (2 + z * (1 - 2 * a))
+
+
+def mlp_ef_objective(params, x, t, v, c, wE, nin, H):
+    """wE·mean((y - t)²) + Σ_s c_s·(v_s·∇_x y(x_s)): the energy + force
+    training objective of one model in FP64 (v: the force error pulled back
+    into standardised feature space, c: the per-sample force weight)."""
+    y, dydx = mlp_forward(params, x, nin, H)
+    return wE * float(np.mean((y - t) ** 2)) + float(np.sum(c * np.einsum("si,si->s", v, dydx)))
+
+
+def mlp_ef_grad_reference(params, x, t, v, c, wE, nin, H):
+    """FP64 numpy gradient of mlp_ef_objective with respect to the parameter
+    vector: the energy backward pass plus the reverse of the tangent pass
+    t1 = W1 v, u1 = s1'⊙t1, t2 = W2 u1, u2 = s2'⊙t2, ẏ = w3·u2."""
+    W1, b1, W2, b2, w3, b3 = (np.asarray(q, np.float64) for q in split_params(params, nin, H))
+    z1 = x @ W1.T + b1
+    h1, s1, q1 = _silu_parts(z1)
+    t1 = v @ W1.T
+    u1 = s1 * t1
+    z2 = h1 @ W2.T + b2
+    h2, s2, q2 = _silu_parts(z2)
+    t2 = u1 @ W2.T
+    u2 = s2 * t2
+    y = h2 @ w3 + b3
+    dy = wE * 2.0 * (y - t) / len(t)
+    G2 = dy[:, None] * w3 * s2 + c[:, None] * w3 * t2 * q2
+    B2 = c[:, None] * w3 * s2
+    bh, bu = G2 @ W2, B2 @ W2
+    G1 = bh * s1 + bu * t1 * q1
+    B1 = bu * s1
+    return np.concatenate([(G1.T @ x + B1.T @ v).ravel(), G1.sum(0), (G2.T @ h1 + B2.T @ u1).ravel(), G2.sum(0),
+                           dy @ h2 + c @ u2, [dy.sum()]])
+
+
 # ---------------------------------------------------------------------------
 # the trained surrogate
 # ---------------------------------------------------------------------------
@@ -320,3 +357,97 @@ def train(h, feat: PackedACE, selected, X, E, Z, *, members=MEMBERS, epochs=40, 
     _, sd, _ = sur.predict(X, Z)
     sur.tau = float(tau_factor * np.quantile(sd, tau_quantile))
     return sur
+
+
+# ---------------------------------------------------------------------------
+# energy + force fine-tuning
+# ---------------------------------------------------------------------------
+def force_training_set(h, full: PackedACE, feat: PackedACE, n_lattices=13, nc=20, seed=11, sigma=(0.03, 0.25)):
+    """B2 lattices with the full model's site energies and forces (plain FP64
+    GPU ACE) and the site features: one dict per lattice."""
+    from . import lib
+    from . import workloads as WL
+    out = []
+    h.ace(full)
+    h.surrogate(feat, None)
+    for k, sg in enumerate(np.linspace(sigma[0], sigma[1], n_lattices)):
+        s = WL.b2(seed=seed + k, nc=nc, sigma=float(sg))
+        h.set_geometry(s.X, s.H, s.pbc, s.species)
+        _, F, _ = h.evaluate(lib.MODEL_ACE, 7)
+        out.append(dict(sys=s, E=h.site_energies(), F=F, X=h.surrogate_features(), Z=s.species.copy()))
+    return out
+
+
+def train_forces(h, sur: "Surrogate", lattices, *, epochs=20, lr=1e-3, lr_final=1e-5, wE=1.0, wF=1.0,
+                 step_disp=1e-4, seed=3, log=None):
+    """Fine-tune every member of the ensemble on energies AND forces with the
+    library's kernels.  Per step (one lattice, full batch): ∂y/∂x of every
+    member (pfw_mlp_input_grad), each member's forces through the feature
+    model (pfw_surrogate_pullback), the force error ΔF_m against the full
+    model, its pull-back into feature space v = D_ΔF x (central difference of
+    the features along ΔF, largest displacement step_disp Å), and one Adam
+    step on wE·MSE(energy) + wF·Σ|ΔF|²/(3 n σ_F²) (pfw_mlp_ef_step).  The
+    feature model must be loaded in h (h.surrogate).  Returns the history of
+    (energy MSE, force RMSE in eV/Å before the epoch's steps) per epoch."""
+    import torch
+
+    dev = torch.device("cuda", h.device)
+    nz, M, nin, H = sur.shape
+    shape = pfw_mlp_shape(nz, M, nin, H)
+    P = torch.from_numpy(np.ascontiguousarray(sur.params, np.float32)).to(dev)
+    m1 = torch.zeros_like(P)
+    m2 = torch.zeros_like(P)
+    xm = torch.from_numpy(sur.x_mean).to(dev)
+    xs = torch.from_numpy(sur.x_std).to(dev)
+    ym, ys = sur.y_mean, sur.y_std
+    sigF = float(np.sqrt(np.mean(np.concatenate([L["F"].ravel() for L in lattices]) ** 2)))
+    data = []
+    for L in lattices:
+        Z = L["Z"].astype(np.int32)
+        zt = torch.from_numpy(Z.astype(np.int64)).to(dev)
+        Xd = torch.from_numpy(L["X"]).to(dev)
+        t = (L["E"] - sur.feature_model.reference[Z] - ym[Z]) / ys[Z]
+        data.append(dict(Z=Z, zt=zt, Xs=((Xd - xm[zt]) / xs[zt]).float().contiguous(),
+                         y=torch.from_numpy(t.astype(np.float32)).to(dev), F=torch.from_numpy(L["F"]).to(dev),
+                         sys=L["sys"], n=len(Z), yscale=torch.from_numpy(ys[Z]).to(dev)))
+    rng = np.random.default_rng(seed)
+    total = epochs * len(data)
+    step = 0
+    hist = []
+    for ep in range(epochs):
+        e_mse, f_sq, f_cnt = 0.0, 0.0, 0
+        for li in rng.permutation(len(data)):
+            d = data[li]
+            n, s = d["n"], d["sys"]
+            G = torch.empty((M, n, nin), dtype=torch.float32, device=dev)
+            h.mlp_input_grad(shape, P, d["Xs"], d["Z"], G)
+            V = torch.empty((M, n, nin), dtype=torch.float32, device=dev)
+            scale = d["yscale"][:, None] / xs[d["zt"]]  # dE/dx = y_std ∂y/∂x̃ / x_std
+            for m in range(M):
+                dEdx = (G[m].double() * scale).contiguous()
+                Fp = torch.empty((n, 3), dtype=torch.float64, device=dev)
+                h.set_geometry(s.X, s.H, s.pbc, s.species)
+                h.surrogate_pullback(dEdx, Fp)
+                dF = (Fp - d["F"]).cpu().numpy()
+                f_sq += float((dF ** 2).sum())
+                f_cnt += dF.size
+                eps = step_disp / max(float(np.abs(dF).max()), 1e-30)
+                h.set_geometry(s.X + eps * dF, s.H, s.pbc, s.species)
+                xp = torch.from_numpy(h.surrogate_features()).to(dev)
+                h.set_geometry(s.X - eps * dF, s.H, s.pbc, s.species)
+                xn = torch.from_numpy(h.surrogate_features()).to(dev)
+                V[m] = ((xp - xn) / (2.0 * eps) / xs[d["zt"]]).float()
+            c = (-2.0 * wF / (3.0 * n * sigF ** 2) * d["yscale"]).float().contiguous()
+            frac = step / max(total - 1, 1)
+            lr_t = lr_final + 0.5 * (lr - lr_final) * (1.0 + np.cos(np.pi * frac))
+            step += 1
+            loss = h.mlp_ef_step(shape, P, m1, m2, d["Xs"], d["y"], d["Z"], V, c, wE=wE, lr=lr_t, step=step,
+                                 with_loss=True)
+            e_mse += float(np.mean(loss))
+        hist.append((e_mse / len(data), float(np.sqrt(f_sq / max(f_cnt, 1)))))
+        if log:
+            log(f"epoch {ep}: energy mse {hist[-1][0]:.3e}, force rmse {hist[-1][1]:.4f} eV/A")
+    torch.cuda.synchronize()
+    sur.params = P.cpu().numpy().reshape(sur.params.shape)
+    sur.force_history = hist
+    return hist

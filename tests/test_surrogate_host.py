@@ -69,3 +69,28 @@ def test_bf16_rounding():
     assert b[2] == 0x3F81  # 1 + 3·2^-9: above the tie
     back = S.from_bf16_bits(b)
     assert np.all(np.abs(back - vals) <= np.abs(vals) * 2.0 ** -8)
+
+
+def test_energy_force_gradient_reference_matches_finite_differences():
+    # the energy + force objective wE·MSE + Σ c·(v·∇_x y): the analytic
+    # gradient (energy backward plus the reverse of the tangent pass) against
+    # central differences of the objective, every parameter of a small model
+    nin, H, n = 5, 4, 7
+    rng = np.random.default_rng(3)
+    p = S.init_params(1, 1, nin, H, 9)[0, 0].astype(np.float64)
+    p[nin * H:nin * H + H] = rng.normal(0, 0.3, H)  # nonzero biases
+    x = rng.normal(0, 1, (n, nin))
+    v = rng.normal(0, 1, (n, nin))
+    t = rng.normal(0, 1, n)
+    c = rng.normal(0, 1, n)
+    g = S.mlp_ef_grad_reference(p, x, t, v, c, 0.7, nin, H)
+    fd = np.zeros_like(p)
+    for k in range(len(p)):
+        d = np.zeros_like(p)
+        d[k] = 1e-6
+        fd[k] = (S.mlp_ef_objective(p + d, x, t, v, c, 0.7, nin, H)
+                 - S.mlp_ef_objective(p - d, x, t, v, c, 0.7, nin, H)) / 2e-6
+    assert np.abs(g - fd).max() <= 1e-7 * max(1.0, np.abs(fd).max())
+    # without the force term it is the energy gradient
+    _, ge = S.mlp_param_grad_reference(p, x, t, nin, H)
+    assert np.allclose(S.mlp_ef_grad_reference(p, x, t, v, np.zeros(n), 1.0, nin, H), ge, rtol=1e-12, atol=1e-14)
