@@ -378,20 +378,46 @@ def force_training_set(h, full: PackedACE, feat: PackedACE, n_lattices=13, nc=20
     return out
 
 
-def train_forces(h, sur: "Surrogate", lattices, *, epochs=20, lr=1e-3, lr_final=1e-5, wE=1.0, wF=1.0,
-                 step_disp=1e-4, seed=3, log=None):
+def train_forces(h, sur: "Surrogate", lattices, *, epochs=40, inner=1, batch=1 << 30, lr=1e-3, lr_final=1e-5,
+                 warmup=50, wE=1.0, wF=1.0, step_disp=1e-4, seed=3, log=None):
     """Fine-tune every member of the ensemble on energies AND forces with the
-    library's kernels.  Per step (one lattice, full batch): ∂y/∂x of every
-    member (pfw_mlp_input_grad), each member's forces through the feature
-    model (pfw_surrogate_pullback), the force error ΔF_m against the full
-    model, its pull-back into feature space v = D_ΔF x (central difference of
-    the features along ΔF, largest displacement step_disp Å), and one Adam
-    step on wE·MSE(energy) + wF·Σ|ΔF|²/(3 n σ_F²) (pfw_mlp_ef_step).  The
-    feature model must be loaded in h (h.surrogate).  Returns the history of
-    (energy MSE, force RMSE in eV/Å before the epoch's steps) per epoch."""
+    library's kernels.  Per lattice visit: ∂y/∂x of every member at every
+    site (pfw_mlp_input_grad), each member's forces through the feature model
+    (pfw_surrogate_pullback), the force error ΔF_m against the full model,
+    and its pull-back into feature space v = D_ΔF x (central difference of
+    the features along ΔF, largest displacement step_disp Å).  Then `inner`
+    Adam steps (pfw_mlp_ef_step) on random batches of `batch` sites of the
+    lattice, each on wE·MSE(energy) + wF·Σ|ΔF|²/(3 n σ_F²) with v held at
+    the visit's value (the force term's gradient is exact at the first step
+    and linearised after it).  Fine-tuning starts from a converged energy
+    fit, so the learning rate ramps up linearly over `warmup` steps (Adam's
+    first steps move every weight by the full rate) and then decays as a
+    cosine to lr_final.  The feature model must be loaded in h
+    (h.surrogate).  Returns the history of (energy MSE, force RMSE in eV/Å
+    at the visits) per epoch."""
     import torch
 
     dev = torch.device("cuda", h.device)
+    # The library's kernels and the torch glue must run in one stream, in
+    # order.  A stream of its own: the legacy default stream's handle is 0,
+    # which pfw_set_stream reads as "the workspace's own stream".
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.synchronize(dev)
+    h.set_stream(C.c_void_p(stream.cuda_stream))
+    try:
+        with torch.cuda.stream(stream):
+            return _train_forces(h, sur, lattices, dev, epochs=epochs, inner=inner, batch=batch, lr=lr,
+                                 lr_final=lr_final, warmup=warmup, wE=wE, wF=wF, step_disp=step_disp, seed=seed,
+                                 log=log)
+    finally:
+        torch.cuda.synchronize(dev)
+        h.set_stream(None)
+
+
+def _train_forces(h, sur, lattices, dev, *, epochs, inner, batch, lr, lr_final, warmup, wE, wF, step_disp, seed,
+                  log):
+    import torch
+
     nz, M, nin, H = sur.shape
     shape = pfw_mlp_shape(nz, M, nin, H)
     P = torch.from_numpy(np.ascontiguousarray(sur.params, np.float32)).to(dev)
@@ -411,7 +437,7 @@ def train_forces(h, sur: "Surrogate", lattices, *, epochs=20, lr=1e-3, lr_final=
                          y=torch.from_numpy(t.astype(np.float32)).to(dev), F=torch.from_numpy(L["F"]).to(dev),
                          sys=L["sys"], n=len(Z), yscale=torch.from_numpy(ys[Z]).to(dev)))
     rng = np.random.default_rng(seed)
-    total = epochs * len(data)
+    total = epochs * len(data) * inner
     step = 0
     hist = []
     for ep in range(epochs):
@@ -437,13 +463,19 @@ def train_forces(h, sur: "Surrogate", lattices, *, epochs=20, lr=1e-3, lr_final=
                 h.set_geometry(s.X - eps * dF, s.H, s.pbc, s.species)
                 xn = torch.from_numpy(h.surrogate_features()).to(dev)
                 V[m] = ((xp - xn) / (2.0 * eps) / xs[d["zt"]]).float()
-            c = (-2.0 * wF / (3.0 * n * sigF ** 2) * d["yscale"]).float().contiguous()
-            frac = step / max(total - 1, 1)
-            lr_t = lr_final + 0.5 * (lr - lr_final) * (1.0 + np.cos(np.pi * frac))
-            step += 1
-            loss = h.mlp_ef_step(shape, P, m1, m2, d["Xs"], d["y"], d["Z"], V, c, wE=wE, lr=lr_t, step=step,
-                                 with_loss=True)
-            e_mse += float(np.mean(loss))
+            B = min(batch, n)
+            # the force weight of a site in a batch of B of the lattice's n sites (unbiased in expectation)
+            c_all = -2.0 * wF / (3.0 * B * sigF ** 2) * d["yscale"]
+            for _ in range(inner):
+                idx = np.sort(rng.choice(n, B, replace=False))
+                it = torch.from_numpy(idx).to(dev)
+                frac = step / max(total - 1, 1)
+                lr_t = (lr_final + 0.5 * (lr - lr_final) * (1.0 + np.cos(np.pi * frac))) * min(1.0, (step + 1) / warmup)
+                step += 1
+                loss = h.mlp_ef_step(shape, P, m1, m2, d["Xs"][it].contiguous(), d["y"][it].contiguous(),
+                                     d["Z"][idx], V[:, it].contiguous(), c_all[it].float().contiguous(), wE=wE,
+                                     lr=lr_t, step=step, with_loss=True)
+                e_mse += float(np.mean(loss)) / inner
         hist.append((e_mse / len(data), float(np.sqrt(f_sq / max(f_cnt, 1)))))
         if log:
             log(f"epoch {ep}: energy mse {hist[-1][0]:.3e}, force rmse {hist[-1][1]:.4f} eV/A")
