@@ -10,6 +10,11 @@
 //   k_scatter, k_cell_rank stable placement: atoms of a cell ordered by
 //                          original index = the reference's sortperm order
 //   k_gather               sorted SoA positions (double4: x, y, z, species)
+//
+// Without an open axis to measure first (every periodic box, and batches of
+// them) the build runs fused: k_bin (system lookup, wrap, windings, key,
+// count), the scan, k_scatter, and k_cell_order (rank, gather, species
+// check, cell → system); the separate kernels serve the open-axis path.
 #include <algorithm>
 #include <cmath>
 
@@ -322,6 +327,108 @@ __global__ void k_gather(int n, const int* __restrict__ perm, const double* __re
   inverse[i] = k;
 }
 
+// ---- the fused build (no open-axis pre-pass): two kernels replace five ----
+__device__ __forceinline__ int system_of_atom(const SysGeom* __restrict__ sys, int nsys, int i) {
+  int lo = 0, hi = nsys - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sys[mid].atom_begin <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// k_atom_sys + k_wrap + k_key_count in one pass: the canonical wrap, the
+// windings, the bin key and the provisional slot of every atom (the same
+// arithmetic as the three kernels, without the bin-coordinate round trip).
+__global__ void k_bin(int n, const double* __restrict__ X, const SysGeom* __restrict__ sys, int nsys,
+                      double* __restrict__ wrapped, int* __restrict__ wind, int* __restrict__ cellid,
+                      int* __restrict__ slot, int* __restrict__ count, int* __restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const SysGeom& g = sys[nsys == 1 ? 0 : system_of_atom(sys, nsys, i)];
+  const double v[3] = {X[3 * i], X[3 * i + 1], X[3 * i + 2]};
+  if (!(isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]))) atomicExch(bad, 1);
+  double w[3], b[3];
+  int wd[3];
+  if (g.minimum_image) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      w[a] = g.pbc[a] ? jl_mod(v[a], g.L[a]) : v[a];
+      b[a] = w[a];
+      wd[a] = g.pbc[a] ? (int)floor(xdiv(v[a], g.L[a])) : 0;
+    }
+  } else {
+    double f[3];
+    xmatvec(g.recip, v[0], v[1], v[2], f);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) wd[a] = g.pbc[a] ? (int)floor(f[a]) : 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) f[a] = g.pbc[a] ? jl_mod(f[a], 1.0) : f[a];
+    xmatvec(g.basis, f[0], f[1], f[2], w);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) b[a] = f[a];
+  }
+  int key[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    wrapped[3 * i + a] = w[a];
+    wind[3 * i + a] = wd[a];
+    if (g.brute) {
+      key[a] = 0;
+    } else if (g.pbc[a]) {
+      const double q = floor(xdiv(b[a], g.sizecell[a]));
+      key[a] = (q >= 0.0) ? (q > g.pdims[a] - 1 ? g.pdims[a] - 1 : (int)q) : 0;
+    } else {
+      // open axes take the pre-pass path; here only a brute-force system has one
+      key[a] = 0;
+    }
+  }
+  const int c = g.cell_begin + (key[0] * g.dims[1] + key[1]) * g.dims[2] + key[2];
+  cellid[i] = c;
+  slot[i] = atomicAdd(&count[c], 1);
+}
+
+// k_cell_rank + k_gather + k_cell_sys in one pass, one warp per cell: the
+// rank of each atom among its cell by original index (stable order), the
+// sorted double4 positions with their validated species channel, the
+// inverse permutation, the cell's system and the largest population.
+__global__ void k_cell_order(int ncells, const SysGeom* __restrict__ sys, int nsys,
+                             const int* __restrict__ cell_start, const int* __restrict__ tmp,
+                             const double* __restrict__ wrapped, const int* __restrict__ species,
+                             int* __restrict__ perm, double4* __restrict__ pos, int* __restrict__ inverse,
+                             int* __restrict__ cell_sys, int* __restrict__ maxpop, int limit,
+                             int* __restrict__ bad_species) {
+  const int cell = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (cell >= ncells) return;
+  const int b = cell_start[cell], e = cell_start[cell + 1];
+  if (lane == 0) {
+    int lo = 0, hi = nsys - 1;  // the last system whose cell range starts at or before this cell
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sys[mid].cell_begin <= cell) lo = mid;
+      else hi = mid - 1;
+    }
+    cell_sys[cell] = lo;
+    if (e > b) atomicMax(maxpop, e - b);
+  }
+  for (int t = b + lane; t < e; t += 32) {
+    const int me = tmp[t];
+    int rank = 0;
+    for (int u = b; u < e; ++u) rank += tmp[u] < me;
+    const int k = b + rank;
+    perm[k] = me;
+    int z = species[me];
+    if (z < 0 || z >= limit) {
+      atomicExch(bad_species, 1);
+      z = 0;
+    }
+    pos[k] = make_double4(wrapped[3 * me], wrapped[3 * me + 1], wrapped[3 * me + 2], (double)z);
+    inverse[me] = k;
+  }
+}
+
 __global__ void k_cell_sys(const SysGeom* __restrict__ sys, int nsys, int ncells, int* __restrict__ cell_sys,
                            const int* __restrict__ cell_start, int* __restrict__ maxpop) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -535,14 +642,33 @@ void prepare_launch(pfw_ws* ws, bool wrap) {
   int* count = ws->cell_count.as<int>();
   int* cell_start = ws->cell_start.as<int>();
   if (wrap) {
+    // no open-axis pre-pass: the fused build (bin; scan; scatter; order)
     PFW_CUDA(cudaMemsetAsync(bad, 0, sizeof(int) * 8, st));
+    PFW_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (ncells + 1), st));
     if (n > 0) {
-      k_atom_sys<<<grid_for(n, 256), 256, 0, st>>>(dsys, nsys, n, atom_sys);
-      k_wrap<<<grid_for(n, 256), 256, 0, st>>>(n, ws->X.as<double>(), atom_sys, dsys, ws->wrapped.as<double>(),
-                                               bincoord, ws->wind.as<int>(), bad);
-      ws->launches += 2;
+      k_bin<<<grid_for(n, 256), 256, 0, st>>>(n, ws->X.as<double>(), dsys, nsys, ws->wrapped.as<double>(),
+                                              ws->wind.as<int>(), ws->cellid.as<int>(), ws->slot.as<int>(), count,
+                                              bad);
+      ws->launches += 1;
     }
+    exclusive_scan_i32(ws, count, cell_start, ncells);
+    if (n > 0) {
+      k_scatter<<<grid_for(n, 256), 256, 0, st>>>(n, ws->cellid.as<int>(), ws->slot.as<int>(), cell_start,
+                                                   ws->tmp_idx.as<int>());
+      ws->launches += 1;
+    }
+    if (ncells > 0) {
+      k_cell_order<<<grid_for((int64_t)ncells * 32, 256), 256, 0, st>>>(
+          (int)ncells, dsys, nsys, cell_start, ws->tmp_idx.as<int>(), ws->wrapped.as<double>(), ws->species.as<int>(),
+          ws->perm.as<int>(), ws->pos.as<double4>(), ws->inverse.as<int>(), ws->cell_sys.as<int>(), bad + 4,
+          ws->species_limit, bad + 2);
+      ws->launches += 1;
+    }
+    PFW_CUDA(cudaGetLastError());
+    return;
   }
+  // after the open-axis pre-pass (k_atom_sys, k_wrap, k_open_minmax in
+  // prepare_plan): key, scan, placement, gather
   PFW_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (ncells + 1), st));
   if (n > 0) {
     k_key_count<<<grid_for(n, 256), 256, 0, st>>>(n, atom_sys, dsys, bincoord, ws->cellid.as<int>(),
