@@ -412,6 +412,8 @@ def parse():
                    help="arithmetic of the headline workload (mixed: FP32 pair/ACE arithmetic, FP64 wrap and "
                         "Kahan energy/virial); the default fp64 is the reference's")
     p.add_argument("--no-tune", action="store_true", help="ACE workloads: the default site-kernel schedule")
+    p.add_argument("--only-form", choices=["skin", "batch", "design"],
+                   help="run one of the other configurations alone and print its record (no headline)")
     return p.parse_args()
 
 
@@ -867,10 +869,32 @@ def surrogate_form(dev, stream, flush, steps=5):
                      "gate: standardised training range +-5 % or ensemble std > tau; FP64 features and pullback")
 
 
+def run_one_form(args):
+    """One form by itself (its own warm-up and steps), on cuda:0 with the L2
+    flush between steps, printed as one JSON line."""
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    with torch.cuda.stream(stream):
+        if args.only_form == "skin":
+            rec = skin_form(dev, stream, flush)
+        elif args.only_form == "batch":
+            rec = batch_form(dev, stream, flush, {})
+        else:
+            rec = design_form(dev, stream, flush)
+    torch.cuda.synchronize()
+    print(json.dumps(dict(form=args.only_form, **rec), default=float))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_form:
+        return run_one_form(args)
     return run_b200(args)
 
 

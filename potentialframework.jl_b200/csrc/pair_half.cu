@@ -14,17 +14,26 @@
 // is visited exactly once, and the displacement is exactly antisymmetric, so
 // the pair set is the full list's.
 //
-// Per home chunk (<= 32 atoms) the candidates of the 14 cells are staged 32
-// at a time (FP32 relative coordinates, box prune as in traverse.cuh), and
-// each window is tested transposed: lanes hold candidates, the warp walks
-// the home atoms, a ballot per home atom gives M_h (its candidates within
-// c²(1 + 2⁻¹⁰)) and each lane collects C_t (its home atoms).  The window's
-// entries are listed home-major, every lane evaluates a strided share of
-// them (exact FP64 displacement and cutoff, or FP32 from the staged
-// coordinates for the mixed form with an FP64 re-test in the guard band) and
-// stores the gradient g in shared memory.  The home side then adds its
-// entries (contiguous) and each candidate its own (in home order): both sums
-// run in a fixed order, so forces are deterministic without atomics.
+// Per home chunk (<= 32 atoms) the candidates of the 14 cells stream through
+// a box prune (a candidate farther than c from the bounding box of the home
+// atoms is dropped) into a staging buffer of up to 160 candidates (FP32
+// coordinates relative to the home cell's first atom).  A full buffer is one
+// pass: first every 32-candidate window is tested transposed (lanes hold
+// candidates, the warp walks the home atoms, a ballot per home atom gives
+// its mask of candidates within c²(1 + 2⁻¹⁰)); then the pass's entries,
+// home-major (home h, its candidates in staging order), are split into
+// contiguous equal shares, one per lane, and evaluated two per step (exact
+// FP64 displacement and cutoff, or FP32 from the staged coordinates for the
+// mixed form with an FP64 re-test in the guard band).  A lane walks its
+// share directly on the per-home masks, so no entry list is built.
+//
+// Reductions, all in a fixed order (deterministic without atomics): the
+// home side accumulates in registers per owner and leaves one partial per
+// (lane, owner) in slot lane + owner, which the owner adds in lane order;
+// the j side groups the lanes of one step that hold the same candidate
+// (match), and the lowest lane adds the group's gradients in lane order to
+// the candidate's accumulator in shared memory.  After the pass each staged
+// candidate's accumulator is complete for this home chunk.
 //
 // Forces leave the kernel as partial sums per (slot, sorted atom): slot 0 the
 // home side, slot 1 the j side of the home cell's own pairs, slots 2..14 the
@@ -44,8 +53,8 @@ namespace pfw {
 
 constexpr int HALF_WARPS = 8;   // home cells per CTA
 constexpr int HALF_NE = 14;     // self + 13 forward neighbour cells
-constexpr int HALF_RING = 64;   // staging ring of pruned candidates
-constexpr int HALF_LIST = 1024; // entries of one window (32 homes × 32 candidates)
+constexpr int HALF_CAP = 160;   // staged candidates of one pass
+constexpr int HALF_WIN = HALF_CAP / 32;
 constexpr int HALF_NSLOT = 15;  // force slots (see above)
 constexpr float HALF_GUARD = 1.0f / 1024.0f;
 #ifndef PFW_HALF_MINBLOCKS
@@ -57,33 +66,22 @@ __constant__ int8_t c_half_off[13][3] = {{0, 0, 1},  {0, 1, -1}, {0, 1, 0},  {0,
                                          {1, -1, 0}, {1, -1, 1}, {1, 0, -1}, {1, 0, 0},  {1, 0, 1},
                                          {1, 1, -1}, {1, 1, 0},  {1, 1, 1}};
 
-// FP64 copies of the staged positions, for the plain path's exact arithmetic
-// (the mixed path reads global memory in the rare guard-band re-test).
-template <class T>
-struct HalfExact {};
-template <>
-struct HalfExact<double> {
-  double cx[HALF_RING], cy[HALF_RING], cz[HALF_RING];  // staged candidates (unshifted)
-  double hx[32], hy[32], hz[32];                       // home atoms
-};
-
 template <class T>
 struct alignas(16) HalfStage {
   double sh[HALF_NE][3];     // image shift of each entry (added to x_j - x_i)
   int jb[HALF_NE];           // first sorted atom of each entry's cell
   int start[HALF_NE + 1];    // flat-list offsets of the entries
-  float rx[HALF_RING], ry[HALF_RING], rz[HALF_RING];  // staged candidates (FP32, shifted, relative to ref)
-  unsigned item[HALF_RING];  // staged candidate: j | entry << 24 | owned << 28 | species << 29
+  float rx[HALF_CAP], ry[HALF_CAP], rz[HALF_CAP];  // staged candidates (FP32, shifted, relative to ref)
+  unsigned item[HALF_CAP];   // staged candidate: j | entry << 24 | owned << 28 | species << 29
+  unsigned mh[HALF_WIN][32]; // per window and home atom: the window's candidates within c²(1 + 2⁻¹⁰)
   alignas(16) float hx[32];  // home atoms (FP32, relative to ref); read as float2 pairs
   alignas(16) float hy[32];
   alignas(16) float hz[32];
+  double hxd[32], hyd[32], hzd[32];  // home atoms (FP64, as stored)
   unsigned char hsp[32];     // home atoms' species channels (clamped to 0..3)
-  int off[33];               // exclusive scan of the home atoms' entry counts
-  unsigned char list[HALF_LIST];  // window entries, home-major: candidate index t
+  int off[33];               // exclusive scan of the home atoms' entry counts in the pass
   T part[63][3];             // home-side partial sums, slot lane + owner
-  T ga[3][32], gb[3][32];    // gradients of one step (first / second entry of each lane)
-  unsigned jma[32], jmb[32]; // per candidate: lanes whose first / second entry is it
-  HalfExact<T> x;
+  T fj[HALF_CAP][3];         // j-side sums of the staged candidates
 };
 static_assert(sizeof(HalfStage<double>) % 16 == 0 && sizeof(HalfStage<float>) % 16 == 0, "stage stride");
 static_assert(offsetof(HalfStage<double>, hx) % 8 == 0 && offsetof(HalfStage<double>, hy) % 8 == 0 &&
@@ -147,29 +145,29 @@ struct HalfAcc<float> {
 struct HalfCtx {
   double c2;
   float c2f, invc2f, eps4f, eps24f, sigma2f, shiftf;
-  int i0;
   unsigned ownmask;
   bool all_own;
 };
 
-// One entry (home h, window slot s = (base + t) mod ring): returns the
-// gradient (force on h += g, on t -= g), zero unless the pair is within the
-// cutoff, and accumulates its energy and virial.
+// One entry (home h, staged candidate t): returns the gradient (force on h
+// += g, on t -= g), zero unless the pair is within the cutoff, and
+// accumulates its energy and virial.
 template <int KIND, class T>
 struct HalfEval;
 
 template <int KIND>
 struct HalfEval<KIND, double> {
   __device__ __forceinline__ static void run(const HalfCtx& cx, const PairParams& prm, const double* sA,
-                                             const double4* __restrict__, const HalfStage<double>& st, int s,
+                                             const double4* __restrict__ pos, const HalfStage<double>& st, int t,
                                              int h, bool valid, HalfAcc<double>& acc, int& np, double& gx,
                                              double& gy, double& gz) {
-    const unsigned it = st.item[s];
+    const unsigned it = st.item[t];
     const int k = (it >> 24) & 15;
+    const double4 pj = pos[it & 0xFFFFFFu];
     double d[3];
-    d[0] = xadd(xsub(st.x.cx[s], st.x.hx[h]), st.sh[k][0]);
-    d[1] = xadd(xsub(st.x.cy[s], st.x.hy[h]), st.sh[k][1]);
-    d[2] = xadd(xsub(st.x.cz[s], st.x.hz[h]), st.sh[k][2]);
+    d[0] = xadd(xsub(pj.x, st.hxd[h]), st.sh[k][0]);
+    d[1] = xadd(xsub(pj.y, st.hyd[h]), st.sh[k][1]);
+    d[2] = xadd(xsub(pj.z, st.hzd[h]), st.sh[k][2]);
     const double r2 = xr2(d[0], d[1], d[2]);
     const bool hit = valid && r2 < cx.c2;
     double en, coef;
@@ -185,21 +183,20 @@ struct HalfEval<KIND, double> {
 template <int KIND>
 struct HalfEval<KIND, float> {
   __device__ __forceinline__ static void run(const HalfCtx& cx, const PairParams&, const double* sA,
-                                             const double4* __restrict__ pos, const HalfStage<float>& st, int s,
+                                             const double4* __restrict__ pos, const HalfStage<float>& st, int t,
                                              int h, bool valid, HalfAcc<float>& acc, int& np, float& gx, float& gy,
                                              float& gz) {
-    const unsigned it = st.item[s];
-    float d[3] = {st.rx[s] - st.hx[h], st.ry[s] - st.hy[h], st.rz[s] - st.hz[h]};
+    const unsigned it = st.item[t];
+    float d[3] = {st.rx[t] - st.hx[h], st.ry[t] - st.hy[h], st.rz[t] - st.hz[h]};
     const float r2 = fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2]));
     bool hit = valid && r2 < cx.c2f * (1.f - HALF_GUARD);
     if (valid && !hit && r2 < cx.c2f * (1.f + HALF_GUARD)) {
       // guard band: the exact reference decision (NeighbourList/geometry.jl:5-19)
       const int k = (it >> 24) & 15;
-      const double4 ph = pos[cx.i0 + h];
       const double4 pj = pos[it & 0xFFFFFFu];
-      const double e0 = xadd(xsub(pj.x, ph.x), st.sh[k][0]);
-      const double e1 = xadd(xsub(pj.y, ph.y), st.sh[k][1]);
-      const double e2 = xadd(xsub(pj.z, ph.z), st.sh[k][2]);
+      const double e0 = xadd(xsub(pj.x, st.hxd[h]), st.sh[k][0]);
+      const double e1 = xadd(xsub(pj.y, st.hyd[h]), st.sh[k][1]);
+      const double e2 = xadd(xsub(pj.z, st.hzd[h]), st.sh[k][2]);
       hit = xr2(e0, e1, e2) < cx.c2;
     }
     const float rr = hit ? r2 : cx.c2f;
@@ -224,19 +221,6 @@ struct HalfEval<KIND, float> {
     np += hit ? 1 : 0;
   }
 };
-
-template <class T>
-__device__ __forceinline__ void stage_exact(HalfStage<T>&, int, const double4&) {}
-template <>
-__device__ __forceinline__ void stage_exact<double>(HalfStage<double>& st, int slot, const double4& q) {
-  st.x.cx[slot] = q.x; st.x.cy[slot] = q.y; st.x.cz[slot] = q.z;
-}
-template <class T>
-__device__ __forceinline__ void home_exact(HalfStage<T>&, int, const double4&) {}
-template <>
-__device__ __forceinline__ void home_exact<double>(HalfStage<double>& st, int lane, const double4& p) {
-  st.x.hx[lane] = p.x; st.x.hy[lane] = p.y; st.x.hz[lane] = p.z;
-}
 
 template <int KIND, class T>
 __global__ void __launch_bounds__(HALF_WARPS * 32, PFW_HALF_MINBLOCKS)
@@ -309,21 +293,20 @@ __global__ void __launch_bounds__(HALF_WARPS * 32, PFW_HALF_MINBLOCKS)
     const double4 ref = pos[b];
     const float c2hi = cx.c2f * (1.f + HALF_GUARD);
     const size_t slotstride = 3 * (size_t)natoms;
-    st.jma[lane] = 0u;
-    st.jmb[lane] = 0u;
     __syncwarp();
     for (int i0 = b; i0 < e; i0 += 32) {
       const int nh = min(32, e - i0);
       const bool have = lane < nh;
       const bool first = i0 == b;
-      cx.i0 = i0;
       const double4 pi = pos[have ? i0 + lane : i0];
       const float hx = (float)(pi.x - ref.x), hy = (float)(pi.y - ref.y), hz = (float)(pi.z - ref.z);
       st.hx[lane] = hx;
       st.hy[lane] = hy;
       st.hz[lane] = hz;
+      st.hxd[lane] = pi.x;
+      st.hyd[lane] = pi.y;
+      st.hzd[lane] = pi.z;
       st.hsp[lane] = (unsigned char)min(max((int)pi.w, 0), 3);
-      home_exact<T>(st, lane, pi);
       cx.ownmask = __ballot_sync(FULL, have && (cx.all_own || perm[i0 + lane] < prm.n_owned));
       // bounding box of the home atoms (lanes without an atom sit at ref)
       float blx = hx, bly = hy, blz = hz, bhx = hx, bhy = hy, bhz = hz;
@@ -337,42 +320,48 @@ __global__ void __launch_bounds__(HALF_WARPS * 32, PFW_HALF_MINBLOCKS)
         bhz = fmaxf(bhz, __shfl_xor_sync(FULL, bhz, o));
       }
       T fh[3] = {0, 0, 0};
-      int wpos = 0, rpos = 0;
       __syncwarp();
-      // ---- one window of n staged candidates ----
-      auto window = [&](int n) {
-        const int base = rpos & (HALF_RING - 1);
-        const bool mine = lane < n;
-        const int s = (base + lane) & (HALF_RING - 1);
-        const unsigned it = st.item[mine ? s : base];
-        const int jt = (int)(it & 0xFFFFFFu);
-        const bool self = mine && ((it >> 24) & 15) == 0;
-        const bool any_self = __any_sync(FULL, self);
-        float2 qx = make_float2(1e30f, 1e30f), qy = qx, qz = qx;
-        if (mine) {
-          qx = make_float2(st.rx[s], st.rx[s]);
-          qy = make_float2(st.ry[s], st.ry[s]);
-          qz = make_float2(st.rz[s], st.rz[s]);
-        }
-        // transposed test: lanes hold candidates, the warp walks the home atoms
-        unsigned Mh = 0u;
-        const float2 m1 = make_float2(-1.f, -1.f);  // q - h as one exactly rounded fma
-        for (int h = 0; h < nh; h += 2) {
-          const float2 ux = *reinterpret_cast<const float2*>(&st.hx[h]);
-          const float2 uy = *reinterpret_cast<const float2*>(&st.hy[h]);
-          const float2 uz = *reinterpret_cast<const float2*>(&st.hz[h]);
-          const float2 dx = __ffma2_rn(ux, m1, qx), dy = __ffma2_rn(uy, m1, qy), dz = __ffma2_rn(uz, m1, qz);
-          const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-          bool a = r2.x < c2hi, bb = h + 1 < nh && r2.y < c2hi;
-          if (any_self) {  // the home cell's own pairs: j after i only (this also drops i == j)
-            a = a && (!self || jt > i0 + h);
-            bb = bb && (!self || jt > i0 + h + 1);
+      // ---- one pass over the n staged candidates ----
+      auto pass = [&](int n) {
+        const int W = (n + 31) >> 5;
+        int cnt = 0;
+        // transposed test, window by window: lanes hold candidates, the warp walks the home atoms
+        for (int w = 0; w < W; ++w) {
+          const int t = (w << 5) + lane;
+          const bool mine = t < n;
+          const unsigned it = st.item[mine ? t : 0];
+          const int jt = (int)(it & 0xFFFFFFu);
+          const bool self = mine && ((it >> 24) & 15) == 0;
+          const bool any_self = __any_sync(FULL, self);
+          float2 qx = make_float2(1e30f, 1e30f), qy = qx, qz = qx;
+          if (mine) {
+            qx = make_float2(st.rx[t], st.rx[t]);
+            qy = make_float2(st.ry[t], st.ry[t]);
+            qz = make_float2(st.rz[t], st.rz[t]);
           }
-          const unsigned ma = __ballot_sync(FULL, a), mb = __ballot_sync(FULL, bb);
-          if (lane == h) Mh = ma;
-          if (lane == h + 1) Mh = mb;
+          unsigned Mh = 0u;
+          const float2 m1 = make_float2(-1.f, -1.f);  // q - h as one exactly rounded fma
+          for (int h = 0; h < nh; h += 2) {
+            const float2 ux = *reinterpret_cast<const float2*>(&st.hx[h]);
+            const float2 uy = *reinterpret_cast<const float2*>(&st.hy[h]);
+            const float2 uz = *reinterpret_cast<const float2*>(&st.hz[h]);
+            const float2 dx = __ffma2_rn(ux, m1, qx), dy = __ffma2_rn(uy, m1, qy), dz = __ffma2_rn(uz, m1, qz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+            bool a = r2.x < c2hi, bb = h + 1 < nh && r2.y < c2hi;
+            if (any_self) {  // the home cell's own pairs: j after i only (this also drops i == j)
+              a = a && (!self || jt > i0 + h);
+              bb = bb && (!self || jt > i0 + h + 1);
+            }
+            const unsigned ma = __ballot_sync(FULL, a), mb = __ballot_sync(FULL, bb);
+            if (lane == h) Mh = ma;
+            if (lane == h + 1) Mh = mb;
+          }
+          st.mh[w][lane] = Mh;
+          cnt += __popc(Mh);
         }
-        const int cnt = __popc(Mh);
+        for (int t = lane; t < n; t += 32) {
+          st.fj[t][0] = 0; st.fj[t][1] = 0; st.fj[t][2] = 0;
+        }
         int inc = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -383,35 +372,43 @@ __global__ void __launch_bounds__(HALF_WARPS * 32, PFW_HALF_MINBLOCKS)
         const int ntot = __shfl_sync(FULL, inc, 31);
         st.off[lane] = offh;
         if (lane == 31) st.off[32] = ntot;
-        {
-          unsigned m = Mh;
-          int q = offh;
-          while (m) {
-            const int t = __ffs(m) - 1;
-            m &= m - 1u;
-            st.list[q++] = (unsigned char)t;
-          }
-        }
         __syncwarp();
-        // Each lane evaluates a contiguous share [q, qe) of the home-major
-        // entries.  The home side accumulates per owner in registers and
-        // leaves one partial per (lane, owner) in slot lane + owner (unique:
-        // along the sequence the lane or the owner grows).  The j side: per
-        // step, the first lane of each group holding the same candidate
-        // records the group, and the candidate's lane adds the group's
-        // gradients in lane order (first entries, then second entries).
+        // this lane's share [q, q + mine) of the home-major entries, walked on the masks
         const int R = (ntot + 31) >> 5;
         const int q = lane * R;
-        const int qe = min(q + R, ntot);
-        int h = 0;  // owner of q: the last home atom with off <= q
+        const int nmine = max(0, min(q + R, ntot) - q);
+        int h = 0, w = 0;
+        unsigned m = 0u;
+        if (nmine > 0) {
 #pragma unroll
-        for (int stp = 16; stp > 0; stp >>= 1)
-          if (h + stp <= 32 && st.off[h + stp] <= q) h += stp;
-        h = min(h, 31);
-        int hend = st.off[h + 1];
+          for (int stp = 16; stp > 0; stp >>= 1)  // owner of q: the last home atom with off <= q
+            if (h + stp <= 32 && st.off[h + stp] <= q) h += stp;
+          h = min(h, 31);
+          int r = q - st.off[h];
+          m = st.mh[0][h];
+          while (r >= __popc(m) && w + 1 < W) {
+            r -= __popc(m);
+            m = st.mh[++w][h];
+          }
+          for (; r > 0; --r) m &= m - 1u;
+        }
+        int left = nmine;
+        auto take = [&](int& hh, int& tt) {  // the next entry of the share (left > 0, m != 0)
+          hh = h;
+          tt = (w << 5) + __ffs(m) - 1;
+          m &= m - 1u;
+          if (--left > 0) {
+            while (m == 0u) {
+              if (++w == W) {
+                w = 0;
+                if (++h == 32) break;
+              }
+              m = st.mh[w][h];
+            }
+          }
+        };
         int cur = -1;
         T px = 0, py = 0, pz = 0;
-        T fj[3] = {0, 0, 0};
         auto home_add = [&](bool v, int hh, T x, T y, T z) {
           if (!v) return;
           if (hh != cur) {
@@ -423,44 +420,39 @@ __global__ void __launch_bounds__(HALF_WARPS * 32, PFW_HALF_MINBLOCKS)
           }
           px += x; py += y; pz += z;
         };
+        // j side: the lanes of one step holding the same candidate form a group; its lowest lane adds
+        // the group's gradients in lane order to the candidate's sum
+        auto j_add = [&](bool v, int tt, T x, T y, T z) {
+          const unsigned grp = __match_any_sync(FULL, v ? (unsigned)tt : 0x10000u + (unsigned)lane);
+          const bool lead = v && (grp & below) == 0u;
+          unsigned rest = lead ? (grp & ~(1u << lane)) : 0u;
+          T sx = x, sy = y, sz = z;
+          while (__any_sync(FULL, rest != 0u)) {
+            const int src = rest ? __ffs(rest) - 1 : lane;
+            const T vx = __shfl_sync(FULL, x, src), vy = __shfl_sync(FULL, y, src), vz = __shfl_sync(FULL, z, src);
+            if (rest) {
+              sx += vx; sy += vy; sz += vz;
+              rest &= rest - 1u;
+            }
+          }
+          if (lead) {
+            st.fj[tt][0] -= sx; st.fj[tt][1] -= sy; st.fj[tt][2] -= sz;
+          }
+          __syncwarp();
+        };
         for (int u = 0; u < R; u += 2) {
-          const int qa = q + u, qb = q + u + 1;
-          const bool va = qa < qe, vb = qb < qe;
-          // owners of qa and qb (entries are home-major; owners only grow)
-          while (va && qa >= hend) hend = st.off[++h + 1];
-          const int ha = h;
-          while (vb && qb >= hend) hend = st.off[++h + 1];
-          const int hb = h;
-          const int ta = va ? st.list[qa] : 0, tb = vb ? st.list[qb] : 0;
-          const int sa = (base + ta) & (HALF_RING - 1), sb = (base + tb) & (HALF_RING - 1);
+          const bool va = u < nmine, vb = u + 1 < nmine;
+          int ha = 0, ta = 0, hb = 0, tb = 0;
+          if (va) take(ha, ta);
+          if (vb) take(hb, tb);
           T ax, ay, az, bx, by, bz;
-          HalfEval<KIND, T>::run(cx, prm, sA, pos, st, sa, ha, va, acc, np, ax, ay, az);
-          HalfEval<KIND, T>::run(cx, prm, sA, pos, st, sb, hb, vb, acc, np, bx, by, bz);
+          HalfEval<KIND, T>::run(cx, prm, sA, pos, st, ta, ha, va, acc, np, ax, ay, az);
+          HalfEval<KIND, T>::run(cx, prm, sA, pos, st, tb, hb, vb, acc, np, bx, by, bz);
           acc.tick();
           home_add(va, ha, ax, ay, az);
           home_add(vb, hb, bx, by, bz);
-          const unsigned grpa = __match_any_sync(FULL, va ? (unsigned)ta : 32u + (unsigned)lane);
-          const unsigned grpb = __match_any_sync(FULL, vb ? (unsigned)tb : 32u + (unsigned)lane);
-          if (va && (grpa & below) == 0u) st.jma[ta] = grpa;
-          if (vb && (grpb & below) == 0u) st.jmb[tb] = grpb;
-          st.ga[0][lane] = ax; st.ga[1][lane] = ay; st.ga[2][lane] = az;
-          st.gb[0][lane] = bx; st.gb[1][lane] = by; st.gb[2][lane] = bz;
-          __syncwarp();
-          unsigned m = st.jma[lane];
-          while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1u;
-            fj[0] -= st.ga[0][l]; fj[1] -= st.ga[1][l]; fj[2] -= st.ga[2][l];
-          }
-          m = st.jmb[lane];
-          while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1u;
-            fj[0] -= st.gb[0][l]; fj[1] -= st.gb[1][l]; fj[2] -= st.gb[2][l];
-          }
-          st.jma[lane] = 0u;
-          st.jmb[lane] = 0u;
-          __syncwarp();
+          j_add(va, ta, ax, ay, az);
+          j_add(vb, tb, bx, by, bz);
         }
         if (cur >= 0) {
           st.part[lane + cur][0] = px; st.part[lane + cur][1] = py; st.part[lane + cur][2] = pz;
@@ -472,18 +464,21 @@ __global__ void __launch_bounds__(HALF_WARPS * 32, PFW_HALF_MINBLOCKS)
             fh[0] += st.part[l + lane][0]; fh[1] += st.part[l + lane][1]; fh[2] += st.part[l + lane][2];
           }
         }
-        if (mine && want_f) {
-          T* p = P + (size_t)half_slot((it >> 24) & 15) * slotstride + jt;
-          if (first) {
-            p[0] = fj[0]; p[natoms] = fj[1]; p[2 * (size_t)natoms] = fj[2];
-          } else {
-            p[0] += fj[0]; p[natoms] += fj[1]; p[2 * (size_t)natoms] += fj[2];
+        if (want_f) {
+          for (int t = lane; t < n; t += 32) {
+            const unsigned it = st.item[t];
+            T* p = P + (size_t)half_slot((it >> 24) & 15) * slotstride + (it & 0xFFFFFFu);
+            if (first) {
+              p[0] = st.fj[t][0]; p[natoms] = st.fj[t][1]; p[2 * (size_t)natoms] = st.fj[t][2];
+            } else {
+              p[0] += st.fj[t][0]; p[natoms] += st.fj[t][1]; p[2 * (size_t)natoms] += st.fj[t][2];
+            }
           }
         }
-        rpos += n;
         __syncwarp();
       };
-      // ---- stream the flat candidate list through the ring ----
+      // ---- stream the flat candidate list through the prune into the staging buffer ----
+      int ns = 0;
       for (int f0 = 0; f0 < total; f0 += 32) {
         const int f = f0 + lane;
         const bool valid = f < total;
@@ -494,12 +489,12 @@ __global__ void __launch_bounds__(HALF_WARPS * 32, PFW_HALF_MINBLOCKS)
         const int jj = valid ? st.jb[kk] + (f - st.start[kk]) : 0;
         float px = 0.f, py = 0.f, pz = 0.f;
         bool keep = false;
-        double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
+        double4 qd = make_double4(0.0, 0.0, 0.0, 0.0);
         if (valid) {
-          q = pos[jj];
-          px = (float)((q.x + st.sh[kk][0]) - ref.x);
-          py = (float)((q.y + st.sh[kk][1]) - ref.y);
-          pz = (float)((q.z + st.sh[kk][2]) - ref.z);
+          qd = pos[jj];
+          px = (float)((qd.x + st.sh[kk][0]) - ref.x);
+          py = (float)((qd.y + st.sh[kk][1]) - ref.y);
+          pz = (float)((qd.z + st.sh[kk][2]) - ref.z);
           const float ex = fmaxf(fmaxf(blx - px, px - bhx), 0.f);
           const float ey = fmaxf(fmaxf(bly - py, py - bhy), 0.f);
           const float ez = fmaxf(fmaxf(blz - pz, pz - bhz), 0.f);
@@ -511,20 +506,21 @@ __global__ void __launch_bounds__(HALF_WARPS * 32, PFW_HALF_MINBLOCKS)
         }
         const unsigned kb = __ballot_sync(FULL, keep);
         if (keep) {
-          const int slot = (wpos + __popc(kb & below)) & (HALF_RING - 1);
+          const int slot = ns + __popc(kb & below);
           st.rx[slot] = px;
           st.ry[slot] = py;
           st.rz[slot] = pz;
-          stage_exact<T>(st, slot, q);
           const unsigned own = (cx.all_own || perm[jj] < prm.n_owned) ? 1u : 0u;
-          const unsigned zj = (unsigned)min(max((int)q.w, 0), 3);
+          const unsigned zj = (unsigned)min(max((int)qd.w, 0), 3);
           st.item[slot] = (unsigned)jj | ((unsigned)kk << 24) | (own << 28) | (zj << 29);
         }
-        wpos += __popc(kb);
+        ns += __popc(kb);
         __syncwarp();
-        if (wpos - rpos >= 32) window(32);
+        if (ns > HALF_CAP - 32 || (f0 + 32 >= total && ns > 0)) {
+          pass(ns);
+          ns = 0;
+        }
       }
-      if (wpos > rpos) window(wpos - rpos);
       if (have && want_f) {
         T* p = P + (i0 + lane);
         p[0] = fh[0]; p[natoms] = fh[1]; p[2 * (size_t)natoms] = fh[2];
@@ -602,7 +598,7 @@ static int half_smem_bytes() {
 
 // Every system's grid has a 3×3×3 stencil with a per-cell image shift.
 bool pair_half_eligible(const Prepared& P) {
-  if (P.sys.empty()) return false;
+  if (P.sys.empty() || P.n >= (1 << 24)) return false;  // staged candidates carry j in 24 bits
   for (const SysGeom& g : P.sys) {
     if (g.brute) return false;
     if (g.minimum_image && !g.fast_shift) return false;

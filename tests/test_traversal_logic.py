@@ -6,12 +6,14 @@
   not below c²·(1 + 2⁻¹⁰).  No atom within the exact FP64 cutoff of a home
   atom may be dropped — checked on random home sets with candidates placed at
   c·(1 ± 1e-7 … 1e-3) from a home atom, the hardest cases;
-* the flat drain: the lanes' lists form one owner-major sequence, lane l
+* the flat drain: the lanes' lists (or a pass's per-home masks) form one owner-major sequence, lane l
   takes entries [l·R, (l+1)·R) with R = ceil(total/32), stores the partial of
   owner h in slot l + h, and owner h adds the slots of lanes off_h/R …
   (off_h + cnt_h − 1)/R.  Slots must be unique, and each owner must collect
   exactly its own entries — checked on random count vectors, zero counts
-  included.
+  included;
+* the half-stencil pass walks each lane's share directly on the per-home
+  candidate masks: every entry taken once, in home-major order, in range.
 """
 import numpy as np
 
@@ -96,3 +98,83 @@ def test_flat_drain_slots_are_unique_and_complete():
         cnt = np.zeros(32, int)
         cnt[:nh] = rng.integers(0, 73, nh) * (rng.random(nh) > 0.2)
         flat_partition(cnt)
+
+
+def popc(x):
+    return bin(int(x)).count("1")
+
+
+def mask_walk(mh, n):
+    """The half-stencil pass's share walk (csrc/pair_half.cu), restated: home
+    h's entries are the set bits of mh[0][h], mh[1][h], ... (candidate 32w +
+    bit), listed home-major; lane l takes entries [l·R, l·R + R) with R =
+    ceil(total/32) and walks them on the masks without a list.  Every entry
+    must be taken exactly once, by the lane whose share holds its position,
+    with t < n and h < 32."""
+    W = len(mh)
+    cnt = [sum(popc(mh[w][h]) for w in range(W)) for h in range(32)]
+    off = np.concatenate([[0], np.cumsum(cnt)]).astype(int)
+    total = int(off[32])
+    R = (total + 31) // 32
+    want = [(h, 32 * w + b) for h in range(32) for w in range(W) for b in range(32) if (mh[w][h] >> b) & 1]
+    assert len(want) == total
+    got = []
+    for lane in range(32):
+        q = lane * R
+        nmine = max(0, min(q + R, total) - q)
+        if nmine == 0:
+            continue
+        h = 0
+        for stp in (16, 8, 4, 2, 1):
+            if h + stp <= 32 and off[h + stp] <= q:
+                h += stp
+        h = min(h, 31)
+        r = q - off[h]
+        w = 0
+        m = mh[0][h]
+        while r >= popc(m) and w + 1 < W:
+            r -= popc(m)
+            w += 1
+            m = mh[w][h]
+        for _ in range(r):
+            m &= m - 1
+        left = nmine
+        for _ in range(nmine):
+            assert m != 0 and h < 32
+            t = 32 * w + ((m & -m).bit_length() - 1)
+            assert t < n
+            got.append((h, t))
+            m &= m - 1
+            left -= 1
+            if left > 0:
+                while m == 0:
+                    w += 1
+                    if w == W:
+                        w = 0
+                        h += 1
+                        if h == 32:
+                            break
+                    m = mh[w][h]
+        assert got[-nmine:] == want[q:q + nmine], lane
+    assert got == want
+
+
+def test_half_pass_mask_walk_takes_every_entry_once():
+    rng = np.random.default_rng(14)
+    mask_walk([[0] * 32], 1)
+    mask_walk([[1] + [0] * 31], 1)
+    mask_walk([[0xFFFFFFFF] * 32] * 5, 160)
+    for _ in range(300):
+        n = int(rng.integers(1, 161))
+        W = (n + 31) // 32
+        nh = int(rng.integers(1, 33))
+        dens = rng.uniform(0.0, 1.0)
+        mh = []
+        for w in range(W):
+            valid = min(32, n - 32 * w)
+            row = []
+            for h in range(32):
+                bits = (rng.random(32) < dens) & (np.arange(32) < valid) & (h < nh) & (rng.random() > 0.15)
+                row.append(int(sum(1 << b for b in range(32) if bits[b])))
+            mh.append(row)
+        mask_walk(mh, n)
