@@ -412,7 +412,7 @@ def parse():
                    help="arithmetic of the headline workload (mixed: FP32 pair/ACE arithmetic, FP64 wrap and "
                         "Kahan energy/virial); the default fp64 is the reference's")
     p.add_argument("--no-tune", action="store_true", help="ACE workloads: the default site-kernel schedule")
-    p.add_argument("--only-form", choices=["skin", "batch", "design"],
+    p.add_argument("--only-form", choices=["skin", "batch", "design", "surrogate"],
                    help="run one of the other configurations alone and print its record (no headline)")
     return p.parse_args()
 
@@ -779,8 +779,12 @@ def surrogate_form(dev, stream, flush, steps=5):
     MLP kernels on 208,000 B2 environments (13 lattices of 16,000 atoms,
     displacement sigma evenly spread over [0.03, 0.25] Å, full-model site
     energies as labels), then fine-tuned on energies and forces
-    (surrogate.train_forces), and evaluated on B2 2·80³ = 1,024,000 atoms
-    (sigma 0.08 Å) against plain FP64 ACE on the same system."""
+    (surrogate.train_forces); the gate's tau is then calibrated on force
+    error on four held-out lattices of the evaluated system's displacement
+    distribution (surrogate.calibrate_gate), and the
+    surrogate is evaluated on B2 2·80³ = 1,024,000 atoms (sigma 0.08 Å)
+    against plain FP64 ACE on the same system, with the calibrated gate and
+    with the energy-only gate rule."""
     import torch
 
     from pfw_b200 import ace_generate as G
@@ -803,6 +807,12 @@ def surrogate_form(dev, stream, flush, steps=5):
     h.surrogate(feat)
     force_hist = S.train_forces(h, sur, lat, epochs=40)
     t3 = time.perf_counter()
+    tau_energy_rule = sur.tau
+    # held-out lattices from the evaluated system's distribution (sigma 0.08 Å, other seeds)
+    calib = [WL.b2(seed=700 + k, nc=20, sigma=0.08) for k in range(4)]
+    curve = S.calibrate_gate(h, sur, model, feat, calib, target=1.9e-2,
+                             quantiles=tuple(np.round(np.arange(1.0, 0.0, -0.05), 2)))
+    t4 = time.perf_counter()
     h.close()
     sysb = WL.b2(seed=12, nc=80, sigma=0.08)
     n = len(sysb)
@@ -828,8 +838,11 @@ def surrogate_form(dev, stream, flush, steps=5):
     h.evaluate_device(lib.MODEL_SURROGATE, 7, *ptrs)
     torch.cuda.synchronize()
     F_energy_only = Fd.cpu().numpy().copy()
-    h.surrogate(feat, sur)
-    for label, sel_model in (("surrogate", lib.MODEL_SURROGATE), ("ace", lib.MODEL_ACE)):
+    runs = (("surrogate", lib.MODEL_SURROGATE, sur.tau), ("surrogate_energy_gate", lib.MODEL_SURROGATE, tau_energy_rule),
+            ("ace", lib.MODEL_ACE, None))
+    for label, sel_model, tau in runs:
+        if tau is not None:
+            h.surrogate(feat, sur, tau=tau)
         h.set_geometry_device(n, ctypes.c_void_p(Xd.data_ptr()), sysb.H, sysb.pbc, ctypes.c_void_p(Sd.data_ptr()))
         for _ in range(2):
             h.evaluate_device(sel_model, 7, *ptrs)
@@ -845,13 +858,16 @@ def surrogate_form(dev, stream, flush, steps=5):
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
         res[label] = dict(ms=float(np.mean(ms)), E=float(Ed.item()), F=Fd.cpu().numpy().copy())
-        if label == "surrogate":
-            res["fallback"] = h.surrogate_stats()
+        if tau is not None:
+            res[label]["fallback"] = h.surrogate_stats()
     h.close()
     dF = res["surrogate"]["F"] - res["ace"]["F"]
     dF0 = F_energy_only - res["ace"]["F"]
-    fb, ns = res["fallback"]
+    dFg = res["surrogate_energy_gate"]["F"] - res["ace"]["F"]
+    fb, ns = res["surrogate"]["fallback"]
+    fbg, _ = res["surrogate_energy_gate"]["fallback"]
     ms_s, ms_a = res["surrogate"]["ms"], res["ace"]["ms"]
+    ms_g = res["surrogate_energy_gate"]["ms"]
     return dict(value=n / (ms_s * 1e-3), unit="atoms/s", ms_per_step=ms_s, atoms=n,
                 plain_ace_value=n / (ms_a * 1e-3), plain_ace_ms_per_step=ms_a, speedup_vs_plain_ace=ms_a / ms_s,
                 plain_ace_schedule=dict(chunk=chunk, groups=groups),
@@ -859,14 +875,21 @@ def surrogate_form(dev, stream, flush, steps=5):
                 energy_only_fit_force_rmse_vs_ace=float(np.sqrt(np.mean(dF0 ** 2))),
                 energy_err_per_atom_vs_ace=abs(res["surrogate"]["E"] - res["ace"]["E"]) / n,
                 fallback_sites=fb, fallback_fraction=fb / max(ns, 1),
+                gate=dict(rule="tau = the largest ensemble-std quantile (steps of 0.05) whose force RMSE against "
+                               "plain ACE on 4 held-out B2 20^3 lattices (sigma 0.08 A, other seeds) is <= 1.9e-2 eV/A",
+                          tau_eV=sur.tau, calibration=curve, calibrate_s=t4 - t3),
+                energy_gate=dict(tau_eV=tau_energy_rule, ms_per_step=ms_g, speedup_vs_plain_ace=ms_a / ms_g,
+                                 force_rmse_vs_ace=float(np.sqrt(np.mean(dFg ** 2))),
+                                 fallback_fraction=fbg / max(ns, 1)),
                 training=dict(environments=int(len(E)), epochs=40, members=S.MEMBERS, features=S.NIN,
                               hidden=S.HIDDEN, final_loss=sur.history[-1], label_s=t1 - t0, train_s=t2 - t1,
                               force_epochs=len(force_hist), force_train_s=t3 - t2,
-                              force_rmse_train_first_last=[force_hist[0][1], force_hist[-1][1]], tau_eV=sur.tau),
+                              force_rmse_train_first_last=[force_hist[0][1], force_hist[-1][1]]),
                 note="MLP 64->64->64->1 SiLU, BF16 weights, tcgen05 TF32 products with hi/lo activation split (FP32 accuracy), ensemble of 4 per species; "
                      "trained on site energies, then on energies and forces of the full model; "
                      "features: the 8 order-1 and first 48 order-2 invariants plus 8 pair radial sums; "
-                     "gate: standardised training range +-5 % or ensemble std > tau; FP64 features and pullback")
+                     "gate: standardised training range +-5 % or ensemble std > tau, tau calibrated on force error; "
+                     "fallback sites evaluated by plain ACE; FP64 features and pullback")
 
 
 def run_one_form(args):
@@ -882,6 +905,8 @@ def run_one_form(args):
             rec = skin_form(dev, stream, flush)
         elif args.only_form == "batch":
             rec = batch_form(dev, stream, flush, {})
+        elif args.only_form == "surrogate":
+            rec = surrogate_form(dev, stream, flush)
         else:
             rec = design_form(dev, stream, flush)
     torch.cuda.synchronize()

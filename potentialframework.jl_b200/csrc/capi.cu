@@ -58,13 +58,10 @@ void upload_geometry(pfw_ws* ws, int64_t n, const double* X, const double* H, co
     PFW_CUDA(cudaMemcpyAsync(ws->X.ptr, X, sizeof(double) * 3 * n, kind, ws->stream));
     PFW_CUDA(cudaMemcpyAsync(ws->species.ptr, species, sizeof(int32_t) * n, kind, ws->stream));
   }
+  // species channels are validated on the device while the cell list is
+  // sorted (outside [0, the model's channel count) raises PFW_EINVAL at the
+  // end of the call), for host and device uploads alike
   ws->max_species = 0;
-  if (!device_ptrs && n > 0) {
-    for (int64_t i = 0; i < n; ++i) {
-      if (species[i] < 0) throw Error(PFW_EINVAL, "species channels must be nonnegative");
-      ws->max_species = std::max(ws->max_species, species[i]);
-    }
-  }
   ws->prep.valid = false;
   ws->nb_total = -1;
   ws->last_pairs = -1;
@@ -180,6 +177,7 @@ void pfw_ws_destroy(pfw_ws* ws) {
   pfw::skin_free(ws);
   pfw::pair_graph_free(ws);
   pfw::mlp_scratch_free(ws);
+  if (ws->flags_host) cudaFreeHost(ws->flags_host);
   pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
                          &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
                          &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
@@ -284,7 +282,20 @@ pfw_status pfw_evaluate(pfw_ws* ws, int32_t model, uint32_t request, double* E, 
     double* dW = static_cast<double*>(ws->out_W.ensure(sizeof(double) * 9));
     double* dF = (request & PFW_REQ_FORCES) ? static_cast<double*>(ws->out_F.ensure(sizeof(double) * 3 * std::max(n, 1)))
                                             : nullptr;
-    dispatch_evaluate(ws, model, request, dE, dF, dW);
+    // the pair path's cell-list flags come back with the outputs (one synchronisation)
+    ws->defer_check = model == PFW_MODEL_PAIR;
+    ws->check_pending = false;
+    try {
+      dispatch_evaluate(ws, model, request, dE, dF, dW);
+    } catch (...) {
+      ws->defer_check = false;
+      if (ws->check_pending) {
+        ws->check_pending = false;
+        cudaStreamSynchronize(ws->stream);
+      }
+      throw;
+    }
+    ws->defer_check = false;
     double hE = 0, hW[9];
     unsigned long long np = 0;
     PFW_CUDA(cudaMemcpyAsync(&hE, dE, sizeof(double), cudaMemcpyDeviceToHost, ws->stream));
@@ -295,6 +306,7 @@ pfw_status pfw_evaluate(pfw_ws* ws, int32_t model, uint32_t request, double* E, 
     if (F && dF && n > 0)
       PFW_CUDA(cudaMemcpyAsync(F, dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ws->stream));
     PFW_CUDA(cudaStreamSynchronize(ws->stream));
+    pfw::prepare_check_finish(ws);
     if (model == PFW_MODEL_PAIR) ws->last_pairs = (int64_t)np / 2;
     // the reference GPU reports nonfinite results as a DomainError (NeighbourList/gpu.jl:391-395)
     bool finite = std::isfinite(hE);

@@ -695,17 +695,40 @@ void prepare_launch(pfw_ws* ws, bool wrap) {
 }
 
 // Synchronise and turn the device flags of the build into errors.
-void prepare_check(pfw_ws* ws) {
-  int hbad[8];
-  PFW_CUDA(cudaMemcpyAsync(hbad, ws->counters.ptr, sizeof(hbad), cudaMemcpyDeviceToHost, ws->stream));
-  PFW_CUDA(cudaStreamSynchronize(ws->stream));
-  PFW_CUDA(cudaGetLastError());
+static void raise_prepare_flags(pfw_ws* ws, const int* hbad) {
   if (hbad[0] == 1) throw Error(PFW_EINVAL, "positions must be finite");
   if (hbad[0] == 2) throw Error(PFW_EINVAL, "atom outside the open-axis cell grid");
   if (hbad[2])
     throw Error(PFW_EINVAL, "species channel outside the model's channels (must be >= 0 and < " +
                                 std::to_string(ws->species_limit) + ")");
   ws->prep.max_cell = hbad[4];
+}
+
+void prepare_check(pfw_ws* ws) {
+  if (ws->defer_check) {
+    if (!ws->flags_host) PFW_CUDA(cudaMallocHost(&ws->flags_host, 8 * sizeof(int32_t)));
+    PFW_CUDA(cudaMemcpyAsync(ws->flags_host, ws->counters.ptr, 8 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             ws->stream));
+    ws->check_pending = true;
+    return;
+  }
+  int hbad[8];
+  PFW_CUDA(cudaMemcpyAsync(hbad, ws->counters.ptr, sizeof(hbad), cudaMemcpyDeviceToHost, ws->stream));
+  PFW_CUDA(cudaStreamSynchronize(ws->stream));
+  PFW_CUDA(cudaGetLastError());
+  raise_prepare_flags(ws, hbad);
+}
+
+void prepare_check_finish(pfw_ws* ws) {
+  if (!ws->check_pending) return;
+  ws->check_pending = false;
+  PFW_CUDA(cudaGetLastError());
+  try {
+    raise_prepare_flags(ws, ws->flags_host);
+  } catch (...) {
+    ws->prep.valid = false;  // the cell list of a rejected input is not reused
+    throw;
+  }
 }
 
 void prepare(pfw_ws* ws, double cutoff) {

@@ -95,10 +95,14 @@ struct pfw_ws {
   std::string err;
   // geometry input (original order)
   int32_t n = 0;
-  int32_t max_species = 0;  // largest species channel of host-uploaded geometry
+  int32_t max_species = 0;  // largest species channel of a host-uploaded batch (single systems: checked on the device)
   // channel count of the model the next cell-list build serves: k_gather
   // flags channels outside [0, species_limit) on the device (device uploads)
   int32_t species_limit = INT32_MAX;
+  // pfw_evaluate reads the cell-list flags with its outputs (one synchronisation):
+  // prepare_check only queues their copy into flags_host while defer_check is set
+  bool defer_check = false, check_pending = false;
+  int32_t* flags_host = nullptr;  // pinned, 8 words
   std::vector<pfw::HostSystem> systems;
   uint64_t geometry_version = 0;  // bumped when the systems (count, sizes, cells) change
   int32_t n_owned = -1;           // atoms [0, n_owned) own E/W (domain decomposition); -1: all
@@ -147,7 +151,8 @@ namespace pfw {
 void prepare(pfw_ws* ws, double cutoff);
 bool prepare_plan(pfw_ws* ws, double cutoff);  // host plan; true if it already wrapped (open axes)
 void prepare_launch(pfw_ws* ws, bool wrap);    // device-only build, capturable
-void prepare_check(pfw_ws* ws);                // synchronise, raise on device flags
+void prepare_check(pfw_ws* ws);                // synchronise, raise on device flags (or queue them, deferred)
+void prepare_check_finish(pfw_ws* ws);         // after the caller's synchronisation: raise on deferred flags
 void exclusive_scan_i32(pfw_ws* ws, const int32_t* in, int32_t* out, int64_t n);  // out has n+1 entries
 void exclusive_scan_i64(pfw_ws* ws, const int32_t* in, int64_t* out, int64_t n);
 // reduce.cu: deterministic partial sums → E[0] and W[9] (either may be null)

@@ -14,11 +14,15 @@ Lux.  This module builds the pieces the library's surrogate path consumes:
   train            standardisation, seeded Xavier initialisation, training with
                    the library's kernels (pfw_mlp_train), BF16 rounding, gate
   Surrogate        the trained ensemble; params() gives the pfw_mlp_params view
+  train_forces     fine-tuning of every member on energies and forces
+  calibrate_gate   tau chosen from the force error the gate leaves behind
 
 Gate rule (recorded with each surrogate): per species and feature, the
 standardised training range widened by 5 % of its width on each side; and the
-ensemble standard deviation of a site energy at most tau = 1.5 × its 99.5th
-percentile over the training sites.
+ensemble standard deviation of a site energy at most tau.  train() sets tau
+to 1.5 × the 99.5th percentile over the training sites (an energy-only
+rule); calibrate_gate() replaces it by the largest tau whose evaluation
+meets a force-RMSE target against plain ACE on held-out systems.
 """
 from __future__ import annotations
 
@@ -483,3 +487,52 @@ def _train_forces(h, sur, lattices, dev, *, epochs, inner, batch, lr, lr_final, 
     sur.params = P.cpu().numpy().reshape(sur.params.shape)
     sur.force_history = hist
     return hist
+
+
+def calibrate_gate(h, sur: "Surrogate", full: PackedACE, feat: PackedACE, systems, target=2e-2,
+                   quantiles=(1.0, 0.95, 0.9, 0.85, 0.8, 0.75, 0.7, 0.6, 0.5, 0.4, 0.3, 0.2, 0.1)):
+    """Choose the ensemble-disagreement threshold tau from forces.
+
+    On the calibration systems (held out from training), plain FP64 ACE
+    forces are the judge.  tau runs down the quantiles of the sites' ensemble
+    standard deviation (numpy restatement of the deployed BF16 ensemble on
+    the library's features; quantile 1 means no disagreement gate); for each,
+    the surrogate is evaluated with its feature-range gate and that tau, and
+    the force RMSE against ACE over all systems is measured together with the
+    fallback fraction.  The first (largest) tau whose RMSE meets `target` is
+    kept in sur.tau; tau = 0 (every site falls back) reproduces ACE exactly,
+    so the walk ends there at the latest.  Returns the curve as a list of
+    dicts (quantile, tau, fallback_fraction, force_rmse)."""
+    from . import lib
+    h.ace(full)
+    h.surrogate(feat, sur, tau=np.inf)
+    refs, sds = [], []
+    for sy in systems:
+        h.set_geometry(sy.X, sy.H, sy.pbc, sy.species)
+        _, Fa, _ = h.evaluate(lib.MODEL_ACE, 7)
+        refs.append(Fa)
+        _, sd, _ = sur.predict(h.surrogate_features(), np.asarray(sy.species))
+        sds.append(sd)
+    sd_all = np.concatenate(sds)
+    curve = []
+    chosen = 0.0
+    for q in list(quantiles) + [None]:
+        tau = 0.0 if q is None else (np.inf if q >= 1.0 else float(np.quantile(sd_all, q)))
+        h.surrogate(feat, sur, tau=tau)
+        se, cnt, fb, ns = 0.0, 0, 0, 0
+        for sy, Fa in zip(systems, refs):
+            h.set_geometry(sy.X, sy.H, sy.pbc, sy.species)
+            _, Fs, _ = h.evaluate(lib.MODEL_SURROGATE, 7)
+            se += float(np.sum((Fs - Fa) ** 2))
+            cnt += Fs.size
+            f, n = h.surrogate_stats()
+            fb += f
+            ns += n
+        rmse = float(np.sqrt(se / max(cnt, 1)))
+        curve.append(dict(quantile=0.0 if q is None else float(q), tau=float(tau),
+                          fallback_fraction=fb / max(ns, 1), force_rmse=rmse))
+        if rmse <= target:
+            chosen = tau
+            break
+    sur.tau = float(chosen)
+    return curve

@@ -94,3 +94,59 @@ def test_energy_force_gradient_reference_matches_finite_differences():
     # without the force term it is the energy gradient
     _, ge = S.mlp_param_grad_reference(p, x, t, nin, H)
     assert np.allclose(S.mlp_ef_grad_reference(p, x, t, v, np.zeros(n), 1.0, nin, H), ge, rtol=1e-12, atol=1e-14)
+
+
+class FakeHandle:
+    """Stands in for lib.Handle in calibrate_gate: the surrogate's force error
+    is the ACE force scaled by the fraction of sites whose ensemble spread
+    does not exceed tau (those stay surrogate), so the RMSE falls as tau
+    falls and is zero at tau = 0."""
+
+    def __init__(self, sd):
+        self.sd, self.tau, self.n = sd, np.inf, len(sd)
+
+    def ace(self, model):
+        pass
+
+    def surrogate(self, feat, sur=None, tau=None):
+        self.tau = np.inf if tau is None else tau
+
+    def set_geometry(self, X, H, pbc, species):
+        pass
+
+    def evaluate(self, model, request):
+        F = np.ones((self.n, 3))
+        if model == 1:  # MODEL_ACE
+            return 0.0, F, None
+        keep = self.sd <= self.tau
+        return 0.0, F + 0.1 * keep.mean(), None
+
+    def surrogate_features(self):
+        return self.sd[:, None]
+
+    def surrogate_stats(self):
+        return int(np.sum(self.sd > self.tau)), self.n
+
+
+class FakeSurrogate:
+    def __init__(self, sd):
+        self.sd, self.tau = sd, 1.0
+
+    def predict(self, feats, species):
+        return None, feats[:, 0], None
+
+
+def test_calibrate_gate_keeps_the_largest_tau_that_meets_the_target():
+    from pfw_b200 import lib
+    assert lib.MODEL_ACE == 1
+    sd = np.linspace(0.01, 1.0, 100)
+    sys1 = WL.System(np.zeros((100, 3)), np.eye(3), (True, True, True), np.zeros(100, np.int32))
+    sur = FakeSurrogate(sd)
+    curve = S.calibrate_gate(FakeHandle(sd), sur, None, None, [sys1], target=0.0501)
+    # RMSE = 0.1 × (fraction kept): the first quantile keeping at most half of the sites is 0.5
+    assert curve[0]["quantile"] == 1.0 and abs(curve[0]["force_rmse"] - 0.1) < 1e-12
+    assert curve[-1]["force_rmse"] <= 0.0501 < curve[-2]["force_rmse"]
+    assert sur.tau == curve[-1]["tau"] == pytest.approx(np.quantile(sd, 0.5))
+    # an unreachable target walks down to tau = 0 (every site falls back)
+    curve = S.calibrate_gate(FakeHandle(sd), sur, None, None, [sys1], target=-1.0)
+    assert sur.tau == 0.0 and curve[-1]["fallback_fraction"] == 1.0
