@@ -412,6 +412,8 @@ def parse():
                    help="arithmetic of the headline workload (mixed: FP32 pair/ACE arithmetic, FP64 wrap and "
                         "Kahan energy/virial); the default fp64 is the reference's")
     p.add_argument("--no-tune", action="store_true", help="ACE workloads: the default site-kernel schedule")
+    p.add_argument("--sharded-forms", action="store_true",
+                   help="run the multi-GPU forms (slab exchange, sharded batch) also with one GPU")
     p.add_argument("--only-form", choices=["skin", "batch", "design", "surrogate"],
                    help="run one of the other configurations alone and print its record (no headline)")
     return p.parse_args()
@@ -463,10 +465,16 @@ def run_b200(args):
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
     dist = None
-    if world > 1:
+    if world > 1 or args.sharded_forms:
         import datetime
+        import socket
 
         import torch.distributed as dist
+        if world == 1 and "MASTER_PORT" not in os.environ:  # a one-rank group without a launcher
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(sk.getsockname()[1]), RANK="0",
+                                  WORLD_SIZE="1")
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     w = Workload(args.workload)
     if args.precision == "mixed":
@@ -503,6 +511,9 @@ def run_b200(args):
         t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
+    sharded = None
+    if (world > 1 and not args.no_forms) or args.sharded_forms:  # every rank, collectives in the same order
+        sharded = sharded_forms(dev, stream, flush, rank, world, dist)
     line = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -539,6 +550,8 @@ def run_b200(args):
         outputs = {w.name: dict(fp64=h.evaluate(w.model_sel, 7), fp64_key="headline", headline_ms=ms)}
         if not args.no_forms and world == 1:  # single-GPU configurations; the other ranks would idle at a barrier
             line["forms"] = forms(args, dev, stream, flush, F_ref, outputs)
+        if sharded:
+            line["forms_sharded"] = sharded
         if world == 1 and not args.no_cpu_baseline:
             cpu_baseline_leg(w, line, outputs, line.get("forms", {}))
     h.close()
@@ -551,6 +564,123 @@ def run_b200(args):
 
 
 MIXED_WORKLOADS = ("lj", "lj1m", "lj_shear", "smooth", "ace")
+
+
+def timed_ranks(fn, steps, warmup, flush, stream, dist):
+    """Warm-up, then `steps` CUDA-event-timed calls of fn on the launch stream
+    (L2 flush outside the events), bracketed by barriers; the mean step time,
+    maximised over ranks."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    dist.barrier()
+    st = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    en = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        st[k].record(stream)
+        fn()
+        en[k].record(stream)
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in zip(st, en)]))
+    t = torch.tensor([ms], dtype=torch.float64, device=flush.device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def sharded_forms(dev, stream, flush, rank, world, dist, steps=10, warmup=3):
+    """The two shapes that shard, run on every rank with one GPU each:
+
+    lj_slab: Lennard-Jones FCC 40 x 40 x 40·world (256,000 atoms per rank,
+    weak scaling) split into slabs along z; each step selects every rank's
+    boundary bands on its GPU (pfw_slab_bands), all-gathers the band sizes
+    and the bands, assembles owned atoms + the neighbours' bands as ghosts,
+    evaluates with pfw_set_owned and all-reduces E and W (parallel.slab_step_dist);
+    forces stay with their owners.  The box is world periodic copies of the
+    headline box, so its energy is world × the headline energy.
+
+    ace_batch4096_sharded: the 4096-system ACE batch sharded over the ranks
+    by longest-processing-time on expected edges (parallel.shard); each step
+    replays every rank's batch graph and all-gathers the per-system energy
+    and virial rows."""
+    import torch
+
+    from pfw_b200 import ace_generate as G
+    from pfw_b200 import lib
+    from pfw_b200 import parallel as PAR
+    from pfw_b200 import workloads as WL
+    from pfw_b200.ace_model import read_resolved
+    out = {}
+    # ---- one box in slabs ----
+    base = WL.lj_fcc(seed=2, nc=40)
+    Hz = base.H[:, 2].copy()
+    H = base.H.copy()
+    H[:, 2] *= world
+    sysw = WL.System(np.concatenate([base.X + k * Hz for k in range(world)]), H, base.pbc,
+                     np.zeros(world * len(base.X), np.int32))
+    plan = PAR.SlabPlan(sysw, world, WL.LJ_CUTOFF)
+    h = lib.Handle(lib.FP64, device=dev.index)
+    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+    h.lj(WL.LJ_EPS, WL.LJ_SIGMA, WL.LJ_CUTOFF)
+    rk = PAR.SlabRank(h, plan, rank, dev)
+    E = torch.zeros(1, dtype=torch.float64, device=dev)
+    W = torch.zeros(9, dtype=torch.float64, device=dev)
+    F = torch.zeros((2 * rk.n_owned + 4096, 3), dtype=torch.float64, device=dev)
+    res = {}
+
+    def slab_step():
+        res["t"] = PAR.slab_step_dist(rk, E, F, W, lib.MODEL_PAIR)
+
+    ms = timed_ranks(slab_step, steps, warmup, flush, stream, dist)
+    e_total = float(res["t"][0].item())
+    h.set_geometry(base.X, base.H, base.pbc, base.species)
+    e_one = h.evaluate(lib.MODEL_PAIR, 7)[0]
+    out["lj_slab_weak"] = dict(value=len(sysw.X) / (ms * 1e-3), unit="atoms/s", ms_per_step=ms, atoms=len(sysw.X),
+                               atoms_per_rank=len(base.X), ranks=world, scaling="weak",
+                               energy_rel_vs_world_x_headline=abs(e_total - world * e_one) / abs(world * e_one),
+                               note="per step: bands on each GPU, all-gather of band sizes and bands (NCCL), "
+                                    "owned + ghosts assembled on the device, pfw_evaluate with owned shares, "
+                                    "all-reduce of E and W; forces stay with their owners")
+    h.close()
+    # ---- the batch, sharded ----
+    model = read_resolved(G.generate_b2_model())
+    systems = WL.batched(seed=5, nsys=4096)
+    parts = PAR.shard(PAR.system_costs(systems, model.cutoff), world)
+    mine = [systems[k] for k in parts[rank]]
+    h = lib.Handle(lib.FP64, device=dev.index)
+    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+    h.ace(model)
+    h.check(h.L.pfw_ace_set_schedule(h.ws, 8, 8))
+    h.set_batch(mine)
+    nsys, n, nfeat = len(mine), h.n, h.feature_count()
+    Eb = torch.zeros(max(nsys, 1), dtype=torch.float64, device=dev)
+    Fb = torch.zeros(3 * max(n, 1), dtype=torch.float64, device=dev)
+    Wb = torch.zeros(9 * max(nsys, 1), dtype=torch.float64, device=dev)
+    Xb = torch.zeros(max(nsys * nfeat, 1), dtype=torch.float64, device=dev)
+    ptrs = [ctypes.c_void_p(t.data_ptr()) for t in (Eb, Fb, Wb, Xb)]
+    width = max(len(p) for p in parts)
+    rows = torch.zeros((width, 10), dtype=torch.float64, device=dev)
+    gathered = [torch.zeros_like(rows) for _ in range(world)]
+
+    def batch_step():
+        h.batch_graph_launch(7, *ptrs)
+        rows[:nsys, 0] = Eb[:nsys]
+        rows[:nsys, 1:] = Wb[: 9 * nsys].reshape(nsys, 9)
+        dist.all_gather(gathered, rows)
+
+    ms = timed_ranks(batch_step, steps, warmup, flush, stream, dist)
+    h.batch_graph_sync()
+    atoms = sum(len(sy.species) for sy in systems)
+    out["ace_batch4096_sharded"] = dict(value=atoms / (ms * 1e-3), unit="atoms/s", ms_per_step=ms, atoms=atoms,
+                                        systems=len(systems), ranks=world, scaling="strong",
+                                        largest_shard_atoms=int(max(sum(len(systems[k].species) for k in p)
+                                                                    for p in parts)),
+                                        note="LPT shards on expected edges; per step every rank replays its batch "
+                                             "graph and the per-system E/W rows are all-gathered (NCCL)")
+    h.close()
+    return out
 
 
 def forms(args, dev, stream, flush, F_head, outputs):

@@ -93,6 +93,19 @@ pfw_status pfw_set_geometry_device(pfw_ws* ws, int64_t n, const double* X_dev,
  * whole system's.  -1 (the default after every geometry upload) = all. */
 pfw_status pfw_set_owned(pfw_ws* ws, int64_t n_owned);
 
+/* Slab decomposition, the per-step exchange's device half (no counterpart in
+ * the reference): of a rank's n owned atoms (X_dev 3×N, species_dev on the
+ * device), the ones whose fractional coordinate along the slab axis,
+ * f = frac_row·x (frac_row: that row of H⁻¹), lies below lo + d (lower band)
+ * and at or above hi - d (upper band), in their owned order, written as
+ * (x, y, z, species) quadruples of doubles with shift_lower / shift_upper
+ * (Cartesian, Å) added: the neighbouring ranks' ghost atoms.  lower_dev and
+ * upper_dev hold 4·n doubles; counts_dev[0..1] receive the band sizes.  Runs
+ * on the workspace's stream without synchronising. */
+pfw_status pfw_slab_bands(pfw_ws* ws, int64_t n, const double* X_dev, const int32_t* species_dev,
+                          const double frac_row[3], double lo, double hi, double d, const double shift_lower[3],
+                          const double shift_upper[3], double* lower_dev, double* upper_dev, int32_t* counts_dev);
+
 /* ---- pair models ------------------------------------------------------ */
 /* SmoothPair(labels, amplitudes, cutoff): U_ab(r) = A_ab (1 - r²/c²)³
  * (PairPotentials/models.jl:28-44 and PreparedSmooth :138-176).

@@ -181,7 +181,7 @@ void pfw_ws_destroy(pfw_ws* ws) {
   pfw::DevBuf* bufs[] = {&ws->X, &ws->species, &ws->atom_sys, &ws->sysgeom, &ws->wrapped, &ws->bincoord,
                          &ws->wind, &ws->cellid, &ws->slot, &ws->cell_count, &ws->cell_start, &ws->cell_sys,
                          &ws->tmp_idx, &ws->perm, &ws->inverse, &ws->pos, &ws->pos32, &ws->scan_tmp,
-                         &ws->minmax, &ws->cellpart, &ws->out_E, &ws->out_F, &ws->out_W, &ws->out_feat, &ws->counters, &ws->red_partial, &ws->pair_slots,
+                         &ws->minmax, &ws->slab_scratch, &ws->cellpart, &ws->out_E, &ws->out_F, &ws->out_W, &ws->out_feat, &ws->counters, &ws->red_partial, &ws->pair_slots,
                          &ws->nb_count, &ws->nb_offsets, &ws->nb_j, &ws->nb_S, &ws->nb_R};
   for (auto* b : bufs) b->release();
   for (auto& e : ws->ev)
@@ -207,6 +207,16 @@ pfw_status pfw_set_owned(pfw_ws* ws, int64_t n_owned) {
     if (ws->systems.size() != 1) throw Error(PFW_ESTATE, "owned atoms apply to a single-system geometry");
     if (n_owned < -1 || n_owned > ws->n) throw Error(PFW_EINVAL, "owned atom count out of range");
     ws->n_owned = (int32_t)n_owned;
+  });
+}
+
+pfw_status pfw_slab_bands(pfw_ws* ws, int64_t n, const double* X_dev, const int32_t* species_dev,
+                          const double frac_row[3], double lo, double hi, double d, const double shift_lower[3],
+                          const double shift_upper[3], double* lower_dev, double* upper_dev, int32_t* counts_dev) {
+  return guarded(ws, [&] {
+    if (!frac_row || !shift_lower || !shift_upper) throw Error(PFW_EINVAL, "slab axis row and shifts required");
+    pfw::slab_bands(ws, n, X_dev, species_dev, frac_row, lo, hi, d, shift_lower, shift_upper, lower_dev, upper_dev,
+                    counts_dev);
   });
 }
 

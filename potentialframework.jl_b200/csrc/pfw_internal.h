@@ -119,6 +119,7 @@ struct pfw_ws {
   // pair evaluation
   pfw::PairModel pair;
   pfw::DevBuf cellpart, out_E, out_F, out_W, out_feat, counters, red_partial, out_design, out_base;
+  pfw::DevBuf slab_scratch;  // band flags and offsets of pfw_slab_bands
   pfw::DevBuf pair_slots;  // per-(slot, sorted atom) partial forces of the half-stencil pair kernel
   int64_t last_pairs = -1;
   // neighbour snapshot
@@ -173,6 +174,9 @@ bool pair_half_eligible(const Prepared& P);
 void pair_half_setup();
 void pair_half_kernel(pfw_ws* ws, const PairParams& prm, double* parts, unsigned long long* np);
 void pair_half_fold(pfw_ws* ws, double* F);
+void slab_bands(pfw_ws* ws, int64_t n, const double* X, const int32_t* species, const double fr[3], double lo,
+                double hi, double d, const double sl[3], const double su[3], double* lower, double* upper,
+                int32_t* counts);
 // snapshot.cu
 int64_t neighbour_build(pfw_ws* ws, double cutoff, bool with_R = true);
 void neighbour_fill(pfw_ws* ws, int64_t* offsets, int32_t* j, int32_t* S, double* R);

@@ -15,7 +15,7 @@ import sys
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "lib", "libpfw_b200.so")
-SOURCES = ["geometry.cu", "reduce.cu", "pair.cu", "pair_half.cu", "snapshot.cu", "ace.cu", "capi.cu", "noalloc.cu", "mlp.cu", "skin.cu"]
+SOURCES = ["geometry.cu", "reduce.cu", "pair.cu", "pair_half.cu", "snapshot.cu", "ace.cu", "capi.cu", "noalloc.cu", "mlp.cu", "skin.cu", "slab.cu"]
 
 
 def nvcc():

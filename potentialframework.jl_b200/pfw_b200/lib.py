@@ -83,6 +83,7 @@ def load():
     L.pfw_batch_graph_launch.argtypes = [vp, C.c_uint32, vp, vp, vp, vp]
     L.pfw_batch_graph_sync.argtypes = [vp]
     L.pfw_set_owned.argtypes = [vp, C.c_int64]
+    L.pfw_slab_bands.argtypes = [vp, C.c_int64, vp, vp, dp, C.c_double, C.c_double, C.c_double, dp, dp, vp, vp, vp]
     L.pfw_pair_set_skin.argtypes = [vp, C.c_double]
     L.pfw_pair_skin_stats.argtypes = [vp, i64p, i64p]
     L.pfw_surrogate_load.argtypes = [vp, C.POINTER(pfw_ace_tables), vp]
@@ -157,6 +158,16 @@ class Handle:
 
     def set_owned(self, n_owned):
         self.check(self.L.pfw_set_owned(self.ws, int(n_owned)))
+
+    def slab_bands(self, n, X_ptr, species_ptr, frac_row, lo, hi, d, shift_lower, shift_upper, lower_ptr,
+                   upper_ptr, counts_ptr):
+        """pfw_slab_bands on device buffers (pointers); queued on the workspace's stream."""
+        fr = np.ascontiguousarray(frac_row, dtype=np.float64).reshape(3)
+        sl = np.ascontiguousarray(shift_lower, dtype=np.float64).reshape(3)
+        su = np.ascontiguousarray(shift_upper, dtype=np.float64).reshape(3)
+        self.check(self.L.pfw_slab_bands(self.ws, int(n), X_ptr, species_ptr, ptr(fr, C.c_double), float(lo),
+                                         float(hi), float(d), ptr(sl, C.c_double), ptr(su, C.c_double), lower_ptr,
+                                         upper_ptr, counts_ptr))
 
     def pair_skin(self, skin):
         self.check(self.L.pfw_pair_set_skin(self.ws, float(skin)))
