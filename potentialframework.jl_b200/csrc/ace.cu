@@ -149,7 +149,9 @@ __global__ void __launch_bounds__(128)
                            });
 }
 
-// Reverse edge of e = (i→j, S): the entry (j→i, -S) of j's list.
+// Reverse edge of e = (i→j, S): the entry (j→i, -S) of j's list.  One warp
+// per atom, a lane per edge; j's list is scanned four entries per step so
+// that four loads are in flight.
 __global__ void k_edge_rev(int n, const int* __restrict__ off, int cap, const int* __restrict__ ej,
                            const int4* __restrict__ eS, int* __restrict__ rev, int* __restrict__ status) {
   const int i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
@@ -161,12 +163,15 @@ __global__ void k_edge_rev(int n, const int* __restrict__ off, int cap, const in
     const int4 s = eS[e];
     int found = -1;
     const int f1 = min(off[j + 1], cap);
-    for (int f = min(off[j], cap); f < f1; ++f) {
-      if (ej[f] == i) {
-        const int4 t = eS[f];
-        if (t.x == -s.x && t.y == -s.y && t.z == -s.z) {
-          found = f;
-          break;
+    for (int f = min(off[j], cap); f < f1 && found < 0; f += 4) {
+      int c[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) c[u] = f + u < f1 ? ej[f + u] : -1;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (found < 0 && c[u] == i) {
+          const int4 t = eS[f + u];
+          if (t.x == -s.x && t.y == -s.y && t.z == -s.z) found = f + u;
         }
       }
     }
@@ -175,23 +180,37 @@ __global__ void k_edge_rev(int n, const int* __restrict__ off, int cap, const in
   }
 }
 
-// F_k = Σ_{e ∈ out(k)} g_e - g_rev(e), written in original order.
+// F_k = Σ_{e ∈ out(k)} g_e - g_rev(e), written in original order.  Eight
+// lanes per atom stride over its out-edges; their sums are combined by a
+// fixed three-step shuffle tree, so the order of every addition is fixed.
+constexpr int GATHER_LANES = 8;
+
 __global__ void k_ace_gather(int n, const int* __restrict__ off, int cap, const int* __restrict__ rev,
                              const double* __restrict__ g, const int* __restrict__ perm, double* __restrict__ F) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = t / GATHER_LANES, q = t % GATHER_LANES;
   double f0 = 0, f1 = 0, f2 = 0;
-  const int e1 = min(off[k + 1], cap);
-  for (int e = min(off[k], cap); e < e1; ++e) {
-    const int r = rev[e];
-    f0 += g[3 * (size_t)e] - g[3 * (size_t)r];
-    f1 += g[3 * (size_t)e + 1] - g[3 * (size_t)r + 1];
-    f2 += g[3 * (size_t)e + 2] - g[3 * (size_t)r + 2];
+  if (k < n) {
+    const int e1 = min(off[k + 1], cap);
+    for (int e = min(off[k], cap) + q; e < e1; e += GATHER_LANES) {
+      const int r = rev[e];
+      f0 += g[3 * (size_t)e] - g[3 * (size_t)r];
+      f1 += g[3 * (size_t)e + 1] - g[3 * (size_t)r + 1];
+      f2 += g[3 * (size_t)e + 2] - g[3 * (size_t)r + 2];
+    }
   }
-  const int o = perm[k];
-  F[3 * o] = f0;
-  F[3 * o + 1] = f1;
-  F[3 * o + 2] = f2;
+#pragma unroll
+  for (int o = GATHER_LANES / 2; o > 0; o >>= 1) {
+    f0 += __shfl_xor_sync(0xffffffffu, f0, o);
+    f1 += __shfl_xor_sync(0xffffffffu, f1, o);
+    f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+  }
+  if (k < n && q == 0) {
+    const int o = perm[k];
+    F[3 * o] = f0;
+    F[3 * o + 1] = f1;
+    F[3 * o + 2] = f2;
+  }
 }
 
 // Site energies in original order.
@@ -688,7 +707,7 @@ static void sites_launch(pfw_ws* ws, AceDevice* a, uint32_t req, int nunits, con
   ws->stage_begin(2);
   if (F_dev && n > 0) {
     if (want_grad) {
-      k_ace_gather<<<grid_for(n, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(), s.g,
+      k_ace_gather<<<grid_for((int64_t)n * GATHER_LANES, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(), s.g,
                                                      ws->perm.as<int>(), F_dev);
       ws->launches += 1;
     } else {
@@ -1333,7 +1352,7 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   ws->stage_begin(2);
   if (F_dev && n > 0) {
     if (want_grad) {
-      k_ace_gather<<<grid_for(n, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(),
+      k_ace_gather<<<grid_for((int64_t)n * GATHER_LANES, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(),
                                                      a->edge_g.as<double>(), ws->perm.as<int>(), F_dev);
       ws->launches += 1;
     } else {
@@ -1385,7 +1404,7 @@ void sur_pullback(pfw_ws* ws, const double* dEdx_dev, double* F_dev) {
     s.want_grad = true;
     const AceTables p = tables_of(a);
     dispatch_sites<double, 2>(a->lmax, p, choose_sur_layout(p, ws->opt.device, 2), s, st, ws->opt.device);
-    k_ace_gather<<<grid_for(n, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(),
+    k_ace_gather<<<grid_for((int64_t)n * GATHER_LANES, 128), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_rev.as<int>(),
                                                    a->edge_g.as<double>(), ws->perm.as<int>(), F_dev);
     ws->launches += 3;
   }
