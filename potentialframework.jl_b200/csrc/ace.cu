@@ -58,6 +58,8 @@ struct AceDevice {
   DevBuf crow_off, crow_k, crow_val;
   // per evaluation
   DevBuf edge_count, edge_off, edge_j, edge_d, edge_S, edge_rev, edge_g, site_out, site_E_orig, status;
+  DevBuf edge_countp;  // per stencil part (but the last) and atom: the part's edge count
+  int edge_parts = 1;
   DevBuf unit_begin, unit_out;  // single system: one unit per site
   // batch: units of at most BATCH_UNIT_SITES sites, never spanning two systems
   DevBuf batch_units, batch_sys_units, batch_out, batch_feat;
@@ -82,71 +84,93 @@ struct AceDevice {
 // ---------------------------------------------------------------------------
 // environments
 // ---------------------------------------------------------------------------
+// Environments of a home cell's atoms over one part of the stencil (the
+// stencil split in order into `parts` ranges, one warp each): the edge count
+// of every atom is added to count (integers: order-free), and the part's own
+// count is kept in countp[part][atom] for the parts after it.
 template <int MODE>
 __global__ void __launch_bounds__(128)
     k_edge_count(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
-                 const double4* __restrict__ pos, int ncells, int* __restrict__ count) {
+                 const double4* __restrict__ pos, int ncells, int parts, int natoms, int* __restrict__ count,
+                 int* __restrict__ countp) {
   __shared__ WarpStage stage[4];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cell = blockIdx.x * 4 + warp;
+  const int w = blockIdx.x * 4 + warp;
+  const int cell = w / parts, part = w - cell * parts;
   if (cell >= ncells) return;
   const SysGeom& g = sysv[cell_sys[cell]];
   int cur = -1, cnt = 0;
-  warp_traverse_cell<MODE>(g, cell, cell_start, pos, stage[warp], lane,
-                           [&](int i, int, const double4&, const double4&, const StencilEntry&, const double*, double) {
-                             if (i != cur) {
-                               if (cur >= 0) count[cur] = cnt;
-                               cur = i;
-                               cnt = 0;
-                             }
-                             ++cnt;
-                           });
-  if (cur >= 0) count[cur] = cnt;
+  auto flush = [&]() {
+    if (cur < 0) return;
+    if (parts == 1) {
+      count[cur] = cnt;
+    } else {
+      atomicAdd(count + cur, cnt);
+      if (part < parts - 1) countp[(size_t)part * natoms + cur] = cnt;
+    }
+  };
+  warp_traverse_cell<MODE>(
+      g, cell, cell_start, pos, stage[warp], lane,
+      [&](int i, int, const double4&, const double4&, const StencilEntry&, const double*, double) {
+        if (i != cur) {
+          flush();
+          cur = i;
+          cnt = 0;
+        }
+        ++cnt;
+      },
+      part, parts);
+  flush();
 }
 
 // Writes edges below `cap` only; an edge past the capacity sets status bit 8.
+// A part's edges of atom i start after the earlier parts' (countp).
 template <int MODE>
 __global__ void __launch_bounds__(128)
     k_edge_fill(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
                 const double4* __restrict__ pos, const int* __restrict__ perm, const int* __restrict__ wind,
-                const double* __restrict__ X, int ncells, const int* __restrict__ off, int cap, int* __restrict__ ej,
-                int4* __restrict__ eS, double4* __restrict__ ed, int* __restrict__ status) {
+                const double* __restrict__ X, int ncells, int parts, int natoms, const int* __restrict__ countp,
+                const int* __restrict__ off, int cap, int* __restrict__ ej, int4* __restrict__ eS,
+                double4* __restrict__ ed, int* __restrict__ status) {
   __shared__ WarpStage stage[4];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cell = blockIdx.x * 4 + warp;
+  const int w = blockIdx.x * 4 + warp;
+  const int cell = w / parts, part = w - cell * parts;
   if (cell >= ncells) return;
   const SysGeom& g = sysv[cell_sys[cell]];
   int cur = -1, o = 0, a = 0;
   int wi[3] = {0, 0, 0};
   double xi[3] = {0, 0, 0};
-  warp_traverse_cell<MODE>(g, cell, cell_start, pos, stage[warp], lane,
-                           [&](int i, int j, const double4& pi, const double4& pj, const StencilEntry& se,
-                               const double*, double) {
-                             if (i != cur) {
-                               cur = i;
-                               o = off[i];
-                               a = perm[i];
-                               wi[0] = wind[3 * a]; wi[1] = wind[3 * a + 1]; wi[2] = wind[3 * a + 2];
-                               xi[0] = X[3 * a]; xi[1] = X[3 * a + 1]; xi[2] = X[3 * a + 2];
-                             }
-                             if (o >= cap) {
-                               atomicOr(status, 8);
-                               ++o;
-                               return;
-                             }
-                             const int b = perm[j];
-                             const int wj[3] = {wind[3 * b], wind[3 * b + 1], wind[3 * b + 2]};
-                             int S[3];
-                             pair_image(g, se, pi, pj, wi, wj, S);
-                             // edge_displacement: X_j - X_i + Hz·S ((t1 + t2) + t3)
-                             double sh[3];
-                             xmatvec(g.Hz, (double)S[0], (double)S[1], (double)S[2], sh);
-                             ej[o] = j;
-                             eS[o] = make_int4(S[0], S[1], S[2], 0);
-                             ed[o] = make_double4(xadd(xsub(X[3 * b], xi[0]), sh[0]), xadd(xsub(X[3 * b + 1], xi[1]), sh[1]),
-                                                  xadd(xsub(X[3 * b + 2], xi[2]), sh[2]), pj.w);
-                             ++o;
-                           });
+  warp_traverse_cell<MODE>(
+      g, cell, cell_start, pos, stage[warp], lane,
+      [&](int i, int j, const double4& pi, const double4& pj, const StencilEntry& se, const double*, double) {
+        if (i != cur) {
+          cur = i;
+          o = off[i];
+          for (int q = 0; q < part; ++q) o += countp[(size_t)q * natoms + i];
+          a = perm[i];
+          wi[0] = wind[3 * a]; wi[1] = wind[3 * a + 1]; wi[2] = wind[3 * a + 2];
+          xi[0] = X[3 * a]; xi[1] = X[3 * a + 1]; xi[2] = X[3 * a + 2];
+        }
+        if (o >= cap) {
+          atomicOr(status, 8);
+          ++o;
+          return;
+        }
+        const int b = perm[j];
+        const int wj[3] = {wind[3 * b], wind[3 * b + 1], wind[3 * b + 2]};
+        int S[3];
+        pair_image(g, se, pi, pj, wi, wj, S);
+        // edge_displacement: X_j - X_i + Hz·S ((t1 + t2) + t3)
+        double sh[3];
+        xmatvec(g.Hz, (double)S[0], (double)S[1], (double)S[2], sh);
+        ej[o] = j;
+        eS[o] = make_int4(S[0], S[1], S[2], 0);
+        ed[o] = make_double4(xadd(xsub(X[3 * b], xi[0]), sh[0]), xadd(xsub(X[3 * b + 1], xi[1]), sh[1]),
+                             xadd(xsub(X[3 * b + 2], xi[2]), sh[2]), pj.w);
+        ++o;
+      },
+      part, parts);
 }
 
 // Reverse edge of e = (i→j, S): the entry (j→i, -S) of j's list.  One warp
@@ -316,7 +340,7 @@ static void free_device(AceDevice* a) {
                     &a->q_len, &a->q_nodes, &a->q_coeff, &a->q_tr, &a->q_pow, &a->q_envk, &a->q_env,
                     &a->density, &a->dn_off, &a->dn, &a->dm_off, &a->dm, &a->prods, &a->term_off, &a->terms,
                     &a->weights, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm, &a->crow_off, &a->crow_k, &a->crow_val,
-                    &a->edge_count, &a->edge_off, &a->edge_j, &a->edge_d, &a->edge_S, &a->edge_rev, &a->edge_g,
+                    &a->edge_count, &a->edge_countp, &a->edge_off, &a->edge_j, &a->edge_d, &a->edge_S, &a->edge_rev, &a->edge_g,
                     &a->site_out, &a->site_E_orig, &a->status, &a->unit_begin, &a->unit_out,
                     &a->batch_units, &a->batch_sys_units, &a->batch_out, &a->batch_feat, &a->design_G,
                     &a->design_order};
@@ -609,23 +633,36 @@ static bool shift_mode(const Prepared& P) {
   return true;
 }
 
+// Stencil parts per home cell for the environment kernels: enough warps to
+// fill the GPU when the cells are few (at most 3 parts of the 27 entries).
+static int edge_parts(const Prepared& P) {
+  const int want = 148 * 16;
+  return std::max(1, std::min(3, (want + std::max(P.ncells, 1) - 1) / std::max(P.ncells, 1)));
+}
+
 // count + scan of the environments (no host synchronisation)
 static void edges_count_launch(pfw_ws* ws, AceDevice* a) {
   const Prepared& P = ws->prep;
   cudaStream_t st = ws->stream;
   const int n = P.n;
+  const int parts = edge_parts(P);
   int* count = a->edge_count.as<int>();
+  int* countp = static_cast<int*>(a->edge_countp.ensure(sizeof(int) * (size_t)std::max(n, 1) * std::max(parts - 1, 1)));
   PFW_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * std::max(n, 1), st));
-  const dim3 grid(grid_for(P.ncells, 4)), block(128);
+  if (parts > 1) PFW_CUDA(cudaMemsetAsync(countp, 0, sizeof(int) * (size_t)n * (parts - 1), st));
+  const dim3 grid(grid_for((int64_t)P.ncells * parts, 4)), block(128);
   if (P.ncells > 0) {
     if (shift_mode(P))
       k_edge_count<0><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(),
-                                              ws->cell_start.as<int>(), ws->pos.as<double4>(), P.ncells, count);
+                                              ws->cell_start.as<int>(), ws->pos.as<double4>(), P.ncells, parts, n,
+                                              count, countp);
     else
       k_edge_count<1><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(),
-                                              ws->cell_start.as<int>(), ws->pos.as<double4>(), P.ncells, count);
+                                              ws->cell_start.as<int>(), ws->pos.as<double4>(), P.ncells, parts, n,
+                                              count, countp);
     ws->launches += 1;
   }
+  a->edge_parts = parts;
   exclusive_scan_i32(ws, count, a->edge_off.as<int>(), n);
 }
 
@@ -634,19 +671,23 @@ static void edges_fill_launch(pfw_ws* ws, AceDevice* a) {
   const Prepared& P = ws->prep;
   cudaStream_t st = ws->stream;
   const int n = P.n;
-  const dim3 grid(grid_for(P.ncells, 4)), block(128);
+  const int parts = a->edge_parts;
+  const dim3 grid(grid_for((int64_t)P.ncells * parts, 4)), block(128);
   int* status = a->status.as<int>();
+  const int* countp = a->edge_countp.as<int>();
   if (P.ncells > 0 && a->cap > 0) {
     if (shift_mode(P))
       k_edge_fill<0><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(), ws->cell_start.as<int>(),
                                              ws->pos.as<double4>(), ws->perm.as<int>(), ws->wind.as<int>(),
-                                             ws->X.as<double>(), P.ncells, a->edge_off.as<int>(), a->cap,
-                                             a->edge_j.as<int>(), a->edge_S.as<int4>(), a->edge_d.as<double4>(), status);
+                                             ws->X.as<double>(), P.ncells, parts, n, countp, a->edge_off.as<int>(),
+                                             a->cap, a->edge_j.as<int>(), a->edge_S.as<int4>(), a->edge_d.as<double4>(),
+                                             status);
     else
       k_edge_fill<1><<<grid, block, 0, st>>>(ws->sysgeom.as<SysGeom>(), ws->cell_sys.as<int>(), ws->cell_start.as<int>(),
                                              ws->pos.as<double4>(), ws->perm.as<int>(), ws->wind.as<int>(),
-                                             ws->X.as<double>(), P.ncells, a->edge_off.as<int>(), a->cap,
-                                             a->edge_j.as<int>(), a->edge_S.as<int4>(), a->edge_d.as<double4>(), status);
+                                             ws->X.as<double>(), P.ncells, parts, n, countp, a->edge_off.as<int>(),
+                                             a->cap, a->edge_j.as<int>(), a->edge_S.as<int4>(), a->edge_d.as<double4>(),
+                                             status);
     k_edge_rev<<<grid_for(n, 4), 128, 0, st>>>(n, a->edge_off.as<int>(), a->cap, a->edge_j.as<int>(),
                                                a->edge_S.as<int4>(), a->edge_rev.as<int>(), status);
     ws->launches += 2;

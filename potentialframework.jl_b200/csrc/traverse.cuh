@@ -110,13 +110,15 @@ __device__ __forceinline__ void drain_lists(const SysGeom& g, const double4* __r
 template <int MODE, class Stage, class Drain, class ChunkEnd>
 __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const int* __restrict__ cell_start,
                                                const double4* __restrict__ pos, Stage& stage, int lane,
-                                               Drain&& drain, ChunkEnd&& chunk_end) {
+                                               Drain&& drain, ChunkEnd&& chunk_end, int part = 0, int parts = 1) {
   const int b = cell_start[cell], e = cell_start[cell + 1];
   if (b == e) return;
   const int local = cell - g.cell_begin;
   const int key[3] = {local / (g.dims[1] * g.dims[2]), (local / g.dims[2]) % g.dims[1], local % g.dims[2]};
   const int cnt0 = stencil_count(g, 0), cnt1 = stencil_count(g, 1), cnt2 = stencil_count(g, 2);
-  const int nstencil = cnt0 * cnt1 * cnt2;
+  const int nall = cnt0 * cnt1 * cnt2;
+  // stencil entries [k_first, nstencil) of this part (parts split the stencil in order)
+  const int k_first = (int)((int64_t)part * nall / parts), nstencil = (int)((int64_t)(part + 1) * nall / parts);
   const float c2hi = (float)g.c2 * PREFILTER_GUARD;
   constexpr int RING = Stage::ring;
   constexpr bool PAIR = RING == 2 * TRAVERSE_STAGE;  // the pair kernels' staging
@@ -145,7 +147,7 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
       }
     }
     int cnt = 0;
-    for (int s0 = 0; s0 < nstencil; s0 += LIST_NE) {
+    for (int s0 = k_first; s0 < nstencil; s0 += LIST_NE) {
       // ---- resolve up to 32 stencil entries, one per lane ----
       __syncwarp();
       int len = 0, jb = 0;
@@ -310,13 +312,13 @@ __device__ __forceinline__ void traverse_lists(const SysGeom& g, int cell, const
 template <int MODE, class Visit>
 __device__ __forceinline__ void warp_traverse_cell(const SysGeom& g, int cell, const int* __restrict__ cell_start,
                                                    const double4* __restrict__ pos, WarpStage& stage, int lane,
-                                                   Visit&& visit) {
+                                                   Visit&& visit, int part = 0, int parts = 1) {
   traverse_lists<MODE>(
       g, cell, cell_start, pos, stage, lane,
       [&](bool have, int i, const double4& pi, int& cnt) {
         drain_lists<MODE>(g, pos, stage, lane, have, i, pi, cnt, visit);
       },
-      [](bool, int, const double4&) {});
+      [](bool, int, const double4&) {}, part, parts);
 }
 
 // Integer image of the directed pair i→j relative to the ORIGINAL
