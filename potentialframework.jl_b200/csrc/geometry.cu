@@ -413,10 +413,16 @@ __global__ void k_cell_order(int ncells, const SysGeom* __restrict__ sys, int ns
     cell_sys[cell] = lo;
     if (e > b) atomicMax(maxpop, e - b);
   }
+  const int pop = e - b;
   for (int t = b + lane; t < e; t += 32) {
     const int me = tmp[t];
     int rank = 0;
-    for (int u = b; u < e; ++u) rank += tmp[u] < me;
+    if (pop <= 32) {
+      // the whole cell is in this warp's lanes: count smaller indices by shuffles
+      for (int u = 0; u < pop; ++u) rank += __shfl_sync(pop == 32 ? 0xffffffffu : (1u << pop) - 1u, me, u) < me;
+    } else {
+      for (int u = b; u < e; ++u) rank += tmp[u] < me;
+    }
     const int k = b + rank;
     perm[k] = me;
     int z = species[me];
