@@ -471,23 +471,43 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         double dummy = 0.0;
         ace_chunk_edges<L, T, true>(p, gb, lay, es, edge_d, eb + c0, nc, iz, lt, dummy, status, wq, s_radp);
         group_sync(g);
-        for (int idx = lt; idx < nc * nR; idx += ACE_GROUP) {
-          const int t = idx / nR, n = idx - t * nR;
-          T acc = T(0);
-          for (int q = s_dnoff[n]; q < s_dnoff[n + 1]; ++q) {
-            const int2 am = s_dn[q];
-            acc += (T)dA[am.x] * (T)Yc[t * YS + am.y];
+        // T1[t, n] = Σ_{(a, m) of radial n} dA[a]·Y[t, m], T2[t, m] = Σ_{(a, n) of order m} dA[a]·R[t, n]:
+        // a task is one column (n of T1, then m of T2) for up to four edges, so
+        // the column's (a, ·) list and dA values are read once per four edges
+        {
+          constexpr int EB = 4;
+          const int ncol = nR + nY, nblk = (nc + EB - 1) / EB;
+          for (int task = lt; task < ncol * nblk; task += ACE_GROUP) {
+            const int blk = task / ncol, col = task - blk * ncol;
+            const int t0 = blk * EB, tn = min(EB, nc - t0);
+            T acc[EB];
+#pragma unroll
+            for (int u = 0; u < EB; ++u) acc[u] = T(0);
+            if (col < nR) {
+              for (int q = s_dnoff[col]; q < s_dnoff[col + 1]; ++q) {
+                const int2 am = s_dn[q];
+                const T w = (T)dA[am.x];
+#pragma unroll
+                for (int u = 0; u < EB; ++u)
+                  if (u < tn) acc[u] += w * (T)Yc[(t0 + u) * YS + am.y];
+              }
+#pragma unroll
+              for (int u = 0; u < EB; ++u)
+                if (u < tn) T1[(t0 + u) * RS + col] = acc[u];
+            } else {
+              const int m = col - nR;
+              for (int q = s_dmoff[m]; q < s_dmoff[m + 1]; ++q) {
+                const int2 an = s_dm[q];
+                const T w = (T)dA[an.x];
+#pragma unroll
+                for (int u = 0; u < EB; ++u)
+                  if (u < tn) acc[u] += w * (T)Rc[(t0 + u) * RS + an.y];
+              }
+#pragma unroll
+              for (int u = 0; u < EB; ++u)
+                if (u < tn) T2[(t0 + u) * YS + m] = acc[u];
+            }
           }
-          T1[t * RS + n] = acc;
-        }
-        for (int idx = lt; idx < nc * nY; idx += ACE_GROUP) {
-          const int t = idx / nY, m = idx - t * nY;
-          T acc = T(0);
-          for (int q = s_dmoff[m]; q < s_dmoff[m + 1]; ++q) {
-            const int2 an = s_dm[q];
-            acc += (T)dA[an.x] * (T)Rc[t * RS + an.y];
-          }
-          T2[t * YS + m] = acc;
         }
         group_sync(g);
         // ACE_GROUP / CH threads per edge (4 or 8)
