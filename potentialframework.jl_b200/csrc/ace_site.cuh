@@ -301,6 +301,68 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   }
 }
 
+// dA[a] = Σ_{terms (k, f1, f2, f3) of density a} w_k·A[f1]·A[f2]·A[f3] with
+// the terms split evenly over the group's threads.  The terms are stored by
+// density and their counts are very uneven (one density of the C3 model owns
+// 265 of 5,691), so a thread per density waits on the longest lists.  Each
+// thread sums its contiguous share density by density; a density split
+// between threads is finished by the thread holding its first term, which
+// adds the later threads' partial sums in thread order (a fixed order, so
+// the result is deterministic).  scratch: 3·ACE_GROUP doubles that are free
+// during this phase.
+template <class T, class Wt>
+__device__ __forceinline__ void adjoint_terms(int D, const int* __restrict__ toff, const ushort4* __restrict__ terms,
+                                              const double* __restrict__ A, double* __restrict__ dA,
+                                              double* __restrict__ scratch, int lt, int g, Wt&& wgt) {
+  const int Tn = toff[D];
+  double* plo = scratch;
+  double* phi = scratch + ACE_GROUP;
+  int* alo = reinterpret_cast<int*>(scratch + 2 * ACE_GROUP);
+  int* ahi = alo + ACE_GROUP;
+  const int q0 = (int)((int64_t)lt * Tn / ACE_GROUP), q1 = (int)((int64_t)(lt + 1) * Tn / ACE_GROUP);
+  for (int a = lt; a < D; a += ACE_GROUP) dA[a] = 0.0;
+  alo[lt] = q0 < q1 ? -1 : -2;  // -2: an empty share (fewer terms than threads), skipped when combining
+  ahi[lt] = -1;
+  group_sync(g);
+  if (q0 < q1) {
+    int lo = 0, hi = D - 1;  // the density of term q0: the last a with toff[a] <= q0
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (toff[mid] <= q0) lo = mid;
+      else hi = mid - 1;
+    }
+    int a = lo, q = q0;
+    while (q < q1) {
+      const int qe = min(toff[a + 1], q1);
+      const bool left = q == q0 && toff[a] < q0;        // continues an earlier thread's share
+      const bool right = qe == q1 && q1 < toff[a + 1];  // continues into a later thread's share
+      T acc = T(0);
+      for (; q < qe; ++q) {
+        const ushort4 tm = terms[q];
+        acc += (T)wgt(tm.x) * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
+      }
+      if (left) {
+        plo[lt] = (double)acc;
+        alo[lt] = a;
+      } else if (right) {
+        phi[lt] = (double)acc;
+        ahi[lt] = a;
+      } else {
+        dA[a] = (double)acc;
+      }
+      ++a;
+    }
+  }
+  group_sync(g);
+  if (ahi[lt] >= 0) {
+    const int a = ahi[lt];
+    double acc = phi[lt];
+    for (int t = lt + 1; t < ACE_GROUP && (alo[t] == a || alo[t] == -2); ++t)
+      if (alo[t] == a) acc += plo[t];
+    dA[a] = acc;
+  }
+}
+
 template <int L, class T, int SUR = 0>
 __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
     k_ace_sites(AceTables p, AceLayout lay, SurParams sp, int nunits, const int* __restrict__ unit_begin,
@@ -410,15 +472,22 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         const ushort4 f = s_prods[k];
         e_acc += __ldg(w + k) * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
       }
-    if (!SUR && want_grad)
-      for (int a = lt; a < D; a += ACE_GROUP) {
-        T acc = T(0);
-        for (int q = s_toff[a]; q < s_toff[a + 1]; ++q) {
-          const ushort4 tm = s_terms[q];
-          acc += (T)__ldg(w + tm.x) * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
+    // the chunk tables (Y … T2) are free between the passes: balanced adjoints when they hold the scratch
+    const bool balanced = lay.CH * (5 * lay.YS + 3 * lay.RS) >= 3 * ACE_GROUP;
+    if (!SUR && want_grad) {
+      if (balanced) {
+        adjoint_terms<T>(D, s_toff, s_terms, A, dA, Yc, lt, g, [&](int k) { return __ldg(w + k); });
+      } else {
+        for (int a = lt; a < D; a += ACE_GROUP) {
+          T acc = T(0);
+          for (int q = s_toff[a]; q < s_toff[a + 1]; ++q) {
+            const ushort4 tm = s_terms[q];
+            acc += (T)__ldg(w + tm.x) * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
+          }
+          dA[a] = acc;
         }
-        dA[a] = acc;
       }
+    }
     if (lay.feat && SUR != 2)  // B = C·P of the centre's species block (fitting.jl:28)
       for (int b = lt; b < p.nB; b += ACE_GROUP) {
         double acc = 0.0;
@@ -453,15 +522,20 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
       if (lt == 0) e_acc += sp.site_e[s];
       group_sync(g);
       wq = wqs;
-      if (want_grad)
-        for (int a = lt; a < D; a += ACE_GROUP) {
-          T acc = T(0);
-          for (int q = s_toff[a]; q < s_toff[a + 1]; ++q) {
-            const ushort4 tm = s_terms[q];
-            acc += (T)wk[tm.x] * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
+      if (want_grad) {
+        if (balanced) {
+          adjoint_terms<T>(D, s_toff, s_terms, A, dA, Yc, lt, g, [&](int k) { return wk[k]; });
+        } else {
+          for (int a = lt; a < D; a += ACE_GROUP) {
+            T acc = T(0);
+            for (int q = s_toff[a]; q < s_toff[a + 1]; ++q) {
+              const ushort4 tm = s_terms[q];
+              acc += (T)wk[tm.x] * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
+            }
+            dA[a] = acc;
           }
-          dA[a] = acc;
         }
+      }
     }
     // ---- pass 2: pullback ----
     if (want_grad) {

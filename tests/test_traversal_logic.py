@@ -178,3 +178,68 @@ def test_half_pass_mask_walk_takes_every_entry_once():
                 row.append(int(sum(1 << b for b in range(32) if bits[b])))
             mh.append(row)
         mask_walk(mh, n)
+
+
+def balanced_adjoint(toff, G=64):
+    """The ACE site kernel's balanced adjoint sums (csrc/ace_site.cuh,
+    adjoint_terms), restated: thread lt sums terms [lt·T/G, (lt+1)·T/G) density
+    by density; a density split between threads is finished by the thread
+    holding its first term from the later threads' partials.  Returns, per
+    density, the list of term indices in the order they were added."""
+    toff = list(toff)
+    D, T = len(toff) - 1, toff[-1]
+    dA = [[] for _ in range(D)]
+    plo, phi, alo, ahi = [None] * G, [None] * G, [-1] * G, [-1] * G
+    for lt in range(G):
+        q0, q1 = lt * T // G, (lt + 1) * T // G
+        if q0 >= q1:
+            alo[lt] = -2  # an empty share
+            continue
+        lo, hi = 0, D - 1
+        while lo < hi:
+            mid = (lo + hi + 1) >> 1
+            if toff[mid] <= q0:
+                lo = mid
+            else:
+                hi = mid - 1
+        a, q = lo, q0
+        while q < q1:
+            assert a < D
+            qe = min(toff[a + 1], q1)
+            left = q == q0 and toff[a] < q0
+            right = qe == q1 and q1 < toff[a + 1]
+            acc = list(range(q, qe))
+            q = qe
+            if left:
+                plo[lt], alo[lt] = acc, a
+            elif right:
+                phi[lt], ahi[lt] = acc, a
+            else:
+                dA[a] = acc
+            a += 1
+    for lt in range(G):
+        if ahi[lt] >= 0:
+            a, acc = ahi[lt], list(phi[lt])
+            t = lt + 1
+            while t < G and alo[t] in (a, -2):
+                if alo[t] == a:
+                    acc += plo[t]
+                t += 1
+            dA[a] = acc
+    return dA
+
+
+def test_balanced_adjoint_sums_every_term_once_in_order():
+    rng = np.random.default_rng(3)
+    cases = [[0, 0], [0, 5], [0, 0, 300, 300, 301], [0, 265] + [265 + 3 * k for k in range(1, 60)]]
+    for _ in range(200):
+        D = int(rng.integers(1, 220))
+        counts = rng.integers(0, 30, D) * (rng.random(D) > 0.2)
+        if rng.random() < 0.3:
+            counts[rng.integers(0, D)] += int(rng.integers(100, 400))
+        cases.append(np.concatenate([[0], np.cumsum(counts)]).tolist())
+    for toff in cases:
+        for G in (64, 128):
+            dA = balanced_adjoint(toff, G)
+            for a in range(len(toff) - 1):
+                assert dA[a] == list(range(toff[a], toff[a + 1])), (a, toff[:5])
