@@ -301,66 +301,78 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   }
 }
 
-// dA[a] = Σ_{terms (k, f1, f2, f3) of density a} w_k·A[f1]·A[f2]·A[f3] with
-// the terms split evenly over the group's threads.  The terms are stored by
-// density and their counts are very uneven (one density of the C3 model owns
-// 265 of 5,691), so a thread per density waits on the longest lists.  Each
-// thread sums its contiguous share density by density; a density split
-// between threads is finished by the thread holding its first term, which
-// adds the later threads' partial sums in thread order (a fixed order, so
-// the result is deterministic).  scratch: 3·ACE_GROUP doubles that are free
-// during this phase.
-template <class T, class Wt>
-__device__ __forceinline__ void adjoint_terms(int D, const int* __restrict__ toff, const ushort4* __restrict__ terms,
-                                              const double* __restrict__ A, double* __restrict__ dA,
-                                              double* __restrict__ scratch, int lt, int g, Wt&& wgt) {
-  const int Tn = toff[D];
+// Row sums of a CSR list (rows: off[r] .. off[r+1]) with the entries split
+// evenly over the group's threads.  The ACE lists are stored by row and their
+// lengths are very uneven (one density of the C3 model owns 265 of its 5,691
+// adjoint terms), so a thread per row waits on the longest rows.  Each thread
+// sums its contiguous share row by row (val(q) gives entry q; the sum is
+// accumulated in Acc); a row split between threads is finished by the thread
+// holding its first entry, which adds the later threads' partial sums in
+// thread order — a fixed order, so the result is deterministic.  put(r, sum)
+// receives every row that has entries, once.  scratch: 3·ACE_GROUP doubles
+// that are free during the call; every thread of the group must call.
+template <class Acc, class Val, class Put>
+__device__ __forceinline__ void balanced_rows(int nrows, const int* __restrict__ off, double* __restrict__ scratch,
+                                              int lt, int g, Val&& val, Put&& put) {
+  const int Tn = off[nrows];
   double* plo = scratch;
   double* phi = scratch + ACE_GROUP;
   int* alo = reinterpret_cast<int*>(scratch + 2 * ACE_GROUP);
   int* ahi = alo + ACE_GROUP;
   const int q0 = (int)((int64_t)lt * Tn / ACE_GROUP), q1 = (int)((int64_t)(lt + 1) * Tn / ACE_GROUP);
-  for (int a = lt; a < D; a += ACE_GROUP) dA[a] = 0.0;
-  alo[lt] = q0 < q1 ? -1 : -2;  // -2: an empty share (fewer terms than threads), skipped when combining
+  alo[lt] = q0 < q1 ? -1 : -2;  // -2: an empty share (fewer entries than threads), skipped when combining
   ahi[lt] = -1;
   group_sync(g);
   if (q0 < q1) {
-    int lo = 0, hi = D - 1;  // the density of term q0: the last a with toff[a] <= q0
+    int lo = 0, hi = nrows - 1;  // the row of entry q0: the last r with off[r] <= q0
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (toff[mid] <= q0) lo = mid;
+      if (off[mid] <= q0) lo = mid;
       else hi = mid - 1;
     }
-    int a = lo, q = q0;
+    int r = lo, q = q0;
     while (q < q1) {
-      const int qe = min(toff[a + 1], q1);
-      const bool left = q == q0 && toff[a] < q0;        // continues an earlier thread's share
-      const bool right = qe == q1 && q1 < toff[a + 1];  // continues into a later thread's share
-      T acc = T(0);
-      for (; q < qe; ++q) {
-        const ushort4 tm = terms[q];
-        acc += (T)wgt(tm.x) * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
-      }
+      const int qe = min(off[r + 1], q1);
+      const bool left = q == q0 && off[r] < q0;        // continues an earlier thread's share
+      const bool right = qe == q1 && q1 < off[r + 1];  // continues into a later thread's share
+      Acc acc = Acc(0);
+      for (; q < qe; ++q) acc += val(q);
       if (left) {
         plo[lt] = (double)acc;
-        alo[lt] = a;
+        alo[lt] = r;
       } else if (right) {
         phi[lt] = (double)acc;
-        ahi[lt] = a;
-      } else {
-        dA[a] = (double)acc;
+        ahi[lt] = r;
+      } else if (off[r + 1] > off[r]) {
+        put(r, (double)acc);
       }
-      ++a;
+      ++r;
     }
   }
   group_sync(g);
   if (ahi[lt] >= 0) {
-    const int a = ahi[lt];
+    const int r = ahi[lt];
     double acc = phi[lt];
-    for (int t = lt + 1; t < ACE_GROUP && (alo[t] == a || alo[t] == -2); ++t)
-      if (alo[t] == a) acc += plo[t];
-    dA[a] = acc;
+    for (int t = lt + 1; t < ACE_GROUP && (alo[t] == r || alo[t] == -2); ++t)
+      if (alo[t] == r) acc += plo[t];
+    put(r, acc);
   }
+}
+
+// dA[a] = Σ_{terms (k, f1, f2, f3) of density a} w_k·A[f1]·A[f2]·A[f3], the
+// terms balanced over the group's threads (densities without terms stay 0).
+template <class T, class Wt>
+__device__ __forceinline__ void adjoint_terms(int D, const int* __restrict__ toff, const ushort4* __restrict__ terms,
+                                              const double* __restrict__ A, double* __restrict__ dA,
+                                              double* __restrict__ scratch, int lt, int g, Wt&& wgt) {
+  for (int a = lt; a < D; a += ACE_GROUP) dA[a] = 0.0;
+  balanced_rows<T>(
+      D, toff, scratch, lt, g,
+      [&](int q) {
+        const ushort4 tm = terms[q];
+        return (T)wgt(tm.x) * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
+      },
+      [&](int a, double v) { dA[a] = v; });
 }
 
 template <int L, class T, int SUR = 0>
@@ -488,15 +500,27 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
         }
       }
     }
-    if (lay.feat && SUR != 2)  // B = C·P of the centre's species block (fitting.jl:28)
-      for (int b = lt; b < p.nB; b += ACE_GROUP) {
-        double acc = 0.0;
-        for (int q = p.crow_off[b]; q < p.crow_off[b + 1]; ++q) {
-          const ushort4 f = s_prods[p.crow_k[q]];
-          acc += p.crow_val[q] * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
+    if (lay.feat && SUR != 2) {  // B = C·P of the centre's species block (fitting.jl:28)
+      if (balanced) {
+        group_sync(g);  // the adjoint's scratch is read by its combining threads until here
+        balanced_rows<double>(
+            p.nB, p.crow_off, Yc, lt, g,
+            [&](int q) {
+              const ushort4 f = s_prods[p.crow_k[q]];
+              return p.crow_val[q] * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
+            },
+            [&](int b, double v) { Facc[iz * p.nB + b] += v; });
+      } else {
+        for (int b = lt; b < p.nB; b += ACE_GROUP) {
+          double acc = 0.0;
+          for (int q = p.crow_off[b]; q < p.crow_off[b + 1]; ++q) {
+            const ushort4 f = s_prods[p.crow_k[q]];
+            acc += p.crow_val[q] * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
+          }
+          Facc[iz * p.nB + b] += acc;
         }
-        Facc[iz * p.nB + b] += acc;
       }
+    }
     const double* wq = nullptr;
     if constexpr (SUR == 1) {
       // ---- surrogate feature pass: keep A and the own-species features ----
