@@ -243,8 +243,9 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
     er.de = __shfl_sync(seg, er.de, src);
     er.du = __shfl_sync(seg, er.du, src);
   }
-  double* Rt = gbase + lay.R + t * lay.RS;
-  double* dRt = gbase + lay.dR + t * lay.RS;
+  // the chunk tables hold T: FP64 for the plain path, FP32 for the mixed form
+  T* Rt = reinterpret_cast<T*>(gbase + lay.R) + t * lay.RS;
+  T* dRt = reinterpret_cast<T*>(gbase + lay.dR) + t * lay.RS;
   edge_channels<T, Grad, 1>(p.R, pidx, er, q, tpe, [&](int n, T v, T dv) {
     Rt[n] = v;
     if constexpr (Grad) dRt[n] = dv;
@@ -282,8 +283,8 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
     es.dq[t] = T(0);
   }
   // harmonics last: the radial set-ups are dead by now
-  double* Yt = gbase + lay.Y + t * lay.YS;
-  double* dYt = gbase + lay.dY + t * lay.YS * 3;
+  T* Yt = reinterpret_cast<T*>(gbase + lay.Y) + t * lay.YS;
+  T* dYt = reinterpret_cast<T*>(gbase + lay.dY) + t * lay.YS * 3;
 #pragma unroll
   for (int m = 0; m <= L; ++m) {
     if ((m & (tpe - 1)) != q) continue;
@@ -363,16 +364,16 @@ __device__ __forceinline__ void balanced_rows(int nrows, const int* __restrict__
 // terms balanced over the group's threads (densities without terms stay 0).
 template <class T, class Wt>
 __device__ __forceinline__ void adjoint_terms(int D, const int* __restrict__ toff, const ushort4* __restrict__ terms,
-                                              const double* __restrict__ A, double* __restrict__ dA,
+                                              const T* __restrict__ A, T* __restrict__ dA,
                                               double* __restrict__ scratch, int lt, int g, Wt&& wgt) {
-  for (int a = lt; a < D; a += ACE_GROUP) dA[a] = 0.0;
+  for (int a = lt; a < D; a += ACE_GROUP) dA[a] = T(0);
   balanced_rows<T>(
       D, toff, scratch, lt, g,
       [&](int q) {
         const ushort4 tm = terms[q];
         return (T)wgt(tm.x) * ((T)A[tm.y] * (T)A[tm.z] * (T)A[tm.w]);
       },
-      [&](int a, double v) { dA[a] = v; });
+      [&](int a, double v) { dA[a] = (T)v; });
 }
 
 template <int L, class T, int SUR = 0>
@@ -414,14 +415,16 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
   const int g = threadIdx.x / ACE_GROUP, lt = threadIdx.x % ACE_GROUP;
   if (g >= lay.G) return;
   double* gb = reinterpret_cast<double*>(smem + lay.tables_end + lay.group_bytes * g);
-  double* A = gb + lay.A;
-  double* dA = gb + lay.dA;
-  double* Yc = gb + lay.Y;
-  double* dYc = gb + lay.dY;
-  double* Rc = gb + lay.R;
-  double* dRc = gb + lay.dR;
-  double* T1 = gb + lay.T1;
-  double* T2 = gb + lay.T2;
+  // per-group tables in T (double-sized slots: the FP32 form uses the first half)
+  T* A = reinterpret_cast<T*>(gb + lay.A);
+  T* dA = reinterpret_cast<T*>(gb + lay.dA);
+  T* Yc = reinterpret_cast<T*>(gb + lay.Y);
+  T* dYc = reinterpret_cast<T*>(gb + lay.dY);
+  T* Rc = reinterpret_cast<T*>(gb + lay.R);
+  T* dRc = reinterpret_cast<T*>(gb + lay.dR);
+  T* T1 = reinterpret_cast<T*>(gb + lay.T1);
+  T* T2 = reinterpret_cast<T*>(gb + lay.T2);
+  double* const chunk_scratch = gb + lay.Y;  // free between the passes
   EdgeScalars<T> es;
   const int CH = lay.CH;
   double* e0p = gb + lay.esc;
@@ -454,9 +457,9 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
     }
     group_sync(g);
     if (SUR == 2)  // the feature pass's A-basis
-      for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? 1.0 : sp.site_A[(size_t)s * D + a];
+      for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? T(1) : (T)sp.site_A[(size_t)s * D + a];
     else
-      for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? 1.0 : 0.0;
+      for (int a = lt; a <= D; a += ACE_GROUP) A[a] = (a == D) ? T(1) : T(0);
     // ---- pass 1: A-basis ----
     for (int c0 = 0; c0 < (SUR == 2 ? 0 : E); c0 += CH) {
       const int nc = min(CH, E - c0);
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
     const bool balanced = lay.CH * (5 * lay.YS + 3 * lay.RS) >= 3 * ACE_GROUP;
     if (!SUR && want_grad) {
       if (balanced) {
-        adjoint_terms<T>(D, s_toff, s_terms, A, dA, Yc, lt, g, [&](int k) { return __ldg(w + k); });
+        adjoint_terms<T>(D, s_toff, s_terms, A, dA, chunk_scratch, lt, g, [&](int k) { return __ldg(w + k); });
       } else {
         for (int a = lt; a < D; a += ACE_GROUP) {
           T acc = T(0);
@@ -504,7 +507,7 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
       if (balanced) {
         group_sync(g);  // the adjoint's scratch is read by its combining threads until here
         balanced_rows<double>(
-            p.nB, p.crow_off, Yc, lt, g,
+            p.nB, p.crow_off, chunk_scratch, lt, g,
             [&](int q) {
               const ushort4 f = s_prods[p.crow_k[q]];
               return p.crow_val[q] * (double)((T)A[f.x] * (T)A[f.y] * (T)A[f.z] * (T)A[f.w]);
@@ -526,7 +529,7 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
       // ---- surrogate feature pass: keep A and the own-species features ----
       group_sync(g);
       const int nB = p.nB, nQ = p.nQ, nin = nB + nQ;
-      for (int a = lt; a < D; a += ACE_GROUP) sp.site_A[(size_t)s * D + a] = A[a];
+      for (int a = lt; a < D; a += ACE_GROUP) sp.site_A[(size_t)s * D + a] = (double)A[a];
       for (int i = lt; i < nin; i += ACE_GROUP)
         sp.site_feat[(size_t)s * nin + i] = i < nB ? Facc[iz * nB + i] : Facc[p.nz * nB + iz * nQ + (i - nB)];
     }
@@ -548,7 +551,7 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
       wq = wqs;
       if (want_grad) {
         if (balanced) {
-          adjoint_terms<T>(D, s_toff, s_terms, A, dA, Yc, lt, g, [&](int k) { return wk[k]; });
+          adjoint_terms<T>(D, s_toff, s_terms, A, dA, chunk_scratch, lt, g, [&](int k) { return wk[k]; });
         } else {
           for (int a = lt; a < D; a += ACE_GROUP) {
             T acc = T(0);
