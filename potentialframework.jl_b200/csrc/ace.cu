@@ -54,6 +54,7 @@ struct AceDevice {
   RadialDev R{}, Q{};
   DevBuf r_len, r_nodes, r_coeff, r_tr, r_pow, r_envk, r_env;
   DevBuf q_len, q_nodes, q_coeff, q_tr, q_pow, q_envk, q_env;
+  DevBuf r_coeff32, q_coeff32, weights32;  // FP32 copies for the mixed form
   DevBuf density, dn_off, dn, dm_off, dm, prods, term_off, terms, weights, wpair, ref, pair_ok, Fnorm;
   DevBuf crow_off, crow_k, crow_val;
   // per evaluation
@@ -297,7 +298,7 @@ static T* upload(DevBuf& b, const T* src, size_t count, cudaStream_t st) {
 }
 
 static RadialDev upload_family(const pfw_radial_family& f, int nz, DevBuf& len, DevBuf& nodes, DevBuf& coeff,
-                               DevBuf& tr, DevBuf& pw, DevBuf& ek, DevBuf& ev, cudaStream_t st) {
+                               DevBuf& coeff32, DevBuf& tr, DevBuf& pw, DevBuf& ek, DevBuf& ev, cudaStream_t st) {
   if (f.nchannels < 0 || f.nknots < 2) throw Error(PFW_EINVAL, "invalid radial family shape");
   const int np = nz * nz;
   for (int k = 0; k < np; ++k) {
@@ -317,7 +318,14 @@ static RadialDev upload_family(const pfw_radial_family& f, int nz, DevBuf& len, 
   d.nz = nz;
   d.lengths = upload(len, f.lengths, np, st);
   d.nodes = upload(nodes, f.nodes, (size_t)np * f.nknots, st);
-  d.coeff = upload(coeff, f.coeff, (size_t)np * (f.nknots - 1) * f.nchannels * 4, st);
+  const size_t ncoeff = (size_t)np * (f.nknots - 1) * f.nchannels * 4;
+  d.coeff = upload(coeff, f.coeff, ncoeff, st);
+  {
+    std::vector<float> c32(std::max<size_t>(ncoeff, 1));
+    for (size_t i = 0; i < ncoeff; ++i) c32[i] = (float)f.coeff[i];
+    d.coeff32 = upload(coeff32, c32.data(), c32.size(), st);
+    PFW_CUDA(cudaStreamSynchronize(st));  // the staging vector goes out of scope
+  }
   d.transform = upload(tr, f.transform, (size_t)np * 6, st);
   d.powers = upload(pw, f.powers, (size_t)np * 2, st);
   d.env_kind = upload(ek, f.envelope_kind, np, st);
@@ -339,7 +347,7 @@ static void free_device(AceDevice* a) {
   DevBuf* bufs[] = {&a->r_len, &a->r_nodes, &a->r_coeff, &a->r_tr, &a->r_pow, &a->r_envk, &a->r_env,
                     &a->q_len, &a->q_nodes, &a->q_coeff, &a->q_tr, &a->q_pow, &a->q_envk, &a->q_env,
                     &a->density, &a->dn_off, &a->dn, &a->dm_off, &a->dm, &a->prods, &a->term_off, &a->terms,
-                    &a->weights, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm, &a->crow_off, &a->crow_k, &a->crow_val,
+                    &a->weights, &a->weights32, &a->r_coeff32, &a->q_coeff32, &a->wpair, &a->ref, &a->pair_ok, &a->Fnorm, &a->crow_off, &a->crow_k, &a->crow_val,
                     &a->edge_count, &a->edge_countp, &a->edge_off, &a->edge_j, &a->edge_d, &a->edge_S, &a->edge_rev, &a->edge_g,
                     &a->site_out, &a->site_E_orig, &a->status, &a->unit_begin, &a->unit_out,
                     &a->batch_units, &a->batch_sys_units, &a->batch_out, &a->batch_feat, &a->design_G,
@@ -394,9 +402,11 @@ static void fill_model(pfw_ws* ws, AceDevice* a, const pfw_ace_tables* t) {
   a->P = t->nproducts;
   a->nB = t->nbasis;
   a->cutoff = t->cutoff;
-  a->R = upload_family(t->radial, nz, a->r_len, a->r_nodes, a->r_coeff, a->r_tr, a->r_pow, a->r_envk, a->r_env, st);
+  a->R = upload_family(t->radial, nz, a->r_len, a->r_nodes, a->r_coeff, a->r_coeff32, a->r_tr, a->r_pow, a->r_envk,
+                       a->r_env, st);
   if (a->nQ > 0)
-    a->Q = upload_family(t->pair, nz, a->q_len, a->q_nodes, a->q_coeff, a->q_tr, a->q_pow, a->q_envk, a->q_env, st);
+    a->Q = upload_family(t->pair, nz, a->q_len, a->q_nodes, a->q_coeff, a->q_coeff32, a->q_tr, a->q_pow, a->q_envk,
+                         a->q_env, st);
   else
     a->Q = a->R;
   // density tables, grouped by radial channel and by harmonic
@@ -485,6 +495,8 @@ static void fill_model(pfw_ws* ws, AceDevice* a, const pfw_ace_tables* t) {
     }
   }
   upload(a->weights, wts.data(), wts.size(), st);
+  const std::vector<float> w32(wts.begin(), wts.end());  // alive until the synchronisation below
+  upload(a->weights32, w32.data(), w32.size(), st);
   upload(a->crow_off, roff.data(), roff.size(), st);
   upload(a->crow_k, rk.data(), rk.size(), st);
   upload(a->crow_val, rv.data(), rv.size(), st);
@@ -526,6 +538,7 @@ static AceTables tables_of(AceDevice* a) {
   p.dm_off = a->dm_off.as<int>();
   p.dm = a->dm.as<int2>();
   p.weights = a->weights.as<double>();
+  p.weights32 = a->weights32.as<float>();
   p.crow_off = a->crow_off.as<int>();
   p.crow_k = a->crow_k.as<int>();
   p.crow_val = a->crow_val.as<double>();

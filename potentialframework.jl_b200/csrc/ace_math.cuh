@@ -9,6 +9,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 namespace pfw {
 
 // One radial family on the device (layout of pfw_radial_family).
@@ -17,6 +19,7 @@ struct RadialDev {
   const int* lengths;          // [nz*nz]
   const double* nodes;         // [nz*nz][nknots]
   const double* coeff;         // [nz*nz][nknots-1][nch][4]
+  const float* coeff32;        // the same in FP32 for the mixed form (null: read coeff)
   const double* transform;     // [nz*nz][6]
   const int* powers;           // [nz*nz][2]
   const int* env_kind;         // [nz*nz]

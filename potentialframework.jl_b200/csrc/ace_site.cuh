@@ -44,6 +44,7 @@ struct AceTables {
   const int* dm_off;              // [nY+1]
   const int2* dm;                 // [D] (a, n)
   const double* weights;          // [nz][P]
+  const float* weights32;         // the same in FP32 (mixed-form adjoints)
   int nB;                         // invariants (fitting features)
   const int* crow_off;            // [nB+1] coupling rows (CSR)
   const int* crow_k;              // product of each stored entry
@@ -164,23 +165,30 @@ struct EdgeScalars {
 template <class T, bool Grad, int NB, class On>
 __device__ __forceinline__ void edge_channels(const RadialDev& f, int pidx, const EdgeRadial<T>& er, int q, int tpe,
                                               On&& on) {
-  const double* cb = channel_coeff(f, pidx, er.k0, 0);
+  constexpr bool F32 = std::is_same<T, float>::value;
+  const bool use32 = F32 && f.coeff32 != nullptr;  // the mixed form reads FP32 coefficients (one 16-B load)
+  const size_t base = (((size_t)pidx * (f.nknots - 1) + er.k0) * f.nch) * 4;
   for (int n0 = q; n0 < f.nch; n0 += NB * tpe) {
-    double2 lo[NB], hi[NB];
+    T c[NB][4];
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       const int n = n0 + j * tpe;
       if (n < f.nch) {
-        const double2* cp = reinterpret_cast<const double2*>(cb + 4 * n);
-        lo[j] = __ldg(cp);
-        hi[j] = __ldg(cp + 1);
+        if (use32) {
+          const float4 cf = __ldg(reinterpret_cast<const float4*>(f.coeff32 + base + 4 * (size_t)n));
+          c[j][0] = (T)cf.x; c[j][1] = (T)cf.y; c[j][2] = (T)cf.z; c[j][3] = (T)cf.w;
+        } else {
+          const double2* cp = reinterpret_cast<const double2*>(f.coeff + base + 4 * (size_t)n);
+          const double2 lo = __ldg(cp), hi = __ldg(cp + 1);
+          c[j][0] = (T)lo.x; c[j][1] = (T)lo.y; c[j][2] = (T)hi.x; c[j][3] = (T)hi.y;
+        }
       }
     }
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       const int n = n0 + j * tpe;
       if (n >= f.nch) break;
-      const T c0 = (T)lo[j].x, c1 = (T)lo[j].y, c2 = (T)hi[j].x, c3 = (T)hi[j].y, u = er.u;
+      const T c0 = c[j][0], c1 = c[j][1], c2 = c[j][2], c3 = c[j][3], u = er.u;
       const T v = ((c3 * u + c2) * u + c1) * u + c0;
       if constexpr (Grad) {
         const T dv = (T(3) * c3 * (u * u) + T(2) * c2 * u + c1);
@@ -491,7 +499,12 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
     const bool balanced = lay.CH * (5 * lay.YS + 3 * lay.RS) >= 3 * ACE_GROUP;
     if (!SUR && want_grad) {
       if (balanced) {
-        adjoint_terms<T>(D, s_toff, s_terms, A, dA, chunk_scratch, lt, g, [&](int k) { return __ldg(w + k); });
+        if constexpr (std::is_same<T, float>::value) {
+          const float* w32 = p.weights32 + (size_t)iz * P;
+          adjoint_terms<T>(D, s_toff, s_terms, A, dA, chunk_scratch, lt, g, [&](int k) { return __ldg(w32 + k); });
+        } else {
+          adjoint_terms<T>(D, s_toff, s_terms, A, dA, chunk_scratch, lt, g, [&](int k) { return __ldg(w + k); });
+        }
       } else {
         for (int a = lt; a < D; a += ACE_GROUP) {
           T acc = T(0);
