@@ -991,6 +991,28 @@ def surrogate_form(dev, stream, flush, steps=5):
         if tau is not None:
             res[label]["fallback"] = h.surrogate_stats()
     h.close()
+    # the mixed workspace: the surrogate's site passes in FP32 (energy-rule gate)
+    h = lib.Handle(lib.MIXED, device=dev.index)
+    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+    h.ace(model)
+    h.check(h.L.pfw_ace_set_schedule(h.ws, chunk, groups))
+    h.surrogate(feat, sur, tau=tau_energy_rule)
+    for k in range(steps + 2):
+        if k == 2:
+            torch.cuda.synchronize()
+            ms = []
+        if k >= 2:
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        h.set_geometry_device(n, ctypes.c_void_p(Xd.data_ptr()), sysb.H, sysb.pbc, ctypes.c_void_p(Sd.data_ptr()))
+        h.evaluate_device(lib.MODEL_SURROGATE, 7, *ptrs)
+        if k >= 2:
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+    res["surrogate_mixed"] = dict(ms=float(np.mean(ms)), F=Fd.cpu().numpy().copy(), fallback=h.surrogate_stats())
+    h.close()
     dF = res["surrogate"]["F"] - res["ace"]["F"]
     dF0 = F_energy_only - res["ace"]["F"]
     dFg = res["surrogate_energy_gate"]["F"] - res["ace"]["F"]
@@ -1011,6 +1033,12 @@ def surrogate_form(dev, stream, flush, steps=5):
                 energy_gate=dict(tau_eV=tau_energy_rule, ms_per_step=ms_g, speedup_vs_plain_ace=ms_a / ms_g,
                                  force_rmse_vs_ace=float(np.sqrt(np.mean(dFg ** 2))),
                                  fallback_fraction=fbg / max(ns, 1)),
+                energy_gate_mixed=dict(ms_per_step=res["surrogate_mixed"]["ms"],
+                                       speedup_vs_plain_ace=ms_a / res["surrogate_mixed"]["ms"],
+                                       force_rmse_vs_ace=float(np.sqrt(np.mean(
+                                           (res["surrogate_mixed"]["F"] - res["ace"]["F"]) ** 2))),
+                                       fallback_fraction=res["surrogate_mixed"]["fallback"][0] / max(ns, 1),
+                                       note="mixed workspace: the two surrogate site passes in FP32"),
                 training=dict(environments=int(len(E)), epochs=40, members=S.MEMBERS, features=S.NIN,
                               hidden=S.HIDDEN, final_loss=sur.history[-1], label_s=t1 - t0, train_s=t2 - t1,
                               force_epochs=len(force_hist), force_train_s=t3 - t2,

@@ -1293,7 +1293,9 @@ static void sur_feature_pass(pfw_ws* ws, SurDevice* d, const SiteLaunch& s) {
   AceDevice* a = d->fm;
   const AceTables p = tables_of(a);
   if (s.nunits > 0) {
-    dispatch_sites<double, 1>(a->lmax, p, choose_sur_layout(p, ws->opt.device, 1), s, ws->stream, ws->opt.device);
+    const AceLayout lay = choose_sur_layout(p, ws->opt.device, 1);
+    if (ws->opt.precision == PFW_PRECISION_MIXED) dispatch_sites<float, 1>(a->lmax, p, lay, s, ws->stream, ws->opt.device);
+    else dispatch_sites<double, 1>(a->lmax, p, lay, s, ws->stream, ws->opt.device);
     ws->launches += 1;
   }
 }
@@ -1345,7 +1347,7 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   if (full->cutoff != d->fm->cutoff || full->nz != d->nz)
     throw Error(PFW_EINVAL, "surrogate feature model and ACE model differ in cutoff or species");
   check_species(ws, d->nz, "feature model has no element channel for a species");
-  if (ws->opt.precision != PFW_PRECISION_FP64) throw Error(PFW_EINVAL, "the surrogate path runs in the FP64 workspace");
+  // a mixed workspace runs the two site passes (and any fallback sites) in FP32
   AceDevice* a = d->fm;
   cudaStream_t st = ws->stream;
   ws->stage_begin(3);
@@ -1374,7 +1376,9 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
   // 3. pullback with the per-site weights
   s.want_grad = want_grad;
   if (n > 0) {
-    dispatch_sites<double, 2>(a->lmax, p, choose_sur_layout(p, ws->opt.device, 2), s, st, ws->opt.device);
+    const AceLayout lay = choose_sur_layout(p, ws->opt.device, 2);
+    if (ws->opt.precision == PFW_PRECISION_MIXED) dispatch_sites<float, 2>(a->lmax, p, lay, s, st, ws->opt.device);
+    else dispatch_sites<double, 2>(a->lmax, p, lay, s, st, ws->opt.device);
     ws->launches += 1;
   }
   // fallback: the flagged sites with the full model on the same environments
@@ -1398,7 +1402,8 @@ void sur_evaluate(pfw_ws* ws, uint32_t req, double* E_dev, double* F_dev, double
     f.unit_begin = nullptr;
     f.unit_sites = list;
     f.unit_out = fb_out;
-    dispatch_sites<double, 0>(full->lmax, pf, lf, f, st, ws->opt.device);
+    if (ws->opt.precision == PFW_PRECISION_MIXED) dispatch_sites<float, 0>(full->lmax, pf, lf, f, st, ws->opt.device);
+    else dispatch_sites<double, 0>(full->lmax, pf, lf, f, st, ws->opt.device);
     k_scatter_sites<<<grid_for((int64_t)count * 10, 256), 256, 0, st>>>(count, list, fb_out, a->unit_out.as<double>());
     ws->launches += 3;
   }

@@ -176,3 +176,23 @@ def test_surrogate_faster_than_ace(models, trained):
         return min(ts)
 
     assert best(lib.MODEL_ACE) > 1.5 * best(lib.MODEL_SURROGATE)
+
+
+def test_mixed_surrogate_matches_fp64_surrogate(models, trained):
+    """A mixed workspace runs the surrogate's two site passes in FP32: the
+    same surrogate energies and forces as the FP64 workspace to FP32
+    accuracy (far below the surrogate's own error against ACE)."""
+    m, feat, _ = models
+    sur, _ = trained
+    s = WL.b2(seed=45, nc=4, sigma=0.1)
+    out = {}
+    for prec in (lib.FP64, lib.MIXED):
+        h = lib.Handle(prec)
+        h.ace(m)
+        h.surrogate(feat, ungated(sur))
+        h.set_geometry(s.X, s.H, s.pbc, s.species)
+        out[prec] = h.evaluate(lib.MODEL_SURROGATE, 7)
+    (E64, F64, W64), (E32, F32, W32) = out[lib.FP64], out[lib.MIXED]
+    assert abs(E32 - E64) <= 1e-5 * max(1.0, abs(E64))
+    assert float(np.sqrt(np.mean((F32 - F64) ** 2))) <= 1e-4
+    assert float(np.abs(W32 - W64).max()) <= 1e-4 * max(1.0, float(np.abs(W64).max()))
