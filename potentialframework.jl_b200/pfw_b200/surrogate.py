@@ -494,7 +494,7 @@ def calibrate_gate(h, sur: "Surrogate", full: PackedACE, feat: PackedACE, system
     """Choose the ensemble-disagreement threshold tau from forces.
 
     On the calibration systems (held out from training), plain FP64 ACE
-    forces are the judge.  tau runs down the quantiles of the sites' ensemble
+    forces are the reference.  tau runs down the quantiles of the sites' ensemble
     standard deviation (numpy restatement of the deployed BF16 ensemble on
     the library's features; quantile 1 means no disagreement gate); for each,
     the surrogate is evaluated with its feature-range gate and that tau, and

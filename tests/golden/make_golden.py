@@ -67,7 +67,7 @@ def main(ref):
 
 def reference_dir(arg=None):
     """The reference checkout: the command-line argument, else $PFW_REFERENCE_DIR,
-    else the mount point this build's container uses."""
+    else the read-only checkout at /root/reference."""
     return arg or os.environ.get("PFW_REFERENCE_DIR") or "/root/reference"
 
 
