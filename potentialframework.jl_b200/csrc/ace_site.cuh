@@ -222,13 +222,26 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
   const T r = r0 > T(0) ? r0 : T(1);
   const bool pair = p.nQ > 0 && p.pair_ok[zj];  // the same for all of the edge's threads
   EdgeRadial<T> er{}, eq{};
+  // thread 0 of the edge sets up the R family, thread 1 the pair family: one
+  // call with the family chosen per thread, so the two run side by side
+  // rather than as two branches of the warp
+  if (q == 0 || (q == 1 && pair)) {
+    RadialDev fam = p.R;
+    const double* famp = radp;
+    if (q == 1) {
+      fam = p.Q;
+      famp = radp ? radp + RADP_W * p.nz * p.nz : nullptr;
+    }
+    const EdgeRadial<T> ex = edge_radial<T>(fam, pidx, r, famp);
+    if (q == 0) er = ex;
+    else eq = ex;
+  }
   if (q == 0) {
     if (!(r0 > T(0))) atomicOr(status, 2);
     es.r[t] = r;
     es.dx[t] = dx;
     es.dy[t] = dy;
     es.dz[t] = dz;
-    er = edge_radial<T>(p.R, pidx, r, radp);
     es.k0[t] = er.k0;
     es.pidx[t] = pidx;
     es.u[t] = er.u;
@@ -236,7 +249,6 @@ __device__ __forceinline__ void ace_chunk_edges(const AceTables& p, double* gbas
     es.de[t] = er.de;
     es.du[t] = er.du;
   } else if (q == 1 && pair) {
-    eq = edge_radial<T>(p.Q, pidx, r, radp ? radp + RADP_W * p.nz * p.nz : nullptr);
     if (!eq.ok) atomicOr(status, 2);
   }
   // the radial set-ups from the edge's first two threads (the tpe threads of
