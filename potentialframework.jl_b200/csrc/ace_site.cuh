@@ -609,30 +609,27 @@ __global__ void __launch_bounds__(ACE_MAX_GROUPS * ACE_GROUP)
             T acc[EB];
 #pragma unroll
             for (int u = 0; u < EB; ++u) acc[u] = T(0);
-            if (col < nR) {
-              for (int q = s_dnoff[col]; q < s_dnoff[col + 1]; ++q) {
-                const int2 am = s_dn[q];
-                const T w = (T)dA[am.x];
-#pragma unroll
-                for (int u = 0; u < EB; ++u)
-                  if (u < tn) acc[u] += w * (T)Yc[(t0 + u) * YS + am.y];
-              }
-#pragma unroll
-              for (int u = 0; u < EB; ++u)
-                if (u < tn) T1[(t0 + u) * RS + col] = acc[u];
-            } else {
-              const int m = col - nR;
-              for (int q = s_dmoff[m]; q < s_dmoff[m + 1]; ++q) {
-                const int2 an = s_dm[q];
-                const T w = (T)dA[an.x];
-#pragma unroll
-                for (int u = 0; u < EB; ++u)
-                  if (u < tn) acc[u] += w * (T)Rc[(t0 + u) * RS + an.y];
-              }
+            // T1 and T2 columns through one code path (the column's list, source
+            // table and output chosen per thread), so a warp holding both kinds
+            // does not run them as two branches
+            const bool isT1 = col < nR;
+            const int c = isT1 ? col : col - nR;
+            const int* off = isT1 ? s_dnoff : s_dmoff;
+            const int2* lst = isT1 ? s_dn : s_dm;
+            const T* src = isT1 ? Yc : Rc;
+            const int sst = isT1 ? YS : RS;
+            T* dst = isT1 ? T1 : T2;
+            const int dsto = isT1 ? RS : YS;
+            for (int q = off[c]; q < off[c + 1]; ++q) {
+              const int2 ai = lst[q];
+              const T w = (T)dA[ai.x];
 #pragma unroll
               for (int u = 0; u < EB; ++u)
-                if (u < tn) T2[(t0 + u) * YS + m] = acc[u];
+                if (u < tn) acc[u] += w * (T)src[(t0 + u) * sst + ai.y];
             }
+#pragma unroll
+            for (int u = 0; u < EB; ++u)
+              if (u < tn) dst[(t0 + u) * dsto + c] = acc[u];
           }
         }
         group_sync(g);
