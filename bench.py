@@ -414,7 +414,7 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="ACE workloads: the default site-kernel schedule")
     p.add_argument("--sharded-forms", action="store_true",
                    help="run the multi-GPU forms (slab exchange, sharded batch) also with one GPU")
-    p.add_argument("--only-form", choices=["skin", "batch", "design", "surrogate"],
+    p.add_argument("--only-form", choices=["skin", "batch", "design", "surrogate", "snapshot"],
                    help="run one of the other configurations alone and print its record (no headline)")
     return p.parse_args()
 
@@ -734,10 +734,59 @@ def forms(args, dev, stream, flush, F_head, outputs):
         outputs[name]["mixed_key"] = key
         h32.close()
     out["lj_fcc40_256000_skin1.0_md"] = skin_form(dev, stream, flush)
+    out["lj_fcc40_256000_snapshot"] = snapshot_form(dev, stream, flush)
     out["ace_batch4096_fp64_graph"] = batch_form(dev, stream, flush, outputs)
     out["surrogate_b2_80_1024000"] = surrogate_form(dev, stream, flush)
     out["ace_design_rows_1024"] = design_form(dev, stream, flush)
     return out
+
+
+def snapshot_form(dev, stream, flush, steps=10):
+    """Neighbour snapshot of LJ FCC 40³ (256,000 atoms, cutoff 8.5 Å): the
+    directed (i, j, S, R) lists of `neighbour_list` built on the device
+    (cell lists, per-atom count, scan, fill) by `pfw_neighbour_count`, which
+    reads the total back to size the lists; then, end to end, the same plus
+    the copy of the lists to host memory (`pfw_neighbour_fill`).  The device
+    time is the whole count call; the fill writes 40 B per directed entry
+    (j, S, R) and the offsets 8 B per atom."""
+    import torch
+
+    from pfw_b200 import lib
+    w = Workload("lj")
+    h = lib.Handle(lib.FP64, device=dev.index)
+    h.set_stream(ctypes.c_void_p(stream.cuda_stream))
+    h.set_geometry(w.sys.X, w.sys.H, w.sys.pbc, w.sys.species)
+    cutoff = w.config["cutoff"]
+    tot = np.zeros(1, np.int64)
+    i64p = ctypes.POINTER(ctypes.c_int64)
+
+    def build():
+        h.check(h.L.pfw_neighbour_count(h.ws, float(cutoff), tot.ctypes.data_as(i64p)))
+
+    for _ in range(3):
+        build()
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        build()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    M = int(tot[0])
+    t0 = time.perf_counter()
+    offs, j, S, R = h.neighbour_list(cutoff)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    h.close()
+    m = float(np.mean(ms))
+    written = 40 * M + 8 * (w.n + 1)
+    return dict(value=M / (m * 1e-3), unit="directed entries/s", ms_per_step=m, entries=M, atoms=w.n,
+                bytes_written=written, write_gbs=written / (m * 1e-3) / 1e9,
+                e2e=dict(ms=e2e_ms, value=M / (e2e_ms * 1e-3), unit="directed entries/s",
+                         d2h_bytes=written, api="pfw_neighbour_count + pfw_neighbour_fill (host lists)"),
+                lists_consistent=bool(offs[-1] == M and (M == 0 or (j.min() >= 0 and j.max() < w.n))),
+                note="device time includes the cell-list build and one host read of the total")
 
 
 def skin_form(dev, stream, flush, steps=50, skin=1.0):
@@ -1065,6 +1114,8 @@ def run_one_form(args):
             rec = batch_form(dev, stream, flush, {})
         elif args.only_form == "surrogate":
             rec = surrogate_form(dev, stream, flush)
+        elif args.only_form == "snapshot":
+            rec = snapshot_form(dev, stream, flush)
         else:
             rec = design_form(dev, stream, flush)
     torch.cuda.synchronize()

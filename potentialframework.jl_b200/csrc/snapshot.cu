@@ -3,8 +3,8 @@
 //
 // Count pass (entries per centre), exclusive scan into original-order CSR
 // offsets, fill pass writing (j, S, R) for each centre in traversal order.
-// Every entry is emitted by its own centre's lane, so the two directions of
-// an unordered pair are produced by different lanes with no shared writes.
+// Every entry is selected by its own centre's lane and written to that
+// centre's range only, so no two threads write the same entry.
 #include <algorithm>
 
 #include "pfw_internal.h"
@@ -37,6 +37,14 @@ __global__ void __launch_bounds__(NB_WARPS * 32)
   if (cur_i >= 0) count[perm[cur_i]] = cnt;
 }
 
+// The fill traverses exactly as the count pass, so each centre's entries land
+// in [offsets[a], offsets[a+1]).  At every drain each lane first keeps its
+// in-range candidates, in visit order, at the front of its own list; then
+// the warp writes the lanes' entries one lane after another, consecutive
+// threads taking consecutive entries, so the j, S and R stores of a warp are
+// contiguous instead of 32 scattered lists.  The displacement is recomputed
+// by the writing thread with the same arithmetic, so R is bit-identical to
+// the tested value.
 template <int MODE>
 __global__ void __launch_bounds__(NB_WARPS * 32)
     k_nb_fill(const SysGeom* __restrict__ sysv, const int* __restrict__ cell_sys, const int* __restrict__ cell_start,
@@ -44,34 +52,82 @@ __global__ void __launch_bounds__(NB_WARPS * 32)
               const int64_t* __restrict__ offsets, int* __restrict__ jout, int* __restrict__ Sout,
               double* __restrict__ Rout) {
   __shared__ WarpStage stage[NB_WARPS];
+  __shared__ double s_pi[NB_WARPS][3][32];  // each lane's centre, read by the writing warp
+  __shared__ long long s_o[NB_WARPS][32];   // each lane's next output entry
+  __shared__ int s_w[NB_WARPS][3][32];      // each lane's centre wrap count
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x * NB_WARPS + warp;
   if (cell >= ncells) return;
   const SysGeom& g = sysv[cell_sys[cell]];
+  WarpStage& sg = stage[warp];
   int cur_i = -1;
   int64_t o = 0;
   int wi[3] = {0, 0, 0};
-  warp_traverse_cell<MODE>(g, cell, cell_start, pos, stage[warp], lane,
-                           [&](int i, int j, const double4& pi, const double4& pj, const StencilEntry& se,
-                               const double* d, double) {
-                             const int a = perm[i], bb = perm[j];
-                             if (i != cur_i) {
-                               cur_i = i;
-                               o = offsets[a];
-                               wi[0] = wind[3 * a]; wi[1] = wind[3 * a + 1]; wi[2] = wind[3 * a + 2];
-                             }
-                             const int wj[3] = {wind[3 * bb], wind[3 * bb + 1], wind[3 * bb + 2]};
-                             int S[3];
-                             pair_image(g, se, pi, pj, wi, wj, S);
-                             if (jout) jout[o] = bb;
-                             if (Sout) {
-                               Sout[3 * o] = S[0]; Sout[3 * o + 1] = S[1]; Sout[3 * o + 2] = S[2];
-                             }
-                             if (Rout) {
-                               Rout[3 * o] = d[0]; Rout[3 * o + 1] = d[1]; Rout[3 * o + 2] = d[2];
-                             }
-                             ++o;
-                           });
+  traverse_lists<MODE>(
+      g, cell, cell_start, pos, sg, lane,
+      [&](bool have, int i, const double4& pi, int& cnt) {
+        __syncwarp();
+        int np = 0;
+        if (have) {
+          if (i != cur_i) {
+            cur_i = i;
+            const int a = perm[i];
+            o = offsets[a];
+            wi[0] = wind[3 * a];
+            wi[1] = wind[3 * a + 1];
+            wi[2] = wind[3 * a + 2];
+          }
+          // compaction in place: slot np <= q was already read
+          for (int q = 0; q < cnt; ++q) {
+            const unsigned item = sg.list[list_slot(q, lane)];
+            const double4 pj = pos[item & 0xFFFFFFu];
+            double d[3];
+            candidate_displacement<MODE>(g, sg.ent[item >> 24], pi, pj, d);
+            if (xr2(d[0], d[1], d[2]) < g.c2) sg.list[list_slot(np++, lane)] = item;
+          }
+        }
+        cnt = 0;
+        s_pi[warp][0][lane] = pi.x;
+        s_pi[warp][1][lane] = pi.y;
+        s_pi[warp][2][lane] = pi.z;
+        s_o[warp][lane] = o;
+        s_w[warp][0][lane] = wi[0];
+        s_w[warp][1][lane] = wi[1];
+        s_w[warp][2][lane] = wi[2];
+        __syncwarp();
+        unsigned pending = __ballot_sync(0xffffffffu, np > 0);
+        while (pending) {
+          const int L = __ffs(pending) - 1;
+          pending &= pending - 1;
+          const int nL = __shfl_sync(0xffffffffu, np, L);
+          const double4 piL = make_double4(s_pi[warp][0][L], s_pi[warp][1][L], s_pi[warp][2][L], 0.0);
+          const int64_t oL = s_o[warp][L];
+          const int wL[3] = {s_w[warp][0][L], s_w[warp][1][L], s_w[warp][2][L]};
+          for (int t = lane; t < nL; t += 32) {
+            const unsigned item = sg.list[list_slot(t, L)];
+            const int j = (int)(item & 0xFFFFFFu);
+            const StencilEntry& se = sg.ent[item >> 24];
+            const double4 pj = pos[j];
+            double d[3];
+            candidate_displacement<MODE>(g, se, piL, pj, d);
+            const int bb = perm[j];
+            const int wj[3] = {wind[3 * bb], wind[3 * bb + 1], wind[3 * bb + 2]};
+            int S[3];
+            pair_image(g, se, piL, pj, wL, wj, S);
+            const int64_t e = oL + t;
+            if (jout) jout[e] = bb;
+            if (Sout) {
+              Sout[3 * e] = S[0]; Sout[3 * e + 1] = S[1]; Sout[3 * e + 2] = S[2];
+            }
+            if (Rout) {
+              Rout[3 * e] = d[0]; Rout[3 * e + 1] = d[1]; Rout[3 * e + 2] = d[2];
+            }
+          }
+        }
+        o += np;
+        __syncwarp();
+      },
+      [](bool, int, const double4&) {});
 }
 
 static bool all_shift_mode(const Prepared& P) {

@@ -66,6 +66,21 @@ using WarpStage = WarpStageK<LIST_K>;
 
 __device__ __forceinline__ int list_slot(int slot, int lane) { return slot * 32 + (lane ^ (slot & 31)); }
 
+// Exact displacement of a listed candidate j from centre i: the stencil
+// entry's shift added to the sorted coordinates' difference (MODE 0), or the
+// cell's minimum-image / explicit-image rule (MODE 1).
+template <int MODE>
+__device__ __forceinline__ void candidate_displacement(const SysGeom& g, const StencilEntry& se, const double4& pi,
+                                                       const double4& pj, double d[3]) {
+  if (MODE == 0) {
+    d[0] = xadd(xsub(pj.x, pi.x), se.sh[0]);
+    d[1] = xadd(xsub(pj.y, pi.y), se.sh[1]);
+    d[2] = xadd(xsub(pj.z, pi.z), se.sh[2]);
+  } else {
+    displacement(g, se, pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, d);
+  }
+}
+
 // Walk the lane's list: PFW_DRAIN_UNROLL neighbour loads are issued before
 // any of them is used, so their latencies overlap.
 template <int MODE, class Stage, class Visit>
@@ -88,13 +103,7 @@ __device__ __forceinline__ void drain_lists(const SysGeom& g, const double4* __r
         const int j = (int)(item[u] & 0xFFFFFFu);
         const StencilEntry& se = stage.ent[item[u] >> 24];
         double d[3];
-        if (MODE == 0) {
-          d[0] = xadd(xsub(pj[u].x, pi.x), se.sh[0]);
-          d[1] = xadd(xsub(pj[u].y, pi.y), se.sh[1]);
-          d[2] = xadd(xsub(pj[u].z, pi.z), se.sh[2]);
-        } else {
-          displacement(g, se, pi.x, pi.y, pi.z, pj[u].x, pj[u].y, pj[u].z, d);
-        }
+        candidate_displacement<MODE>(g, se, pi, pj[u], d);
         const double r2 = xr2(d[0], d[1], d[2]);
         if (r2 < g.c2) visit(i, j, pi, pj[u], se, d, r2);
       }
