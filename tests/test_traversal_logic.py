@@ -13,7 +13,11 @@
   exactly its own entries — checked on random count vectors, zero counts
   included;
 * the half-stencil pass walks each lane's share directly on the per-home
-  candidate masks: every entry taken once, in home-major order, in range.
+  candidate masks: every entry taken once, in home-major order, in range;
+* the ACE site kernel's balanced adjoint sums every term once, in order;
+* the snapshot fill compacts each lane's in-range candidates in place and
+  writes the lanes' entries with the whole warp: every entry of every centre
+  lands once, in visit order, inside the centre's CSR range.
 """
 import numpy as np
 
@@ -243,3 +247,91 @@ def test_balanced_adjoint_sums_every_term_once_in_order():
             dA = balanced_adjoint(toff, G)
             for a in range(len(toff) - 1):
                 assert dA[a] == list(range(toff[a], toff[a + 1])), (a, toff[:5])
+
+
+def list_slot(slot, lane):
+    """The shared-memory list layout (csrc/traverse.cuh): slot·32 + (lane ^ (slot & 31))."""
+    return slot * 32 + (lane ^ (slot & 31))
+
+
+def snapshot_fill(chunks, K=64):
+    """The snapshot fill (csrc/snapshot.cu, k_nb_fill), restated for one warp.
+
+    chunks: per chunk of home atoms, a list of drains; a drain gives each of
+    the 32 lanes (centre atom id, or None) a list of (candidate id, in range).
+    Returns the offsets of the count pass and the output array of
+    (centre, candidate) written by the warp-cooperative fill."""
+    # count pass: in-range candidates per centre
+    count = {}
+    for drains in chunks:
+        for drain in drains:
+            for centre, cand in drain:
+                if centre is not None:
+                    count[centre] = count.get(centre, 0) + sum(1 for _, ok in cand if ok)
+    centres = sorted(count)
+    offsets, total = {}, 0
+    for a in centres:
+        offsets[a] = total
+        total += count[a]
+    out = [None] * total
+    written = [0] * total
+    cur, o = [None] * 32, [0] * 32
+    for drains in chunks:
+        for drain in drains:
+            lists = [None] * (K * 32)
+            np_ = [0] * 32
+            for lane, (centre, cand) in enumerate(drain):
+                assert len(cand) <= K
+                for q, item in enumerate(cand):
+                    lists[list_slot(q, lane)] = item
+                if centre is None:
+                    continue
+                if centre != cur[lane]:
+                    cur[lane], o[lane] = centre, offsets[centre]
+                # compaction in place: slot np <= q has been read already
+                for q in range(len(cand)):
+                    item = lists[list_slot(q, lane)]
+                    if item[1]:
+                        assert np_[lane] <= q
+                        lists[list_slot(np_[lane], lane)] = item
+                        np_[lane] += 1
+            for L in range(32):
+                for t0 in range(0, np_[L], 32):
+                    slots = [list_slot(t, L) for t in range(t0, min(t0 + 32, np_[L]))]
+                    assert len({s % 32 for s in slots}) == len(slots)  # distinct banks
+                    for t in range(t0, min(t0 + 32, np_[L])):
+                        e = o[L] + t
+                        assert 0 <= e < total
+                        out[e] = (cur[L], lists[list_slot(t, L)][0])
+                        written[e] += 1
+            for lane in range(32):
+                o[lane] += np_[lane]
+    return offsets, count, out, written
+
+
+def test_snapshot_fill_writes_every_entry_once_in_visit_order():
+    rng = np.random.default_rng(11)
+    for _ in range(60):
+        chunks, expect, next_id = [], {}, 0
+        for _c in range(int(rng.integers(1, 4))):
+            nh = int(rng.integers(1, 33))
+            homes = list(range(next_id, next_id + nh))
+            next_id += nh
+            drains = []
+            for _d in range(int(rng.integers(1, 6))):
+                drain = []
+                for lane in range(32):
+                    if lane >= nh:
+                        drain.append((None, []))
+                        continue
+                    n = int(rng.integers(0, 65)) if rng.random() > 0.1 else 0
+                    cand = [(int(rng.integers(0, 10 ** 6)), bool(rng.random() < 0.6)) for _ in range(n)]
+                    drain.append((homes[lane], cand))
+                    expect.setdefault(homes[lane], []).extend(j for j, ok in cand if ok)
+                drains.append(drain)
+            chunks.append(drains)
+        offsets, count, out, written = snapshot_fill(chunks)
+        assert all(w == 1 for w in written)
+        for a, js in expect.items():
+            assert count[a] == len(js)
+            assert [out[offsets[a] + k] for k in range(count[a])] == [(a, j) for j in js]
