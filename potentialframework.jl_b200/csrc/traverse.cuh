@@ -332,12 +332,17 @@ __device__ __forceinline__ void warp_traverse_cell(const SysGeom& g, int cell, c
 
 // Integer image of the directed pair i→j relative to the ORIGINAL
 // coordinates: S = lattice + wind[i] - wind[j] (interface.jl:126-134).
+// Minimum image takes lattice = -rint((x_j - x_i)/L) per periodic axis.
+// With the per-cell wrap (fast_shift: at least 4 bins of width >= c, so
+// L >= 4c) an in-range pair has x_j - x_i = d - s·L with |d| < c <= L/4 for
+// its stencil entry's shift s, so that rint is -s with a margin of a quarter
+// and the lattice is the entry's own s: no division.
 __device__ __forceinline__ void pair_image(const SysGeom& g, const StencilEntry& se, const double4& pi,
                                            const double4& pj, const int* wi, const int* wj, int S[3]) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     int lattice;
-    if (g.minimum_image) {
+    if (g.minimum_image && !g.fast_shift) {
       const double dd = xsub(a == 0 ? pj.x : a == 1 ? pj.y : pj.z, a == 0 ? pi.x : a == 1 ? pi.y : pi.z);
       lattice = g.pbc[a] ? -(int)rint(xdiv(dd, g.L[a])) : 0;
     } else {
