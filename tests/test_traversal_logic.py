@@ -17,7 +17,10 @@
 * the ACE site kernel's balanced adjoint sums every term once, in order;
 * the snapshot fill compacts each lane's in-range candidates in place and
   writes the lanes' entries with the whole warp: every entry of every centre
-  lands once, in visit order, inside the centre's CSR range.
+  lands once, in visit order, inside the centre's CSR range;
+* on minimum-image grids with the per-cell wrap (at least 4 bins of width
+  >= c per periodic axis) the stencil entry's shift s equals the reference's
+  image -rint((x_j - x_i)/L) for every in-range pair.
 """
 import numpy as np
 
@@ -335,3 +338,40 @@ def test_snapshot_fill_writes_every_entry_once_in_visit_order():
         for a, js in expect.items():
             assert count[a] == len(js)
             assert [out[offsets[a] + k] for k in range(count[a])] == [(a, j) for j in js]
+
+
+def test_per_cell_wrap_shift_is_the_minimum_image_lattice():
+    """csrc/traverse.cuh pair_image: with L >= 4c the image of an in-range
+    pair found through stencil offset o (shift s when the neighbour cell index
+    wraps) is -rint(fl(fl(x_j - x_i) / L)) = s; checked per axis on wrapped
+    coordinates, pairs placed at distances up to c(1 - 1e-15) and at cell and
+    box edges."""
+    rng = np.random.default_rng(5)
+    wrapped = checked = 0
+    for _ in range(300):
+        c = float(rng.uniform(0.5, 10.0))
+        dims = int(rng.integers(4, 40))
+        L = float(rng.uniform(dims * c, (dims + 1) * c))  # floor(L / c) = dims
+        dims = int(np.floor(L / c))
+        assert dims >= 4
+        size = L / dims
+        xi = np.concatenate([rng.uniform(0.0, L, 200), [0.0, np.nextafter(L, 0.0), size, np.nextafter(size, 0.0)]])
+        dist = np.concatenate([rng.uniform(-c, c, 200), [c * (1 - 1e-15), -c * (1 - 1e-15), 0.5 * c, -0.5 * c]])
+        xj = np.mod(xi + dist, L)
+        xj = np.where(xj >= L, 0.0, xj)
+        ci = np.minimum(np.floor(xi / size).astype(int), dims - 1)
+        cj = np.minimum(np.floor(xj / size).astype(int), dims - 1)
+        for a_i, a_j, k_i, k_j in zip(xi, xj, ci, cj):
+            for o in (-1, 0, 1):
+                v = k_i + o
+                s = -1 if v < 0 else (1 if v >= dims else 0)
+                if (v - s * dims) != k_j:
+                    continue
+                d = (a_j - a_i) + s * L  # the kernel's displacement through this entry
+                if abs(d) >= c:
+                    continue
+                lattice = -int(np.rint((a_j - a_i) / L))
+                assert lattice == s, (c, L, a_i, a_j, o)
+                checked += 1
+                wrapped += s != 0
+    assert checked > 30000 and wrapped > 1000, (checked, wrapped)
