@@ -2,8 +2,8 @@
 hot path of PotentialFrameWork.jl (cell lists, SmoothPair/LJ pairs, ACE)."""
 from .api import (ACECalculator, Energy, EnergyForcesVirial, EnergyOnly, Forces, LennardJones, SmoothPair,  # noqa
                   Virial, Workspace, calculate, energy_forces, energy_forces_, energy_forces_virial,
-                  energy_forces_virial_, evaluate, evaluate_, forces, forces_, lennard_jones, load_resolved,
-                  neighbour_list, neighbours, potential_energy, save_calculator, trainable_parameters, virial,
-                  with_parameters)
+                  energy_forces_virial_, evaluate, evaluate_, forces, forces_, get_parameters, lennard_jones,
+                  load_resolved, neighbour_list, neighbours, potential_energy, save_calculator, set_parameters,
+                  trainable_parameters, virial, with_parameters)
 from .lib import ArgumentError, DimensionMismatch, DomainError, PFWError  # noqa: F401
 from .precision import compare_precision  # noqa: F401

@@ -99,6 +99,17 @@ class SmoothPair:
     def cutoff(self):
         return self.radius
 
+    def get_parameters(self):
+        """AC.get_parameters (PairPotentials/parameters.jl:34-37): the upper
+        triangle of the amplitude table in column order, A[i, j] for
+        j = 1..n, i = 1..j."""
+        n = len(self.labels)
+        return {"amplitudes": np.array([self.amplitudes[i, j] for j in range(n) for i in range(j + 1)])}
+
+    def set_parameters(self, parameters):
+        """AC.set_parameters! (parameters.jl:54): a new model, as with_parameters."""
+        return with_parameters(self, parameters)
+
 
 class LennardJones:
     """Energy-shifted LJ (PairPotentials/lennard_jones.jl:5-33)."""
@@ -110,6 +121,13 @@ class LennardJones:
 
     def cutoff(self):
         return self.radius
+
+    def get_parameters(self):
+        """AC.get_parameters (PairPotentials/lennard_jones.jl:23)."""
+        return {"epsilon": self.epsilon, "sigma": self.sigma}
+
+    def set_parameters(self, parameters):
+        return with_parameters(self, parameters)
 
 
 def lennard_jones(epsilon=0.0103, sigma=3.4, radius=8.5):
@@ -206,14 +224,16 @@ def evaluate(sys, p, width=4, precision="Float64", bruteforce_threshold=32, **kw
 
 
 def with_parameters(p, parameters):
-    """with_parameters (PairPotentials/models.jl:103-110, lennard_jones.jl:26-29)."""
+    """with_parameters (PairPotentials/parameters.jl:38-53, lennard_jones.jl:24-27)."""
     if isinstance(p, SmoothPair):
         if set(parameters) != {"amplitudes"}:
             raise ArgumentError(_lib.EINVAL, "SmoothPair parameters must contain only amplitudes; cutoff is fixed")
         a = np.asarray(parameters["amplitudes"], dtype=np.float64)
         n = len(p.labels)
         if a.shape != (n * (n + 1) // 2,):
-            raise ArgumentError(_lib.EINVAL, "incorrect SmoothPair amplitude count")
+            raise ArgumentError(_lib.EINVAL, "amplitudes must be a real vector of length n*(n+1)/2")
+        if not np.all(np.isfinite(a)):
+            raise ArgumentError(_lib.EINVAL, "amplitudes must be finite")
         A = np.zeros((n, n))
         for j in range(n):
             for i in range(j + 1):
@@ -335,6 +355,22 @@ class ACECalculator:
 
     def cutoff(self):
         return self.model.cutoff
+
+
+def get_parameters(p):
+    """AtomsCalculators.get_parameters for the pair models and ACECalculator."""
+    if not hasattr(p, "get_parameters"):
+        raise ArgumentError(_lib.EINVAL, f"{type(p).__name__} has no parameters")
+    return p.get_parameters()
+
+
+def set_parameters(p, parameters):
+    """AtomsCalculators.set_parameters!: the pair models are immutable and
+    return a new model (parameters.jl:54); ACECalculator installs the
+    parameters in place and returns itself (ACE/calculators.jl:38-42)."""
+    if not hasattr(p, "set_parameters"):
+        raise ArgumentError(_lib.EINVAL, f"{type(p).__name__} has no parameters")
+    return p.set_parameters(parameters)
 
 
 def load_resolved(path):
