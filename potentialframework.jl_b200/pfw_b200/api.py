@@ -357,6 +357,14 @@ class ACECalculator:
         return self.model.cutoff
 
 
+def cutoff(p):
+    """cutoff(p) (PairPotentials/models.jl:44 and RadialPotential): the model's
+    cutoff radius in Å, for SmoothPair, Lennard-Jones and ACECalculator."""
+    if not hasattr(p, "cutoff"):
+        raise ArgumentError(_lib.EINVAL, f"{type(p).__name__} has no cutoff")
+    return p.cutoff()
+
+
 def get_parameters(p):
     """AtomsCalculators.get_parameters for the pair models and ACECalculator."""
     if not hasattr(p, "get_parameters"):

@@ -47,6 +47,13 @@ def test_lennard_jones_parameters():
         api.with_parameters(p, {"epsilon": -1.0, "sigma": 3.0})
 
 
+def test_cutoff():
+    assert api.cutoff(api.lennard_jones(radius=8.5)) == 8.5
+    assert api.cutoff(api.SmoothPair(["H"], [[1.0]], 2.0)) == 2.0
+    with pytest.raises(ArgumentError):
+        api.cutoff(object())
+
+
 def test_models_without_parameters_are_rejected():
     with pytest.raises(ArgumentError):
         api.get_parameters(object())
