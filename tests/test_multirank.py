@@ -1,4 +1,4 @@
-"""Multi-rank paths on CPU (world size 2, gloo).  Batches: the LPT shards
+"""Multi-rank paths on CPU (world sizes 2 and 3, gloo).  Batches: the LPT shards
 cover every system once and balance the expected edge counts; each rank
 evaluates its shard with the CPU oracle (standing in for the rank's GPU batch
 launch) and the gathered per-system energies, virials and forces equal a
@@ -174,14 +174,14 @@ class CpuSlabRank:
         W.zero_()
 
 
-def _exchange_main(rank, world, port, out_path):
+def _exchange_main(rank, world, port, out_path, nc=10):
     import torch
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         m = _tial()
-        s = WL.b2(seed=9, nc=10, a=2.95)
+        s = WL.b2(seed=9, nc=nc, a=2.95)
         plan = PAR.SlabPlan(s, world, 2.0 * m.cutoff)
         rk = CpuSlabRank(plan, rank, m)
         E = torch.zeros(1, dtype=torch.float64)
@@ -198,13 +198,17 @@ def _exchange_main(rank, world, port, out_path):
         dist.destroy_process_group()
 
 
-def test_two_rank_slab_exchange_matches_serial(tmp_path):
+@pytest.mark.parametrize("world,nc", [(2, 10), (3, 14)])
+def test_slab_exchange_matches_serial(tmp_path, world, nc):
+    """With 2 ranks a rank's lower and upper neighbour are the same rank; with
+    3 they are different ranks, and every band crosses to its own receiver."""
     from oracle import oracle as O
     out = str(tmp_path / "exch.npy")
-    mp.start_processes(_exchange_main, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
+    mp.start_processes(_exchange_main, args=(world, _free_port(), out, nc), nprocs=world, join=True,
+                       start_method="spawn")
     got = np.load(out)
     m = _tial()
-    s = WL.b2(seed=9, nc=10, a=2.95)
+    s = WL.b2(seed=9, nc=nc, a=2.95)
     r = O.AceOracle(m).evaluate(s.X, s.H, s.pbc, s.species)
     assert abs(got[0] - r["energy"]) <= 1e-9 * abs(r["energy"])
     assert np.allclose(got[1:].reshape(-1, 3), r["forces"], rtol=0, atol=1e-9 * np.abs(r["forces"]).max())
