@@ -6,7 +6,9 @@
 * the analytic known answers of test/periodic_images.jl:97-104,
   test/runtests.jl:89-93,152-154 and test/neighbour_interface.jl:103-110;
 * independent O(N²) brute-force sums (tests/brute.py) over the fixture
-  sweeps of test/runtests.jl:66-96 and test/periodic_images.jl:61-124.
+  sweeps of test/runtests.jl:66-96 and test/periodic_images.jl:61-124;
+* the directed neighbour set of test/ace.jl:21-58's skew 2 Å cell at the
+  5.5 Å ACE cutoff against its +-6 shell image sum.
 """
 import os
 
@@ -149,3 +151,24 @@ def test_snapshot_min_image_vs_bruteforce():
     for i in range(len(s)):
         for k in range(offs[i], offs[i + 1]):
             assert np.allclose(R[k], s.X[j[k]] - s.X[i] + s.H @ S[k], atol=1e-12)
+
+
+@pytest.mark.parametrize("pbc", [(1, 1, 1), (1, 0, 1), (0, 0, 0)])
+@pytest.mark.parametrize("n", [3, 1, 0, 2])
+def test_ace_environment_set_skew_cell(pbc, n):
+    # test/ace.jl:21-58: a skew cell of about 2 Å against the 5.5 Å ACE cutoff,
+    # the first atom placed two cell vectors outside the cell; the directed
+    # (i, j, S) set equals the +-6 shell image sum
+    H = np.array([[2.1, 0.6, 0.2], [0, 2.2, 0.4], [0, 0, 2.0]])
+    frac = np.array([[0.1, 0.4, 0.8], [0.2, 0.6, 0.3], [0.1, 0.7, 0.5]])[:, :n]
+    X = (H @ frac).T.copy()
+    if n > 0:
+        X[0] += 2 * H[:, 0]
+    sp = np.array([0, 1, 0][:n], np.int32)
+    offs, j, S, R = O.neighbour_list(X, H, pbc, 5.5)
+    _, _, _, pairs = image_oracle(X, H, pbc, sp, smooth(), 5.5, shell=6)
+    got = {(i, int(j[k]), tuple(int(v) for v in S[k])) for i in range(n) for k in range(offs[i], offs[i + 1])}
+    assert got == pairs
+    for i in range(n):
+        for k in range(offs[i], offs[i + 1]):
+            assert np.allclose(R[k], X[j[k]] - X[i] + H @ S[k], atol=1e-12)
