@@ -155,7 +155,9 @@ typedef struct pfw_ace_tables {
   const int32_t* density;       /* [D][2] (radial channel, harmonic index) */
   int32_t nproducts;            /* P */
   const int32_t* product_offsets; /* [P+1] CSR into product_factors */
-  const int32_t* product_factors; /* density indices of each product */
+  const int32_t* product_factors; /* density indices of each product: 1 to 4 per
+                                     product (correlation order <= 4; longer or empty
+                                     products are rejected with PFW_EINVAL) */
   int32_t nbasis;               /* nB invariants (rows of the coupling) */
   int32_t ncoupling;            /* stored coupling entries */
   const int32_t* coupling_rows; /* [nnz] invariant index, column-major (CSC) order */

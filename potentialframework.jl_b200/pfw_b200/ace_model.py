@@ -21,6 +21,9 @@ import numpy as np
 
 from .errors import argument_error, dimension_mismatch
 
+# factors per product the device records hold (ushort4 with a sentinel)
+MAX_ORDER = 4
+
 ENVELOPE_KIND = {"PolyEnvelope2sX": 1, "ACE1_PolyEnvelope1sR": 2, "PolyEnvelope1sR": 3}
 
 
@@ -198,7 +201,14 @@ class PackedACE:
         return self.atomic_numbers.index(z)
 
     def tables(self) -> pfw_ace_tables:
-        """C struct view; the arrays stay owned by this object."""
+        """C struct view; the arrays stay owned by this object.  The device
+        kernels hold a product's factors in one 4-wide record, so products of
+        more than 4 densities (correlation order above 4) are rejected here,
+        as the library rejects them; every shipped model has order <= 3."""
+        if any(len(p) > MAX_ORDER for p in self.products):
+            raise argument_error(f"ACE correlation order above {MAX_ORDER} is not supported on the device")
+        if any(len(p) == 0 for p in self.products):
+            raise argument_error("empty ACE product")
         offs, facs = self.product_csr()
         dens = np.ascontiguousarray(self.density, dtype=np.int32)
         self._keep = [offs, facs, dens]

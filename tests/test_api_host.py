@@ -103,3 +103,21 @@ def test_in_place_destinations_check_their_shape():
     assert F.sum() == 12
     with pytest.raises(DimensionMismatch):
         api._add_into(F, np.ones((3, 3)))
+
+
+def test_device_tables_reject_products_above_order_4():
+    import dataclasses
+
+    from pfw_b200 import ace_generate as G
+    from pfw_b200.ace_model import MAX_ORDER, read_resolved
+    m = read_resolved(G.generate_b2_model())
+    assert max(len(p) for p in m.products) <= MAX_ORDER
+    m.tables()  # the shipped order-3 model packs
+    long = dataclasses.replace(m, products=[list(p) for p in m.products])
+    long.products[0] = [0, 1, 2, 3, 4]
+    with pytest.raises(ArgumentError, match="correlation order above 4"):
+        long.tables()
+    empty = dataclasses.replace(m, products=[list(p) for p in m.products])
+    empty.products[-1] = []
+    with pytest.raises(ArgumentError, match="empty ACE product"):
+        empty.tables()
