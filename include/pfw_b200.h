@@ -147,13 +147,13 @@ typedef struct pfw_radial_family {
 } pfw_radial_family;
 
 typedef struct pfw_ace_tables {
-  int32_t nz;                   /* species channels */
+  int32_t nz;                   /* species channels, 1..16 */
   int32_t lmax;                 /* harmonics degree (L2, l*l+l+m order), 0..6 */
   pfw_radial_family radial;     /* R channels */
   pfw_radial_family pair;       /* Q (pair) channels */
-  int32_t ndensity;             /* D */
+  int32_t ndensity;             /* D, at most 65534 */
   const int32_t* density;       /* [D][2] (radial channel, harmonic index) */
-  int32_t nproducts;            /* P */
+  int32_t nproducts;            /* P, at most 65535 */
   const int32_t* product_offsets; /* [P+1] CSR into product_factors */
   const int32_t* product_factors; /* density indices of each product: 1 to 4 per
                                      product (correlation order <= 4; longer or empty
