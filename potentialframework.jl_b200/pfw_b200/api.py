@@ -19,7 +19,8 @@ Same names, argument meaning and error behaviour as PotentialFrameWork.jl:
                                     ACE/persistence.jl:101-167, ACE/serial.jl:12-16
 
 Systems are numeric (Å): any object with X (n,3), H (3,3, columns = cell
-vectors), pbc (3 flags) and species (channel ints or label strings).  Unit
+vectors), pbc (3 flags) and species (channel ints, the model's labels, or
+element symbols for ACE models, which are labelled by atomic number).  Unit
 handling is the caller's: the Julia shim strips Unitful units at the boundary
 exactly where the reference does (storage.jl:74-78).  Every evaluation runs
 on the GPU through libpfw_b200.so; there is no CPU path.
@@ -77,6 +78,35 @@ def _request_bits(request):
         else:
             raise ArgumentError(_lib.EINVAL, "supported properties are Energy(), Forces() and Virial()")
     return bits
+
+
+_ELEMENTS = ("H He Li Be B C N O F Ne Na Mg Al Si P S Cl Ar K Ca Sc Ti V Cr Mn Fe Co Ni Cu Zn Ga Ge As Se Br Kr "
+             "Rb Sr Y Zr Nb Mo Tc Ru Rh Pd Ag Cd In Sn Sb Te I Xe Cs Ba La Ce Pr Nd Pm Sm Eu Gd Tb Dy Ho Er Tm Yb "
+             "Lu Hf Ta W Re Os Ir Pt Au Hg Tl Pb Bi Po At Rn Fr Ra Ac Th Pa U Np Pu Am Cm Bk Cf Es Fm Md No Lr Rf "
+             "Db Sg Bh Hs Mt Ds Rg Cn Nh Fl Mc Lv Ts Og").split()
+
+
+def species_channels(species, labels):
+    """Species of a system → the model's channel indices (bind_species,
+    PairPotentials/models.jl:50-58; ACE channels by atomic number).  Integer
+    arrays are channel indices already.  Other entries are matched to the
+    labels by equality; for models labelled by atomic number (ACE) an element
+    symbol is matched through its atomic number.  An entry the model has no
+    parameters for raises ArgumentError."""
+    sp = np.asarray(species)
+    if sp.dtype.kind in "iu":
+        return sp.astype(np.int32)
+    labels = list(labels)
+    numeric = all(isinstance(v, (int, np.integer)) for v in labels)
+    ids = []
+    for s in sp:
+        key = s
+        if numeric and isinstance(s, str) and s in _ELEMENTS:
+            key = _ELEMENTS.index(s) + 1
+        if key not in labels:
+            raise ArgumentError(_lib.EINVAL, f"potential has no parameters for species {s}")
+        ids.append(labels.index(key))
+    return np.array(ids, np.int32)
 
 
 class SmoothPair:
@@ -167,15 +197,7 @@ class Workspace:
 
     # geometry/model binding -------------------------------------------
     def _species(self, sys, labels):
-        sp = np.asarray(sys.species)
-        if sp.dtype.kind in "iu":
-            return sp.astype(np.int32)
-        ids = []
-        for s in sp:
-            if s not in labels:
-                raise ArgumentError(_lib.EINVAL, f"potential has no parameters for species {s}")
-            ids.append(labels.index(s))
-        return np.array(ids, np.int32)
+        return species_channels(sys.species, labels)
 
     def bind(self, sys, p):
         if isinstance(p, SmoothPair):

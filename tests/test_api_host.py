@@ -121,3 +121,17 @@ def test_device_tables_reject_products_above_order_4():
     empty.products[-1] = []
     with pytest.raises(ArgumentError, match="empty ACE product"):
         empty.tables()
+
+
+def test_species_channels():
+    # integer arrays are channel indices
+    assert api.species_channels(np.array([1, 0, 1]), ["H", "He"]).tolist() == [1, 0, 1]
+    # labels by equality (SmoothPair)
+    assert api.species_channels(np.array(["He", "H"]), ["H", "He"]).tolist() == [1, 0]
+    # ACE models are labelled by atomic number: element symbols map through it
+    assert api.species_channels(["Ti", "Al", "Ti"], [22, 13]).tolist() == [0, 1, 0]
+    assert api.species_channels(["V", "Al", "Ti"], [22, 13, 23]).tolist() == [2, 1, 0]
+    with pytest.raises(ArgumentError, match="no parameters for species Fe"):
+        api.species_channels(["Ti", "Fe"], [22, 13])
+    with pytest.raises(ArgumentError, match="no parameters for species Li"):
+        api.species_channels(["Li"], ["H", "He"])
