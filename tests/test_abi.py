@@ -41,3 +41,37 @@ def test_no_silent_cpu_fallback_without_gpu():
 def test_version():
     from pfw_b200 import lib
     assert lib.load().pfw_version().decode().count(".") == 2
+
+
+C_TO_JULIA = {"int32_t": "Int32", "double": "Float64", "uint8_t": "UInt8"}
+
+
+def c_struct_fields(name):
+    src = open(os.path.join(ROOT, "include", "pfw_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    body = re.search(r"typedef struct " + name + r"\s*\{(.*?)\}\s*" + name + ";", src, re.S).group(1)
+    out = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        m = re.match(r"(?:const\s+)?(\w+)\s*(\*?)\s*(\w+)$", decl)
+        ctype, ptr, field = m.groups()
+        jl = C_TO_JULIA.get(ctype, {"pfw_radial_family": "RadialFamilyC"}.get(ctype, ctype))
+        out.append((field, f"Ptr{{{jl}}}" if ptr else jl))
+    return out
+
+
+def julia_struct_fields(name):
+    src = open(os.path.join(ROOT, "potentialframework.jl_b200", "julia", "PFWB200.jl")).read()
+    body = re.search(r"\nstruct " + name + r"\n(.*?)\nend\n", src, re.S).group(1)
+    return [tuple(x.strip() for x in line.split("#")[0].split("::")) for line in body.strip().splitlines()]
+
+
+def test_julia_binding_structs_match_the_header():
+    """The Julia binding passes pfw_options, pfw_radial_family and
+    pfw_ace_tables by reference: its isbits mirrors must list the same
+    fields, in the same order, with the same types."""
+    assert julia_struct_fields("Options") == c_struct_fields("pfw_options")
+    assert julia_struct_fields("RadialFamilyC") == c_struct_fields("pfw_radial_family")
+    assert julia_struct_fields("ACETablesC") == c_struct_fields("pfw_ace_tables")
