@@ -1,5 +1,6 @@
 """CPU-side checks of the C ABI: the library builds, loads, and exports every
-symbol that include/pfw_b200.h declares; without a GPU it fails loudly."""
+symbol that include/pfw_b200.h declares; without a GPU it fails loudly; the
+Julia binding's struct mirrors match the header's structs."""
 import ctypes
 import os
 import re
