@@ -1,6 +1,7 @@
 """CPU-side checks of the C ABI: the library builds, loads, and exports every
 symbol that include/pfw_b200.h declares; without a GPU it fails loudly; the
-Julia binding's struct mirrors match the header's structs."""
+Julia binding's struct mirrors match the header's structs and its ccalls the
+declared argument counts."""
 import ctypes
 import os
 import re
@@ -76,3 +77,24 @@ def test_julia_binding_structs_match_the_header():
     assert julia_struct_fields("Options") == c_struct_fields("pfw_options")
     assert julia_struct_fields("RadialFamilyC") == c_struct_fields("pfw_radial_family")
     assert julia_struct_fields("ACETablesC") == c_struct_fields("pfw_ace_tables")
+
+
+def header_arity():
+    src = open(os.path.join(ROOT, "include", "pfw_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    out = {}
+    for name, args in re.findall(r"\b(pfw_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", src):
+        args = args.strip()
+        out[name] = 0 if args in ("", "void") else args.count(",") + 1
+    return out
+
+
+def test_julia_ccalls_match_the_header_arity():
+    src = open(os.path.join(ROOT, "potentialframework.jl_b200", "julia", "PFWB200.jl")).read()
+    calls = re.findall(r"ccall\(\(:(pfw_[a-z0-9_]+), libpfw\),\s*\w+(?:\{\w+\})?,\s*\(([^()]*(?:\([^()]*\))?[^()]*)\)", src)
+    assert len(calls) == src.count("ccall(")  # every ccall parsed
+    arity = header_arity()
+    for name, types in calls:
+        n = len([t for t in types.split(",") if t.strip()])
+        assert name in arity, name
+        assert n == arity[name], (name, n, arity[name])
